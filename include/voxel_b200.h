@@ -1,0 +1,192 @@
+/*
+ * libvoxel_b200 -- matrix-free Hex8 voxel elasticity on NVIDIA B200 (sm_100a).
+ *
+ * Plain C ABI: device pointers, sizes and a cudaStream_t in; an int status out (VX_OK == 0).
+ * The library never allocates or frees device memory: the caller owns every buffer, including
+ * the small `partials` scratch of the reducing kernels (sized by vx_partials_size()).  Calls are
+ * asynchronous on `stream` and never synchronise the device.  On failure the call returns a
+ * non-zero status and vx_last_error() gives a message for the calling host thread.
+ *
+ * Layouts.  "Author" layout (the hot path, as in the reference's src/voxel_mg.py:20-38): node
+ * n = (ix*(ny+1)+iy)*(nz+1)+iz, DOF 3n+c, element e = (ex*ny+ey)*nz+ez -- x slowest, z fastest.
+ * "Natural" layout (the reference's C product, experiments/session_a/inputs/reference.cc:23-28):
+ * x fastest.  Grids are element counts (nx, ny, nz), each >= 1, with 3*(nx+1)(ny+1)(nz+1) < 2^31.
+ *
+ * Dirichlet masks.  The hot path encodes the reference's 0/1 DOF mask (src/voxel_mg.py:129-130)
+ * as one byte per node: bit c set <=> DOF 3n+c is free.  A NULL node mask means "all free".
+ */
+#ifndef VOXEL_B200_H
+#define VOXEL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------- status */
+enum {
+    VX_OK = 0,
+    VX_ERR_INVALID_ARGUMENT = 1, /* bad shape, size or enum value                               */
+    VX_ERR_NULL_POINTER = 2,     /* a required pointer is NULL                                  */
+    VX_ERR_ALIGNMENT = 3,        /* a pointer is not aligned to its element size                */
+    VX_ERR_LAUNCH = 4,           /* CUDA launch error                                           */
+    VX_ERR_UNSUPPORTED = 5,      /* element outside the parity-block model, or unsupported mode */
+    VX_ERR_TIMEOUT = 6,          /* a bounded device wait ran out                               */
+    VX_ERR_CUDA = 7              /* another CUDA runtime error                                  */
+};
+
+/* Precision / storage selectors */
+enum {
+    VX_F64 = 0,       /* FP64 storage, FP64 arithmetic                                  */
+    VX_F32 = 1,       /* FP32 storage, FP32 arithmetic                                  */
+    VX_BF16_F32 = 2   /* operand u and modulus E stored in BF16, FP32 arithmetic/output */
+};
+
+const char* vx_last_error(void);
+int vx_version(void);
+
+/* ---------------------------------------------------------------------------- element (host) */
+
+/* Hex8 element matrix (24x24, row-major, native node order) of an isotropic hx*hy*hz brick with
+ * unit Young's modulus, 2x2x2 Gauss quadrature.
+ * Replaces: code/hex_modal/modal.py:19-40 quadrature(lengths, nu). */
+int vx_element_matrix(double hx, double hy, double hz, double nu, double* ke);
+
+/* Cube element of edge h.  Same signature and result as the reference's C oracle
+ * Replaces: experiments/session_a/inputs/reference.cc:12-15 element(h, nu, ke). */
+int vx_element(double h, double nu, double* ke);
+
+/* Parity blocks (8 x 3 x 3 = 72 doubles, row-major per block) of T ke T^T / 64 and the relative
+ * norm of what the block model discards; returns VX_ERR_UNSUPPORTED if it exceeds 2e-14.
+ * Replaces: code/hex_modal/modal.py:55-77 Modal(ke).blocks / .discarded_relative. */
+int vx_parity_blocks(const double* ke, double* blocks, double* discarded_relative);
+
+/* ---------------------------------------------------------------------------- operator */
+
+/* y = K(E) u on the author layout, computed in the parity form with no atomics (deterministic).
+ * `blocks` is a HOST pointer to the 72 parity coefficients (vx_parity_blocks); the kernel carries
+ * them in its parameter (constant) bank.  Overwrites y (the reference kernel accumulated into a
+ * caller-zeroed y; the result is the same).
+ * Replaces: code/hex_modal_cuda/cuda.py:18-21 modal8(blocks, E, u, y, nx, ny, nz) and the
+ * session-I variant experiments/session_i/dependencies/cuda.py:83-110 modal8_muladd. */
+int vx_modal8(const double* blocks, const double* E, const double* u, double* y,
+              int nx, int ny, int nz, cudaStream_t stream);
+
+/* General operator application on the author layout.
+ *   prec      VX_F64 (E,u,y double), VX_F32 (float), VX_BF16_F32 (E,u bf16; y float)
+ *   node_mask NULL: y = K u (the reference's raw(u, E), src/voxel_mg.py:50-53)
+ *             else: y = M K (M u) + (I - M) u (src/voxel_mg.py:129-130 Level.apply)
+ * Replaces: src/voxel_mg.py:41-58 NumpyProduct.raw; experiments/session_a/donor/src/gpu_fem/
+ * cuda_operators.py:658-699 OperatorSuite.matvec_full (node_fp64/node_fp32/fused paths). */
+int vx_matvec(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+              const void* u, void* y, const uint8_t* node_mask, cudaStream_t stream);
+
+/* Reference-style dense node-owned gather (24x24 rows, FP64/FP32), kept as an independent
+ * control path for testing.  Replaces: cuda_operators.py:204-285 node_matvec_fp64/fp32. */
+int vx_matvec_dense(int prec, int nx, int ny, int nz, const double* ke, const void* E,
+                    const void* u, void* y, cudaStream_t stream);
+
+/* Jacobi diagonal of K(E): diag, or with `inverse` != 0 the smoother's inverse diagonal
+ * 1/diag on free DOFs and 1 on fixed DOFs (node_mask may be NULL).  prec VX_F64 or VX_F32
+ * (E and d of that type).  `ke` is a HOST pointer to the 24x24 element matrix.
+ * Replaces: src/voxel_mg.py:55-58 NumpyProduct.diagonal, :126-127 Level.inv_diag;
+ * cuda_operators.py:371-424 jacobi_diag_fp64/fp32. */
+int vx_diagonal(int prec, int nx, int ny, int nz, const double* ke, const void* E,
+                const uint8_t* node_mask, int inverse, void* d, cudaStream_t stream);
+
+/* Element energy ce_e = u_e^T ke u_e (FP64), the SIMP sensitivity kernel.  With `rho` non-NULL
+ * it also writes dc_e = -penal * rho_e^(penal-1) * (emax - emin) * ce_e to `dc` (may be NULL).
+ * Replaces: cuda_operators.py:304-358 elem_compliance_fp64; reference.cc:31-35 (ce);
+ * code/hex_modal/modal.py:89-98 product() gradient. */
+int vx_element_energy(int nx, int ny, int nz, const double* ke, const double* u, double* ce,
+                      const double* rho, double emin, double emax, double penal, double* dc,
+                      cudaStream_t stream);
+
+/* The reference C product on the device, natural layout, same argument meaning:
+ *   E = emin + (emax-emin) rho^penal; y = M K (M u) + (I-M) u; ce_e = (Mu)_e^T ke (Mu)_e;
+ *   diag = diag K on free DOFs, 1 on fixed.  mask: 3N doubles, non-zero = free.
+ * Any of y, ce, diag may be NULL to skip it.
+ * Replaces: experiments/session_a/inputs/reference.cc:16-39 product(). */
+int vx_product(int nx, int ny, int nz, const double* rho, const double* u, const double* ke,
+               const double* mask, double emin, double emax, double penal,
+               double* y, double* ce, double* diag, cudaStream_t stream);
+
+/* SIMP modulus E = emin + (emax - emin) rho^penal, written in `prec` (VX_F64/VX_F32/VX_BF16_F32:
+ * bf16 E).  Replaces: reference.cc:25; experiments/session_i/run_gpu.py:128. */
+int vx_simp_modulus(int prec, int64_t n, const double* rho, double emin, double emax, double penal,
+                    void* E, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------- multigrid */
+
+/* Fused damped-Jacobi sweep: x_out = x + omega * inv_diag * (r - A x), A = M K M + (I-M).
+ * x_out may not alias x.  All vectors of `prec` (VX_BF16_F32: x in bf16 as the operand AND
+ * written rounded to bf16, r/inv_diag/x_out float); E of the operator's storage type.
+ * Replaces one smoothing step of src/voxel_mg.py:161-175 vcycle. */
+int vx_jacobi_sweep(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                    const uint8_t* node_mask, const void* x, const void* r, const void* inv_diag,
+                    double omega, void* x_out, cudaStream_t stream);
+
+/* Fused masked residual: res = (r - A x) * M.  Replaces src/voxel_mg.py:168. */
+int vx_residual(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                const uint8_t* node_mask, const void* x, const void* r, void* res,
+                cudaStream_t stream);
+
+/* Restriction R = P^T (27-point, separable trilinear weights) onto the coarse grid of
+ * fine (nx,ny,nz) (all even), times the coarse node mask.  prec VX_F64/VX_F32.
+ * Replaces: src/voxel_mg.py:83-89,100-105 restrict (+ the coarse mask of :169). */
+int vx_restrict(int prec, int nx, int ny, int nz, const void* fine, const uint8_t* coarse_mask,
+                void* coarse, cudaStream_t stream);
+
+/* x += (P ec) * M on the fine grid (nx,ny,nz) from coarse (nx/2,ny/2,nz/2).
+ * Replaces: src/voxel_mg.py:74-80,92-97 prolong (+ the add and mask of :171). */
+int vx_prolong_add(int prec, int nx, int ny, int nz, const void* coarse, const uint8_t* fine_mask,
+                   void* x, cudaStream_t stream);
+
+/* Coarse modulus (2x2x2 mean) and injected node mask of the fine grid (nx,ny,nz), all even.
+ * E in `prec` storage (VX_BF16_F32: bf16).  Replaces src/voxel_mg.py:108-116. */
+int vx_coarsen_modulus(int prec, int nx, int ny, int nz, const void* E_fine, void* E_coarse,
+                       cudaStream_t stream);
+int vx_coarsen_mask(int nx, int ny, int nz, const uint8_t* mask_fine, uint8_t* mask_coarse,
+                    cudaStream_t stream);
+
+/* Dense constrained coarse matrix A = M K M + (I - M), n x n row-major FP64 with n = 3 * nodes;
+ * deterministic (no atomics).  `ke` is a HOST pointer.  Replaces src/voxel_mg.py:61-70. */
+int vx_assemble_dense(int nx, int ny, int nz, const double* ke, const double* E,
+                      const uint8_t* node_mask, double* A, cudaStream_t stream);
+
+/* Dense symmetric coarse solve z = (Ainv r) * M with a precomputed FP64 inverse (n x n), r and z
+ * in `prec` (accumulation in FP64).  Replaces src/voxel_mg.py:152-159 coarse_solve + :163. */
+int vx_coarse_apply(int prec, int n, const double* Ainv, const void* r, const uint8_t* node_mask,
+                    void* z, cudaStream_t stream);
+
+/* Node masks <-> the reference's 0/1 DOF masks (double, 3 per node, author layout). */
+int vx_mask_from_dofs(int64_t nodes, const double* dof_mask, uint8_t* node_mask, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------- CG vector kernels */
+
+/* Number of doubles the `partials` scratch of the reducing kernels needs for vectors of length n
+ * (per reduction slot; kernels reducing k quantities need k times this). */
+int64_t vx_partials_size(int64_t n);
+
+/* Deterministic dot products (fixed reduction order; bitwise reproducible run to run):
+ * out[k] (device double) = sum_i a_k[i] * b_k[i] for k < count (count <= 3), in FP64, vectors
+ * of `prec` (VX_F64 or VX_F32).  `partials` holds count * vx_partials_size(n) doubles.
+ * Replaces the `@` / linalg.norm reductions of src/voxel_mg.py:192-211 and donor simp_r2.py. */
+int vx_dots(int prec, int64_t n, int count, const void* const* a, const void* const* b,
+            double* partials, double* out, cudaStream_t stream);
+
+/* Fused y := alpha * x + beta * y (FP64 scalars read from DEVICE memory if `dev_scalars` != 0,
+ * else taken from alpha/beta) -- see vx_axpby_dev for the device-scalar form. */
+int vx_axpby(int prec, int64_t n, double alpha, const void* x, double beta, void* y, cudaStream_t stream);
+
+/* Cast between storage precisions (VX_F64 <-> VX_F32 <-> bf16), optional scale (dst = scale*src). */
+int vx_cast(int64_t n, int src_prec, const void* src, int dst_prec, void* dst, double scale,
+            cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VOXEL_B200_H */

@@ -1,0 +1,96 @@
+"""ctypes binding of libvoxel_b200.so (the C ABI declared in include/voxel_b200.h).
+
+There is no fallback: if the library is missing or a call fails, an exception is raised.
+Status codes map to Python exceptions in the reference's style: invalid shapes/arguments and
+elements outside the parity-block model raise ValueError (as the reference's Modal does,
+code/hex_modal/modal.py:65-66), CUDA failures raise RuntimeError.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_double, c_int, c_int64, c_void_p, c_char_p, c_uint8
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libvoxel_b200.so"
+
+VX_OK, VX_ERR_INVALID_ARGUMENT, VX_ERR_NULL_POINTER, VX_ERR_ALIGNMENT = 0, 1, 2, 3
+VX_ERR_LAUNCH, VX_ERR_UNSUPPORTED, VX_ERR_TIMEOUT, VX_ERR_CUDA = 4, 5, 6, 7
+VX_F64, VX_F32, VX_BF16_F32 = 0, 1, 2
+
+_P = c_void_p          # device or host pointer
+_D = POINTER(c_double)  # host double array
+
+# name -> (restype, argtypes); every entry point of include/voxel_b200.h
+SIGNATURES = {
+    "vx_last_error": (c_char_p, []),
+    "vx_version": (c_int, []),
+    "vx_element_matrix": (c_int, [c_double, c_double, c_double, c_double, _D]),
+    "vx_element": (c_int, [c_double, c_double, _D]),
+    "vx_parity_blocks": (c_int, [_D, _D, _D]),
+    "vx_modal8": (c_int, [_D, _P, _P, _P, c_int, c_int, c_int, _P]),
+    "vx_matvec": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P]),
+    "vx_matvec_dense": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P, _P]),
+    "vx_diagonal": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, c_int, _P, _P]),
+    "vx_element_energy": (c_int, [c_int, c_int, c_int, _D, _P, _P, _P, c_double, c_double, c_double, _P, _P]),
+    "vx_product": (c_int, [c_int, c_int, c_int, _P, _P, _D, _P, c_double, c_double, c_double, _P, _P, _P, _P]),
+    "vx_simp_modulus": (c_int, [c_int, c_int64, _P, c_double, c_double, c_double, _P, _P]),
+    "vx_jacobi_sweep": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, c_double, _P, _P]),
+    "vx_residual": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P]),
+    "vx_operator_partials": (c_int64, [c_int, c_int, c_int]),
+    "vx_apply_dot": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P]),
+    "vx_true_residual": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
+    "vx_restrict": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P]),
+    "vx_prolong_add": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P]),
+    "vx_coarsen_modulus": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P]),
+    "vx_coarsen_mask": (c_int, [c_int, c_int, c_int, _P, _P, _P]),
+    "vx_assemble_dense": (c_int, [c_int, c_int, c_int, _D, _P, _P, _P, _P]),
+    "vx_coarse_apply": (c_int, [c_int, c_int, _P, _P, _P, _P, _P]),
+    "vx_mask_from_dofs": (c_int, [c_int64, _P, _P, _P]),
+    "vx_partials_size": (c_int64, [c_int64]),
+    "vx_dots": (c_int, [c_int, c_int64, c_int, POINTER(c_void_p), POINTER(c_void_p), _P, _P, _P]),
+    "vx_reduce_partials": (c_int, [c_int64, c_int, _P, _P, _P]),
+    "vx_axpby": (c_int, [c_int, c_int64, c_double, _P, c_double, _P, _P]),
+    "vx_cast": (c_int, [c_int64, c_int, _P, c_int, _P, c_double, _P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library (once) and bind every signature; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"libvoxel_b200.so not found at {LIB_PATH}; build it with "
+                           "`python -c 'import __graft_entry__ as g; g.build()'` (needs nvcc)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().vx_last_error().decode(errors="replace")
+
+
+def check(status: int, what: str = "") -> None:
+    if status == VX_OK:
+        return
+    msg = f"{what}: {last_error()}" if what else last_error()
+    if status in (VX_ERR_INVALID_ARGUMENT, VX_ERR_UNSUPPORTED, VX_ERR_NULL_POINTER, VX_ERR_ALIGNMENT):
+        raise ValueError(msg)
+    if status == VX_ERR_TIMEOUT:
+        raise TimeoutError(msg)
+    raise RuntimeError(msg)
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args), name)
+
+
+def dptr(a) -> _D:
+    """Host double* of a C-contiguous float64 numpy array."""
+    return a.ctypes.data_as(_D)

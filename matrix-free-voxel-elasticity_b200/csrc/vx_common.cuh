@@ -1,0 +1,86 @@
+// Shared definitions for libvoxel_b200: status codes, the thread-local error string, launch checks,
+// storage types and the 45-entry parity-block pattern of an affine brick Hex8 element.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/voxel_b200.h"
+
+namespace vx {
+
+// Last error message of the calling host thread (returned by vx_last_error()).
+void set_error(const char* fmt, ...);
+
+#define VX_CHECK_ARG(cond, code, ...)            \
+    do {                                         \
+        if (!(cond)) {                           \
+            ::vx::set_error(__VA_ARGS__);        \
+            return (code);                       \
+        }                                        \
+    } while (0)
+
+#define VX_CHECK_LAUNCH(what)                                                              \
+    do {                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess) {                                                           \
+            ::vx::set_error("%s: launch failed: %s", (what), cudaGetErrorString(e_));      \
+            return VX_ERR_LAUNCH;                                                          \
+        }                                                                                  \
+    } while (0)
+
+inline bool aligned(const void* p, size_t bytes) { return (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
+
+// Grid extents: element grid (nx, ny, nz); nodes (nx+1)(ny+1)(nz+1); author layout, z fastest.
+struct Grid {
+    int nx, ny, nz;
+    __host__ __device__ int64_t nodes() const { return int64_t(nx + 1) * (ny + 1) * (nz + 1); }
+    __host__ __device__ int64_t elems() const { return int64_t(nx) * ny * nz; }
+    __host__ __device__ int64_t node(int ix, int iy, int iz) const {
+        return (int64_t(ix) * (ny + 1) + iy) * (nz + 1) + iz;
+    }
+    __host__ __device__ int64_t elem(int ex, int ey, int ez) const {
+        return (int64_t(ex) * ny + ey) * nz + ez;
+    }
+};
+
+int check_grid(int nx, int ny, int nz);
+
+// ---------------------------------------------------------------------------- storage conversion
+template <typename S> struct Storage;
+template <> struct Storage<double> {
+    __device__ static double load(const double* p) { return *p; }
+    __device__ static void store(double* p, double v) { *p = v; }
+};
+template <> struct Storage<float> {
+    __device__ static float load(const float* p) { return *p; }
+    __device__ static void store(float* p, float v) { *p = v; }
+};
+template <> struct Storage<__nv_bfloat16> {
+    __device__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ static void store(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+// ---------------------------------------------------------------------------- parity blocks
+// The parity (Walsh-Hadamard) form of an affine-brick Hex8 element matrix: T ke T^T / 64 is block
+// diagonal with 8 groups of 3x3; group g couples component x at parity g^1, y at g^2, z at g^4
+// (parity p = px + 2 py + 4 pz).  Translations (parity 0) have zero rows, so 45 of the 72 entries
+// are structurally non-zero.  The kernels take the 72 coefficients by value and use only these 45.
+struct Blocks {
+    double c[72];   // c[9*g + 3*a + b] = block g, row a (component a), column b
+};
+template <typename T> struct BlocksT { T c[72]; };
+
+// true if entry (g, a, b) of the parity blocks is structurally non-zero for a brick element
+__host__ __device__ constexpr bool parity_nonzero(int g, int a, int b) {
+    // parity of component a in group g is g ^ (1 << a); a zero parity (translation) has no stiffness
+    return ((g ^ (1 << a)) != 0) && ((g ^ (1 << b)) != 0) &&
+           // cross-coupling pattern (a != b): measured structure of T ke T^T for a brick
+           (a == b || !((g == 3 && (a == 2 || b == 2)) || (g == 5 && (a == 1 || b == 1)) ||
+                        (g == 6 && (a == 0 || b == 0))));
+}
+
+}  // namespace vx

@@ -1,0 +1,268 @@
+// Multigrid kernels of the rediscretised voxel hierarchy: trilinear restriction / prolongation,
+// modulus and mask coarsening, dense coarse assembly and the dense coarse solve.
+// The transfers evaluate the separable per-axis passes in the reference's order (x, then y,
+// then z; restriction adds the right neighbour before the left), so FP64 results agree with the
+// reference's NumPy transfers to the last bit or within an ulp.
+#include "vx_common.cuh"
+
+namespace vx {
+
+__device__ __forceinline__ void node_coords(const Grid& g, int64_t n, int& ix, int& iy, int& iz) {
+    iz = int(n % (g.nz + 1));
+    iy = int((n / (g.nz + 1)) % (g.ny + 1));
+    ix = int(n / (int64_t(g.nz + 1) * (g.ny + 1)));
+}
+
+// coarse node (I,J,K) of fine grid f: rc = sum w(a) w(b) w(d) f(2I+a, 2J+b, 2K+d), w(0)=1, w(+-1)=1/2
+template <typename T>
+__global__ void restrict_kernel(Grid f, Grid c, const T* __restrict__ fine, const uint8_t* __restrict__ cmask,
+                                T* __restrict__ coarse) {
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= c.nodes()) return;
+    int I, J, K;
+    node_coords(c, n, I, J, K);
+    const unsigned bits = cmask ? unsigned(cmask[n]) : 7u;
+    for (int comp = 0; comp < 3; ++comp) {
+        T ty[3][3];   // after the x pass, at fine (y = 2J + b - 1, z = 2K + d - 1)
+        for (int b = 0; b < 3; ++b)
+            for (int d = 0; d < 3; ++d) {
+                const int fy = 2 * J + b - 1, fz = 2 * K + d - 1;
+                T v = T(0);
+                if (fy >= 0 && fy <= f.ny && fz >= 0 && fz <= f.nz) {
+                    v = fine[3 * f.node(2 * I, fy, fz) + comp];
+                    if (2 * I + 1 <= f.nx) v = v + T(0.5) * fine[3 * f.node(2 * I + 1, fy, fz) + comp];
+                    if (I >= 1) v = v + T(0.5) * fine[3 * f.node(2 * I - 1, fy, fz) + comp];
+                }
+                ty[b][d] = v;
+            }
+        T tz[3];
+        for (int d = 0; d < 3; ++d) {
+            T v = ty[1][d];
+            if (2 * J + 1 <= f.ny) v = v + T(0.5) * ty[2][d];
+            if (J >= 1) v = v + T(0.5) * ty[0][d];
+            tz[d] = v;
+        }
+        T v = tz[1];
+        if (2 * K + 1 <= f.nz) v = v + T(0.5) * tz[2];
+        if (K >= 1) v = v + T(0.5) * tz[0];
+        coarse[3 * n + comp] = ((bits >> comp) & 1u) ? v : T(0);
+    }
+}
+
+// x(i,j,k) += (P ec)(i,j,k) * mask; P is the separable trilinear interpolation
+template <typename T>
+__global__ void prolong_add_kernel(Grid f, Grid c, const T* __restrict__ coarse, const uint8_t* __restrict__ fmask,
+                                   T* __restrict__ x) {
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= f.nodes()) return;
+    int i, j, k;
+    node_coords(f, n, i, j, k);
+    const unsigned bits = fmask ? unsigned(fmask[n]) : 7u;
+    const int I0 = i >> 1, J0 = j >> 1, K0 = k >> 1;
+    const bool ox = i & 1, oy = j & 1, oz = k & 1;
+    for (int comp = 0; comp < 3; ++comp) {
+        T py[2];
+        for (int d = 0; d <= int(oz); ++d) {
+            T px[2];
+            for (int b = 0; b <= int(oy); ++b) {
+                const int64_t a0 = 3 * c.node(I0, J0 + b, K0 + d) + comp;
+                px[b] = ox ? T(0.5) * (coarse[a0] + coarse[a0 + 3 * int64_t(c.ny + 1) * (c.nz + 1)]) : coarse[a0];
+            }
+            py[d] = oy ? T(0.5) * (px[0] + px[1]) : px[0];
+        }
+        const T v = oz ? T(0.5) * (py[0] + py[1]) : py[0];
+        if ((bits >> comp) & 1u) x[3 * n + comp] = x[3 * n + comp] + v;
+    }
+}
+
+template <typename S>
+__global__ void coarsen_modulus_kernel(Grid f, Grid c, const S* __restrict__ Ef, S* __restrict__ Ec) {
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= c.elems()) return;
+    const int ez = int(e % c.nz), ey = int((e / c.nz) % c.ny), ex = int(e / (int64_t(c.nz) * c.ny));
+    double s = 0.0;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int d = 0; d < 2; ++d) s += double(Storage<S>::load(Ef + f.elem(2 * ex + a, 2 * ey + b, 2 * ez + d)));
+    Storage<S>::store(Ec + e, decltype(Storage<S>::load(Ef))(s * 0.125));
+}
+
+__global__ void coarsen_mask_kernel(Grid f, Grid c, const uint8_t* __restrict__ mf, uint8_t* __restrict__ mc) {
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= c.nodes()) return;
+    int I, J, K;
+    node_coords(c, n, I, J, K);
+    mc[n] = mf[f.node(2 * I, 2 * J, 2 * K)];
+}
+
+struct Ke576 { double k[576]; };
+
+// one thread per (row DOF, neighbour offset, column component); A is zeroed beforehand
+__global__ void assemble_dense_kernel(Grid g, const __grid_constant__ Ke576 ke, const double* __restrict__ E,
+                                      const uint8_t* __restrict__ mask, double* __restrict__ A) {
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t nn = g.nodes();
+    if (t >= nn * 3 * 81) return;
+    const int64_t row = t / 81;
+    const int rem = int(t % 81);
+    const int off = rem / 3, cd = rem % 3;
+    const int64_t nr = row / 3;
+    const int cr = int(row % 3);
+    int ix, iy, iz;
+    node_coords(g, nr, ix, iy, iz);
+    const int ox = off % 3 - 1, oy = (off / 3) % 3 - 1, oz = off / 9 - 1;
+    const int mx = ix + ox, my = iy + oy, mz = iz + oz;
+    if (mx < 0 || mx > g.nx || my < 0 || my > g.ny || mz < 0 || mz > g.nz) return;
+    constexpr int nat[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+    double v = 0.0;
+    for (int bx = 0; bx < 2; ++bx) for (int by = 0; by < 2; ++by) for (int bz = 0; bz < 2; ++bz) {
+        const int ex = ix - 1 + bx, ey = iy - 1 + by, ez = iz - 1 + bz;   // element containing the row node
+        if (ex < 0 || ex >= g.nx || ey < 0 || ey >= g.ny || ez < 0 || ez >= g.nz) continue;
+        const int qx = mx - ex, qy = my - ey, qz = mz - ez;              // column node's offset in it
+        if (qx < 0 || qx > 1 || qy < 0 || qy > 1 || qz < 0 || qz > 1) continue;
+        const int li = nat[(1 - bx) + 2 * (1 - by) + 4 * (1 - bz)];
+        const int lj = nat[qx + 2 * qy + 4 * qz];
+        v += E[g.elem(ex, ey, ez)] * ke.k[(3 * li + cr) * 24 + 3 * lj + cd];
+    }
+    const int64_t col = 3 * g.node(mx, my, mz) + cd;
+    const double mr = mask ? double((mask[nr] >> cr) & 1u) : 1.0;
+    const double mcv = mask ? double((mask[col / 3] >> cd) & 1u) : 1.0;
+    double out = mr * v * mcv;
+    if (col == row) out += 1.0 - mr;
+    A[row * (nn * 3) + col] = out;
+}
+
+// z = (Ainv r) * mask, one warp per row, FP64 accumulation
+template <typename T>
+__global__ void coarse_apply_kernel(int n, const double* __restrict__ Ainv, const T* __restrict__ r,
+                                    const uint8_t* __restrict__ mask, T* __restrict__ z) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double* row = Ainv + int64_t(warp) * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s = fma(row[j], double(r[j]), s);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const bool fr = mask ? ((mask[warp / 3] >> (warp % 3)) & 1u) : true;
+        z[warp] = fr ? T(s) : T(0);
+    }
+}
+
+__global__ void mask_from_dofs_kernel(int64_t nodes, const double* __restrict__ m, uint8_t* __restrict__ out) {
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= nodes) return;
+    out[n] = uint8_t((m[3 * n] != 0.0) | ((m[3 * n + 1] != 0.0) << 1) | ((m[3 * n + 2] != 0.0) << 2));
+}
+
+inline unsigned blocks_for(int64_t n, int t) { return unsigned((n + t - 1) / t); }
+
+int check_even(int nx, int ny, int nz, const char* what) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    if ((nx | ny | nz) & 1) {
+        set_error("%s: fine grid (%d, %d, %d) must have even extents", what, nx, ny, nz);
+        return VX_ERR_INVALID_ARGUMENT;
+    }
+    return VX_OK;
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" int vx_restrict(int prec, int nx, int ny, int nz, const void* fine, const uint8_t* coarse_mask,
+                           void* coarse, cudaStream_t stream) {
+    int st = check_even(nx, ny, nz, "vx_restrict");
+    if (st) return st;
+    VX_CHECK_ARG(fine && coarse, VX_ERR_NULL_POINTER, "vx_restrict: NULL pointer");
+    Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
+    if (prec == VX_F64)
+        restrict_kernel<double><<<blocks_for(c.nodes(), 128), 128, 0, stream>>>(f, c, (const double*)fine, coarse_mask, (double*)coarse);
+    else if (prec == VX_F32)
+        restrict_kernel<float><<<blocks_for(c.nodes(), 128), 128, 0, stream>>>(f, c, (const float*)fine, coarse_mask, (float*)coarse);
+    else { set_error("vx_restrict: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_restrict");
+    return VX_OK;
+}
+
+extern "C" int vx_prolong_add(int prec, int nx, int ny, int nz, const void* coarse, const uint8_t* fine_mask,
+                              void* x, cudaStream_t stream) {
+    int st = check_even(nx, ny, nz, "vx_prolong_add");
+    if (st) return st;
+    VX_CHECK_ARG(coarse && x, VX_ERR_NULL_POINTER, "vx_prolong_add: NULL pointer");
+    Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
+    if (prec == VX_F64)
+        prolong_add_kernel<double><<<blocks_for(f.nodes(), 256), 256, 0, stream>>>(f, c, (const double*)coarse, fine_mask, (double*)x);
+    else if (prec == VX_F32)
+        prolong_add_kernel<float><<<blocks_for(f.nodes(), 256), 256, 0, stream>>>(f, c, (const float*)coarse, fine_mask, (float*)x);
+    else { set_error("vx_prolong_add: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_prolong_add");
+    return VX_OK;
+}
+
+extern "C" int vx_coarsen_modulus(int prec, int nx, int ny, int nz, const void* E_fine, void* E_coarse,
+                                  cudaStream_t stream) {
+    int st = check_even(nx, ny, nz, "vx_coarsen_modulus");
+    if (st) return st;
+    VX_CHECK_ARG(E_fine && E_coarse, VX_ERR_NULL_POINTER, "vx_coarsen_modulus: NULL pointer");
+    Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
+    const unsigned gb = blocks_for(c.elems(), 256);
+    if (prec == VX_F64) coarsen_modulus_kernel<double><<<gb, 256, 0, stream>>>(f, c, (const double*)E_fine, (double*)E_coarse);
+    else if (prec == VX_F32) coarsen_modulus_kernel<float><<<gb, 256, 0, stream>>>(f, c, (const float*)E_fine, (float*)E_coarse);
+    else if (prec == VX_BF16_F32)
+        coarsen_modulus_kernel<__nv_bfloat16><<<gb, 256, 0, stream>>>(f, c, (const __nv_bfloat16*)E_fine, (__nv_bfloat16*)E_coarse);
+    else { set_error("vx_coarsen_modulus: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_coarsen_modulus");
+    return VX_OK;
+}
+
+extern "C" int vx_coarsen_mask(int nx, int ny, int nz, const uint8_t* mask_fine, uint8_t* mask_coarse,
+                               cudaStream_t stream) {
+    int st = check_even(nx, ny, nz, "vx_coarsen_mask");
+    if (st) return st;
+    VX_CHECK_ARG(mask_fine && mask_coarse, VX_ERR_NULL_POINTER, "vx_coarsen_mask: NULL pointer");
+    Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
+    coarsen_mask_kernel<<<blocks_for(c.nodes(), 256), 256, 0, stream>>>(f, c, mask_fine, mask_coarse);
+    VX_CHECK_LAUNCH("vx_coarsen_mask");
+    return VX_OK;
+}
+
+extern "C" int vx_assemble_dense(int nx, int ny, int nz, const double* ke, const double* E,
+                                 const uint8_t* node_mask, double* A, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(ke && E && A, VX_ERR_NULL_POINTER, "vx_assemble_dense: NULL pointer");
+    Grid g{nx, ny, nz};
+    const int64_t n = 3 * g.nodes();
+    VX_CHECK_ARG(n <= 65536, VX_ERR_INVALID_ARGUMENT, "vx_assemble_dense: %lld DOFs is too many for a dense matrix",
+                 (long long)n);
+    Ke576 k;
+    for (int i = 0; i < 576; ++i) k.k[i] = ke[i];
+    cudaError_t e = cudaMemsetAsync(A, 0, size_t(n) * size_t(n) * sizeof(double), stream);
+    if (e != cudaSuccess) { set_error("vx_assemble_dense: memset: %s", cudaGetErrorString(e)); return VX_ERR_CUDA; }
+    assemble_dense_kernel<<<blocks_for(g.nodes() * 243, 256), 256, 0, stream>>>(g, k, E, node_mask, A);
+    VX_CHECK_LAUNCH("vx_assemble_dense");
+    return VX_OK;
+}
+
+extern "C" int vx_coarse_apply(int prec, int n, const double* Ainv, const void* r, const uint8_t* node_mask,
+                               void* z, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply: n must be positive");
+    VX_CHECK_ARG(Ainv && r && z, VX_ERR_NULL_POINTER, "vx_coarse_apply: NULL pointer");
+    const unsigned gb = blocks_for(int64_t(n) * 32, 256);
+    if (prec == VX_F64) coarse_apply_kernel<double><<<gb, 256, 0, stream>>>(n, Ainv, (const double*)r, node_mask, (double*)z);
+    else if (prec == VX_F32) coarse_apply_kernel<float><<<gb, 256, 0, stream>>>(n, Ainv, (const float*)r, node_mask, (float*)z);
+    else { set_error("vx_coarse_apply: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_coarse_apply");
+    return VX_OK;
+}
+
+extern "C" int vx_mask_from_dofs(int64_t nodes, const double* dof_mask, uint8_t* node_mask, cudaStream_t stream) {
+    VX_CHECK_ARG(nodes > 0, VX_ERR_INVALID_ARGUMENT, "vx_mask_from_dofs: nodes must be positive");
+    VX_CHECK_ARG(dof_mask && node_mask, VX_ERR_NULL_POINTER, "vx_mask_from_dofs: NULL pointer");
+    mask_from_dofs_kernel<<<blocks_for(nodes, 256), 256, 0, stream>>>(nodes, dof_mask, node_mask);
+    VX_CHECK_LAUNCH("vx_mask_from_dofs");
+    return VX_OK;
+}

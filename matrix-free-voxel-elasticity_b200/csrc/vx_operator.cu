@@ -1,0 +1,665 @@
+// Matrix-free Hex8 voxel operator kernels (author layout, z fastest).
+//
+// parity_stream: y = K(E) u in the parity (Walsh-Hadamard) form, node-owned and atomic-free.
+//   A CTA is NW warps x 32 lanes; lane <-> z node column, warp <-> y node row, and the CTA marches
+//   along x (the slowest axis) over a chunk of node planes.  Thread (row, lane) holds node column
+//   (iy, iz) = (y0 - 1 + row, z0 - 1 + lane) and element (ex, iy, iz).  The 2x2x2 transform is done
+//   separably and SHARED between neighbouring elements:
+//     X stage  (per x-edge, in registers: previous plane carried)      2 adds / component
+//     Y stage  (per xy-face, neighbour row through shared memory)      4 adds
+//     Z stage  (per element, neighbour lane through a shuffle, E folded in)
+//     parity-block product (45 structurally non-zero coefficients, constant bank)
+//     inverse Z / Y / X with the face, edge and node accumulations done the same way.
+//   Rows 0 / NW-1 and lanes 0 / 31 are halo: a CTA owns nodes rows 1..NW-2, lanes 1..30, and
+//   recomputes the elements of its one-node halo, so no output needs atomics and results are
+//   bitwise deterministic.  Elements outside the grid get modulus 0, which removes every branch
+//   on the grid boundary.
+// dense_gather: the reference's node-owned dense 24x24 mapping (independent control path).
+// diag / energy / coarse-grid helpers.
+#include "vx_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace vx {
+
+constexpr int NW = 16;          // warps per CTA (node rows incl. 2 halo rows)
+constexpr int TYR = NW - 2;     // owned node rows per CTA
+constexpr int TZ = 30;          // owned node columns per CTA
+constexpr int CX = 32;          // owned node planes per CTA (x chunk)
+
+enum Epi { EPI_RAW = 0, EPI_JACOBI = 1, EPI_RESIDUAL = 2, EPI_TRUE_RES = 3, EPI_APPLY_DOT = 4 };
+enum MaskKind { MASK_NONE = 0, MASK_NODE = 1, MASK_DOF = 2 };
+
+template <typename TC, typename TU, typename TE, typename TY>
+struct OpArgs {
+    Grid g;
+    const TU* u;              // operand (smoother: current iterate x)
+    const TE* E;              // element modulus (or rho when SIMP)
+    TY* y;                    // output
+    const uint8_t* node_mask; // MASK_NODE: bit c set <=> DOF c free
+    const double* dof_mask;   // MASK_DOF: 3 doubles per node, non-zero = free
+    const TY* r;              // JACOBI / RESIDUAL / TRUE_RES right-hand side
+    const TY* invd;           // JACOBI inverse diagonal
+    TC omega;
+    double* partials;         // TRUE_RES (|res|^2) / APPLY_DOT (p.q): one double per CTA
+    double emin, de, penal;   // SIMP modulus E = emin + de * rho^penal
+    BlocksT<TC> C;
+};
+
+template <typename T>
+__device__ __forceinline__ T shfl_down1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+template <typename T>
+__device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+
+template <typename TC, typename TE, bool SIMP>
+__device__ __forceinline__ TC load_modulus(const TE* E, int64_t e, double emin, double de, double penal) {
+    if constexpr (SIMP) {
+        const double rho = double(Storage<TE>::load(E + e));
+        return TC(emin + de * pow(rho, penal));
+    } else {
+        return TC(Storage<TE>::load(E + e));
+    }
+}
+
+// Block reduce of one double per thread; thread 0 writes partials[block].
+template <int NT>
+__device__ __forceinline__ void block_sum_store(double v, double* out) {
+    __shared__ double red[NT / 32];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double s = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) *out = s;
+    }
+}
+
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP>
+__global__ void __launch_bounds__(NW * 32, 1)
+parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
+    const int lane = threadIdx.x & 31;
+    const int row = threadIdx.x >> 5;
+    const Grid g = a.g;
+    const int iz = blockIdx.x * TZ - 1 + lane;
+    const int iy = blockIdx.y * TYR - 1 + row;
+    const int x0 = blockIdx.z * CX;
+    const int x1 = min(x0 + CX, g.nx + 1);                 // owned node planes [x0, x1)
+    const bool in_node = iy >= 0 && iy <= g.ny && iz >= 0 && iz <= g.nz;
+    const bool owner = in_node && lane >= 1 && lane <= TZ && row >= 1 && row <= TYR;
+    const bool elem_ok = iy >= 0 && iy < g.ny && iz >= 0 && iz < g.nz && lane < 31 && row < NW - 1;
+    const int rown = row + 1 < NW ? row + 1 : row;        // clamped neighbour rows (halo rows only)
+    const int rowp = row > 0 ? row - 1 : 0;
+
+    // X-stage results for the row below, then inverse-Y contributions for the row above
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TC* xs = reinterpret_cast<TC*>(smem_raw);
+    TC* hs = xs + NW * 6 * 32;
+#define XS(r, k) xs[((r) * 6 + (k)) * 32 + lane]
+#define HS(r, k) hs[((r) * 6 + (k)) * 32 + lane]
+
+    const int64_t plane_nodes = int64_t(g.ny + 1) * (g.nz + 1);
+    const int64_t col = int64_t(iy) * (g.nz + 1) + iz;     // node offset within a plane
+    const int64_t ecol = int64_t(iy) * g.nz + iz;          // element offset within a plane
+    const int64_t plane_elems = int64_t(g.ny) * g.nz;
+
+    auto load_node = [&](int ix, TC* uu, TC* um, unsigned& bits) {
+        uu[0] = uu[1] = uu[2] = TC(0);
+        bits = 7u;
+        if (in_node && ix >= 0 && ix <= g.nx) {
+            const int64_t n = int64_t(ix) * plane_nodes + col;
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) uu[c] = TC(Storage<TU>::load(a.u + 3 * n + (REV ? 2 - c : c)));
+            if constexpr (MASK == MASK_NODE) bits = a.node_mask ? unsigned(a.node_mask[n]) : 7u;
+            if constexpr (MASK == MASK_DOF) {
+                bits = 0;
+                #pragma unroll
+                for (int c = 0; c < 3; ++c) bits |= (a.dof_mask[3 * n + (REV ? 2 - c : c)] != 0.0) << c;
+            }
+        }
+        #pragma unroll
+        for (int c = 0; c < 3; ++c) um[c] = ((bits >> c) & 1u) ? uu[c] : TC(0);
+    };
+    auto load_E = [&](int ex) -> TC {
+        if (elem_ok && ex >= 0 && ex < g.nx)
+            return load_modulus<TC, TE, SIMP>(a.E, int64_t(ex) * plane_elems + ecol, a.emin, a.de, a.penal);
+        return TC(0);
+    };
+
+    TC up[3], uprev_raw[3], carry[3] = {TC(0), TC(0), TC(0)};
+    unsigned bits_prev = 7u;
+    // prefetched next plane
+    TC un_raw[3], un[3];
+    unsigned bits_n;
+    load_node(x0 - 1, un_raw, un, bits_n);
+    TC En = load_E(x0 - 1);
+    double acc = 0.0;
+
+    for (int ix = x0 - 1; ix <= x1; ++ix) {
+        TC ucur_raw[3] = {un_raw[0], un_raw[1], un_raw[2]};
+        TC ucur[3] = {un[0], un[1], un[2]};
+        const unsigned bits_cur = bits_n;
+        const TC Ee = En;                                   // element plane ex = ix - 1
+        if (ix < x1) {                                      // prefetch plane ix + 1
+            load_node(ix + 1, un_raw, un, bits_n);
+            En = load_E(ix);
+        }
+        // epilogue operands of node plane ix - 1
+        TC rr[3] = {TC(0), TC(0), TC(0)}, dd[3] = {TC(0), TC(0), TC(0)};
+        const bool out_now = owner && ix - 1 >= x0;
+        const int64_t nout = int64_t(ix - 1) * plane_nodes + col;
+        if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
+            if (out_now) {
+                #pragma unroll
+                for (int c = 0; c < 3; ++c) rr[c] = TC(Storage<TY>::load(a.r + 3 * nout + (REV ? 2 - c : c)));
+                if constexpr (EPI == EPI_JACOBI) {
+                    #pragma unroll
+                    for (int c = 0; c < 3; ++c) dd[c] = TC(Storage<TY>::load(a.invd + 3 * nout + (REV ? 2 - c : c)));
+                }
+            }
+        }
+
+        if (ix >= x0) {
+            // ---- X stage: edge (ix-1 -> ix) at (iy, iz)
+            TC X0[3], X1[3];
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) { X0[c] = up[c] + ucur[c]; X1[c] = up[c] - ucur[c]; }
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) { XS(row, c) = X0[c]; XS(row, 3 + c) = X1[c]; }
+            __syncthreads();
+            // ---- Y stage: face (iy -> iy+1); Y[c][px][py]
+            TC Y[3][2][2];
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const TC b0 = XS(rown, c), b1 = XS(rown, 3 + c);
+                Y[c][0][0] = X0[c] + b0; Y[c][0][1] = X0[c] - b0;
+                Y[c][1][0] = X1[c] + b1; Y[c][1][1] = X1[c] - b1;
+            }
+            // ---- Z stage with the modulus folded in: v[c][p], p = px + 2 py + 4 pz (p = 0 unused)
+            TC v[3][8];
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                #pragma unroll
+                for (int px = 0; px < 2; ++px) {
+                    #pragma unroll
+                    for (int py = 0; py < 2; ++py) {
+                        const TC ya = Y[c][px][py];
+                        const TC m = Ee * shfl_down1(ya);
+                        const int p = px + 2 * py;
+                        if (p != 0) v[c][p] = fma(Ee, ya, m);
+                        v[c][p + 4] = fma(Ee, ya, -m);
+                    }
+                }
+                v[c][0] = TC(0);
+            }
+            // ---- parity-block product, in place per group
+            #pragma unroll
+            for (int gi = 0; gi < 8; ++gi) {
+                const int pa[3] = {gi ^ 1, gi ^ 2, gi ^ 4};
+                TC in[3] = {v[0][pa[0]], v[1][pa[1]], v[2][pa[2]]};
+                #pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    if (pa[r] == 0) continue;
+                    TC s = TC(0);
+                    bool first = true;
+                    #pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        if (!parity_nonzero(gi, r, cc)) continue;
+                        const TC coef = a.C.c[9 * gi + 3 * r + cc];
+                        s = first ? coef * in[cc] : fma(coef, in[cc], s);
+                        first = false;
+                    }
+                    v[r][pa[r]] = s;
+                }
+            }
+            // ---- inverse Z: G0 -> face iz (own), G1 -> face iz+1 (lane + 1)
+            TC FY[3][2][2];
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                #pragma unroll
+                for (int px = 0; px < 2; ++px) {
+                    #pragma unroll
+                    for (int py = 0; py < 2; ++py) {
+                        const int p = px + 2 * py;
+                        const TC f0 = v[c][p], f1 = v[c][p + 4];
+                        if (p == 0) {
+                            FY[c][px][py] = f1 - shfl_up1(f1);
+                        } else {
+                            const TC g1 = f0 - f1;
+                            FY[c][px][py] = (f0 + f1) + shfl_up1(g1);
+                        }
+                    }
+                }
+            }
+            // ---- inverse Y: H0 -> edge iy (own), H1 -> edge iy+1 (row + 1)
+            TC H0[3][2];
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                #pragma unroll
+                for (int px = 0; px < 2; ++px) {
+                    H0[c][px] = FY[c][px][0] + FY[c][px][1];
+                    HS(row, 3 * px + c) = FY[c][px][0] - FY[c][px][1];
+                }
+            }
+            __syncthreads();
+            // ---- edge totals and inverse X
+            TC yout[3];
+            #pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const TC fx0 = H0[c][0] + (row > 0 ? HS(rowp, c) : TC(0));
+                const TC fx1 = H0[c][1] + (row > 0 ? HS(rowp, 3 + c) : TC(0));
+                yout[c] = carry[c] + (fx0 + fx1);
+                carry[c] = fx0 - fx1;
+            }
+            // ---- epilogue for node plane ix - 1
+            if (out_now) {
+                TY* yo = a.y + 3 * nout;
+                #pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const bool free_dof = (bits_prev >> c) & 1u;
+                    TC ax;                                   // operator applied (Dirichlet form)
+                    if constexpr (MASK == MASK_NONE) ax = yout[c];
+                    else ax = free_dof ? yout[c] : uprev_raw[c];
+                    TC o;
+                    if constexpr (EPI == EPI_RAW) {
+                        o = ax;
+                    } else if constexpr (EPI == EPI_APPLY_DOT) {
+                        o = ax;
+                        acc += double(uprev_raw[c]) * double(ax);
+                    } else if constexpr (EPI == EPI_JACOBI) {
+                        o = uprev_raw[c] + a.omega * dd[c] * (rr[c] - ax);
+                    } else if constexpr (EPI == EPI_RESIDUAL) {
+                        o = free_dof ? rr[c] - ax : TC(0);
+                    } else {  // EPI_TRUE_RES
+                        o = rr[c] - ax;
+                        acc += double(o) * double(o);
+                    }
+                    Storage<TY>::store(yo + (REV ? 2 - c : c), o);
+                }
+            }
+        }
+        #pragma unroll
+        for (int c = 0; c < 3; ++c) { up[c] = ucur[c]; uprev_raw[c] = ucur_raw[c]; }
+        bits_prev = bits_cur;
+    }
+    if constexpr (EPI == EPI_TRUE_RES || EPI == EPI_APPLY_DOT) {
+        const int64_t bid = (int64_t(blockIdx.z) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        block_sum_store<NW * 32>(acc, a.partials + bid);
+    }
+#undef XS
+#undef HS
+}
+
+inline dim3 stream_grid(const Grid& g) {
+    return dim3((g.nz + 1 + TZ - 1) / TZ, (g.ny + 1 + TYR - 1) / TYR, (g.nx + 1 + CX - 1) / CX);
+}
+
+int64_t stream_ctas(const Grid& g) {
+    dim3 d = stream_grid(g);
+    return int64_t(d.x) * d.y * d.z;
+}
+
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP>
+int launch_stream(const OpArgs<TC, TU, TE, TY>& a, cudaStream_t s, const char* what) {
+    auto kern = parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
+    constexpr size_t smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
+    static bool configured = false;          // once per instantiation (per process)
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) {
+            set_error("%s: cudaFuncSetAttribute: %s", what, cudaGetErrorString(e));
+            return VX_ERR_CUDA;
+        }
+        configured = true;
+    }
+    kern<<<stream_grid(a.g), NW * 32, smem, s>>>(a);
+    VX_CHECK_LAUNCH(what);
+    return VX_OK;
+}
+
+template <typename TC>
+BlocksT<TC> convert_blocks(const double* blocks) {
+    BlocksT<TC> b;
+    for (int i = 0; i < 72; ++i) b.c[i] = TC(blocks[i]);
+    return b;
+}
+
+// ------------------------------------------------------------------------- dense control path
+template <typename T>
+__global__ void dense_gather(Grid g, const T* __restrict__ ke, const T* __restrict__ E,
+                             const T* __restrict__ u, T* __restrict__ y) {
+    __shared__ T K[576];
+    for (int i = threadIdx.x; i < 576; i += blockDim.x) K[i] = ke[i];
+    __syncthreads();
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= g.nodes()) return;
+    const int iz = int(n % (g.nz + 1));
+    const int iy = int((n / (g.nz + 1)) % (g.ny + 1));
+    const int ix = int(n / (int64_t(g.nz + 1) * (g.ny + 1)));
+    // native node index of binary offset (bx, by, bz): 0,1,3,2,4,5,7,6
+    constexpr int nat[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int bx = 0; bx < 2; ++bx) for (int by = 0; by < 2; ++by) for (int bz = 0; bz < 2; ++bz) {
+        const int ex = ix - 1 + bx, ey = iy - 1 + by, ez = iz - 1 + bz;
+        if (ex < 0 || ex >= g.nx || ey < 0 || ey >= g.ny || ez < 0 || ez >= g.nz) continue;
+        const T Ee = E[g.elem(ex, ey, ez)];
+        const int li = nat[(1 - bx) + 2 * (1 - by) + 4 * (1 - bz)];
+        for (int b = 0; b < 8; ++b) {
+            const int m = nat[b];
+            const int64_t nb = g.node(ex + (b & 1), ey + ((b >> 1) & 1), ez + ((b >> 2) & 1));
+            const T u0 = u[3 * nb], u1 = u[3 * nb + 1], u2 = u[3 * nb + 2];
+            for (int c = 0; c < 3; ++c) {
+                const T* kr = K + (3 * li + c) * 24 + 3 * m;
+                acc[c] += Ee * (kr[0] * u0 + kr[1] * u1 + kr[2] * u2);
+            }
+        }
+    }
+    for (int c = 0; c < 3; ++c) y[3 * n + c] = acc[c];
+}
+
+// ------------------------------------------------------------------------- diagonal
+// mode 0: diag K; mode 1: 1/diag on free DOFs, 1 on fixed; mode 2: diag on free DOFs, 1 on fixed.
+template <typename T, bool REV, int MASK, bool SIMP>
+__global__ void diag_kernel(Grid g, BlocksT<T> kd /* c[0..23]: diagonal of ke */, const T* __restrict__ E,
+                            const uint8_t* __restrict__ node_mask, const double* __restrict__ dof_mask,
+                            double emin, double de, double penal, int mode, T* __restrict__ d) {
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= g.nodes()) return;
+    const int iz = int(n % (g.nz + 1));
+    const int iy = int((n / (g.nz + 1)) % (g.ny + 1));
+    const int ix = int(n / (int64_t(g.nz + 1) * (g.ny + 1)));
+    constexpr int nat[8] = {0, 1, 3, 2, 4, 5, 7, 6};   // native index of binary offset code
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int bx = 0; bx < 2; ++bx) for (int by = 0; by < 2; ++by) for (int bz = 0; bz < 2; ++bz) {
+        const int ex = ix - 1 + bx, ey = iy - 1 + by, ez = iz - 1 + bz;
+        if (ex < 0 || ex >= g.nx || ey < 0 || ey >= g.ny || ez < 0 || ez >= g.nz) continue;
+        const T Ee = load_modulus<T, T, SIMP>(E, g.elem(ex, ey, ez), emin, de, penal);
+        const int li = nat[(1 - bx) + 2 * (1 - by) + 4 * (1 - bz)];
+        for (int c = 0; c < 3; ++c) acc[c] += Ee * kd.c[3 * li + c];
+    }
+    unsigned bits = 7u;
+    if constexpr (MASK == MASK_NODE) bits = node_mask ? unsigned(node_mask[n]) : 7u;
+    if constexpr (MASK == MASK_DOF) {
+        bits = 0;
+        for (int c = 0; c < 3; ++c) bits |= (dof_mask[3 * n + (REV ? 2 - c : c)] != 0.0) << c;
+    }
+    for (int c = 0; c < 3; ++c) {
+        const bool fr = (bits >> c) & 1u;
+        T v = acc[c];
+        if (mode == 1) v = fr ? T(1) / v : T(1);
+        else if (mode == 2) v = fr ? v : T(1);
+        d[3 * n + (REV ? 2 - c : c)] = v;
+    }
+}
+
+// ------------------------------------------------------------------------- element energy
+struct Ke { double k[576]; };
+
+template <bool REV, int MASK>
+__global__ void energy_kernel(Grid g, const __grid_constant__ Ke ke, const double* __restrict__ u,
+                              const double* __restrict__ dof_mask, double* __restrict__ ce,
+                              const double* __restrict__ rho, double emin, double de, double penal,
+                              double* __restrict__ dc) {
+    const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= g.elems()) return;
+    const int ez = int(e % g.nz);
+    const int ey = int((e / g.nz) % g.ny);
+    const int ex = int(e / (int64_t(g.nz) * g.ny));
+    constexpr int ox[8] = {0, 1, 1, 0, 0, 1, 1, 0}, oy[8] = {0, 0, 1, 1, 0, 0, 1, 1},
+                  oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    double ue[24];
+    #pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int64_t n = g.node(ex + ox[i], ey + oy[i], ez + oz[i]);
+        #pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t k = 3 * n + (REV ? 2 - c : c);
+            double val = u[k];
+            if constexpr (MASK == MASK_DOF) val = dof_mask[k] != 0.0 ? val : 0.0;
+            ue[3 * i + c] = val;
+        }
+    }
+    double s = 0.0;
+    #pragma unroll 4
+    for (int r = 0; r < 24; ++r) {
+        double t = 0.0;
+        #pragma unroll
+        for (int c = 0; c < 24; ++c) t = fma(ke.k[24 * r + c], ue[c], t);
+        s = fma(ue[r], t, s);
+    }
+    ce[e] = s;
+    if (dc) {
+        const double rr = rho[e];
+        dc[e] = -penal * pow(rr, penal - 1.0) * de * s;
+    }
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+// =========================================================================== C ABI
+extern "C" int vx_matvec(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                         const void* u, void* y, const uint8_t* node_mask, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(blocks && E && u && y, VX_ERR_NULL_POINTER, "vx_matvec: NULL pointer");
+    Grid g{nx, ny, nz};
+    if (prec == VX_F64) {
+        OpArgs<double, double, double, double> a{};
+        a.g = g; a.u = (const double*)u; a.E = (const double*)E; a.y = (double*)y; a.node_mask = node_mask;
+        a.C = convert_blocks<double>(blocks);
+        return node_mask ? launch_stream<double, double, double, double, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
+                         : launch_stream<double, double, double, double, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
+    } else if (prec == VX_F32) {
+        OpArgs<float, float, float, float> a{};
+        a.g = g; a.u = (const float*)u; a.E = (const float*)E; a.y = (float*)y; a.node_mask = node_mask;
+        a.C = convert_blocks<float>(blocks);
+        return node_mask ? launch_stream<float, float, float, float, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
+                         : launch_stream<float, float, float, float, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
+    } else if (prec == VX_BF16_F32) {
+        OpArgs<float, __nv_bfloat16, __nv_bfloat16, float> a{};
+        a.g = g; a.u = (const __nv_bfloat16*)u; a.E = (const __nv_bfloat16*)E; a.y = (float*)y; a.node_mask = node_mask;
+        a.C = convert_blocks<float>(blocks);
+        return node_mask ? launch_stream<float, __nv_bfloat16, __nv_bfloat16, float, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
+                         : launch_stream<float, __nv_bfloat16, __nv_bfloat16, float, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
+    }
+    set_error("vx_matvec: unknown precision %d", prec);
+    return VX_ERR_INVALID_ARGUMENT;
+}
+
+extern "C" int vx_modal8(const double* blocks, const double* E, const double* u, double* y,
+                         int nx, int ny, int nz, cudaStream_t stream) {
+    return vx_matvec(VX_F64, nx, ny, nz, blocks, E, u, y, nullptr, stream);
+}
+
+extern "C" int vx_matvec_dense(int prec, int nx, int ny, int nz, const double* ke, const void* E,
+                               const void* u, void* y, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(ke && E && u && y, VX_ERR_NULL_POINTER, "vx_matvec_dense: NULL pointer");
+    Grid g{nx, ny, nz};
+    const int64_t n = g.nodes();
+    const unsigned blocksz = 128;
+    const unsigned grid = unsigned((n + blocksz - 1) / blocksz);
+    if (prec == VX_F64) {
+        dense_gather<double><<<grid, blocksz, 0, stream>>>(g, ke, (const double*)E, (const double*)u, (double*)y);
+    } else if (prec == VX_F32) {
+        // ke is device FP32 here
+        dense_gather<float><<<grid, blocksz, 0, stream>>>(g, (const float*)ke, (const float*)E, (const float*)u, (float*)y);
+    } else {
+        set_error("vx_matvec_dense: unsupported precision %d", prec);
+        return VX_ERR_INVALID_ARGUMENT;
+    }
+    VX_CHECK_LAUNCH("vx_matvec_dense");
+    return VX_OK;
+}
+
+extern "C" int vx_diagonal(int prec, int nx, int ny, int nz, const double* ke, const void* E,
+                           const uint8_t* node_mask, int inverse, void* d, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(ke && E && d, VX_ERR_NULL_POINTER, "vx_diagonal: NULL pointer");
+    Grid g{nx, ny, nz};
+    const int64_t n = g.nodes();
+    const unsigned grid = unsigned((n + 255) / 256);
+    if (prec == VX_F64) {
+        BlocksT<double> kd{};
+        for (int i = 0; i < 24; ++i) kd.c[i] = ke[25 * i];
+        diag_kernel<double, false, MASK_NODE, false><<<grid, 256, 0, stream>>>(
+            g, kd, (const double*)E, node_mask, nullptr, 0, 0, 0, inverse ? 1 : 0, (double*)d);
+    } else if (prec == VX_F32) {
+        BlocksT<float> kd{};
+        for (int i = 0; i < 24; ++i) kd.c[i] = float(ke[25 * i]);
+        diag_kernel<float, false, MASK_NODE, false><<<grid, 256, 0, stream>>>(
+            g, kd, (const float*)E, node_mask, nullptr, 0, 0, 0, inverse ? 1 : 0, (float*)d);
+    } else {
+        set_error("vx_diagonal: unsupported precision %d", prec);
+        return VX_ERR_INVALID_ARGUMENT;
+    }
+    VX_CHECK_LAUNCH("vx_diagonal");
+    return VX_OK;
+}
+
+extern "C" int vx_element_energy(int nx, int ny, int nz, const double* ke, const double* u, double* ce,
+                                 const double* rho, double emin, double emax, double penal, double* dc,
+                                 cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(ke && u && ce, VX_ERR_NULL_POINTER, "vx_element_energy: NULL pointer");
+    VX_CHECK_ARG(!dc || rho, VX_ERR_NULL_POINTER, "vx_element_energy: dc requested without rho");
+    Grid g{nx, ny, nz};
+    Ke k;
+    for (int i = 0; i < 576; ++i) k.k[i] = ke[i];
+    const int64_t n = g.elems();
+    energy_kernel<false, MASK_NONE><<<unsigned((n + 127) / 128), 128, 0, stream>>>(
+        g, k, u, nullptr, ce, rho, emin, emax - emin, penal, dc);
+    VX_CHECK_LAUNCH("vx_element_energy");
+    return VX_OK;
+}
+
+// Natural layout = author layout of the grid (nz, ny, nx) with the x<->z axes swapped; the
+// kernels read component c from storage slot 2-c (REV) and use the axis-permuted element matrix.
+namespace {
+void permute_ke_xz(const double* ke, double* kp) {
+    // native offsets; kernel-native node i' has offsets (z_i, y_i, x_i) of physical node pi(i')
+    const int ox[8] = {0, 1, 1, 0, 0, 1, 1, 0}, oy[8] = {0, 0, 1, 1, 0, 0, 1, 1}, oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    int pi[8];
+    for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j)
+            if (ox[j] == oz[i] && oy[j] == oy[i] && oz[j] == ox[i]) pi[i] = j;
+    for (int i = 0; i < 8; ++i) for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 8; ++j) for (int b = 0; b < 3; ++b)
+            kp[(3 * i + a) * 24 + 3 * j + b] = ke[(3 * pi[i] + (2 - a)) * 24 + 3 * pi[j] + (2 - b)];
+}
+}  // namespace
+
+extern "C" int vx_product(int nx, int ny, int nz, const double* rho, const double* u, const double* ke,
+                          const double* mask, double emin, double emax, double penal,
+                          double* y, double* ce, double* diag, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(rho && u && ke && mask, VX_ERR_NULL_POINTER, "vx_product: NULL pointer");
+    // kernel grid: (nz, ny, nx) author layout == natural layout of (nx, ny, nz)
+    Grid g{nz, ny, nx};
+    double kp[576], blocks[72], disc = 0.0;
+    permute_ke_xz(ke, kp);
+    if (y) {
+        st = vx_parity_blocks(kp, blocks, &disc);
+        if (st) return st;
+        OpArgs<double, double, double, double> a{};
+        a.g = g; a.u = u; a.E = rho; a.y = y; a.dof_mask = mask;
+        a.emin = emin; a.de = emax - emin; a.penal = penal;
+        a.C = convert_blocks<double>(blocks);
+        st = launch_stream<double, double, double, double, EPI_RAW, MASK_DOF, true, true>(a, stream, "vx_product");
+        if (st) return st;
+    }
+    if (ce) {
+        Ke k;
+        for (int i = 0; i < 576; ++i) k.k[i] = kp[i];
+        const int64_t n = g.elems();
+        energy_kernel<true, MASK_DOF><<<unsigned((n + 127) / 128), 128, 0, stream>>>(
+            g, k, u, mask, ce, nullptr, 0.0, 0.0, 0.0, nullptr);
+        VX_CHECK_LAUNCH("vx_product(ce)");
+    }
+    if (diag) {
+        BlocksT<double> kd{};
+        for (int i = 0; i < 24; ++i) kd.c[i] = kp[25 * i];
+        diag_kernel<double, true, MASK_DOF, true><<<unsigned((g.nodes() + 255) / 256), 256, 0, stream>>>(
+            g, kd, rho, nullptr, mask, emin, emax - emin, penal, 2, diag);
+        VX_CHECK_LAUNCH("vx_product(diag)");
+    }
+    return VX_OK;
+}
+
+// Fused smoother / residual / outer-CG operator forms (author layout, node mask optional).
+namespace {
+template <int EPI, typename T>
+int fused_op(const char* what, int nx, int ny, int nz, const double* blocks, const void* E,
+             const uint8_t* node_mask, const void* x, const void* r, const void* invd, double omega,
+             void* out, double* partials, cudaStream_t stream) {
+    OpArgs<T, T, T, T> a{};
+    a.g = Grid{nx, ny, nz};
+    a.u = (const T*)x; a.E = (const T*)E; a.y = (T*)out; a.node_mask = node_mask;
+    a.r = (const T*)r; a.invd = (const T*)invd; a.omega = T(omega); a.partials = partials;
+    a.C = convert_blocks<T>(blocks);
+    return node_mask ? launch_stream<T, T, T, T, EPI, MASK_NODE, false, false>(a, stream, what)
+                     : launch_stream<T, T, T, T, EPI, MASK_NONE, false, false>(a, stream, what);
+}
+
+template <int EPI>
+int fused_dispatch(const char* what, int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                   const uint8_t* node_mask, const void* x, const void* r, const void* invd, double omega,
+                   void* out, double* partials, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(blocks && E && x && out, VX_ERR_NULL_POINTER, "%s: NULL pointer", what);
+    VX_CHECK_ARG(x != out, VX_ERR_INVALID_ARGUMENT, "%s: output may not alias the operand", what);
+    if (prec == VX_F64)
+        return fused_op<EPI, double>(what, nx, ny, nz, blocks, E, node_mask, x, r, invd, omega, out, partials, stream);
+    if (prec == VX_F32)
+        return fused_op<EPI, float>(what, nx, ny, nz, blocks, E, node_mask, x, r, invd, omega, out, partials, stream);
+    set_error("%s: unsupported precision %d", what, prec);
+    return VX_ERR_INVALID_ARGUMENT;
+}
+}  // namespace
+
+extern "C" int vx_jacobi_sweep(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                               const uint8_t* node_mask, const void* x, const void* r, const void* inv_diag,
+                               double omega, void* x_out, cudaStream_t stream) {
+    VX_CHECK_ARG(r && inv_diag, VX_ERR_NULL_POINTER, "vx_jacobi_sweep: NULL r / inv_diag");
+    return fused_dispatch<EPI_JACOBI>("vx_jacobi_sweep", prec, nx, ny, nz, blocks, E, node_mask, x, r,
+                                      inv_diag, omega, x_out, nullptr, stream);
+}
+
+extern "C" int vx_residual(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                           const uint8_t* node_mask, const void* x, const void* r, void* res,
+                           cudaStream_t stream) {
+    VX_CHECK_ARG(r, VX_ERR_NULL_POINTER, "vx_residual: NULL r");
+    return fused_dispatch<EPI_RESIDUAL>("vx_residual", prec, nx, ny, nz, blocks, E, node_mask, x, r,
+                                        nullptr, 0.0, res, nullptr, stream);
+}
+
+extern "C" int64_t vx_operator_partials(int nx, int ny, int nz) {
+    if (check_grid(nx, ny, nz)) return -1;
+    return stream_ctas(Grid{nx, ny, nz});
+}
+
+extern "C" int vx_apply_dot(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                            const uint8_t* node_mask, const void* p, void* q, double* partials,
+                            cudaStream_t stream) {
+    VX_CHECK_ARG(partials, VX_ERR_NULL_POINTER, "vx_apply_dot: NULL partials");
+    return fused_dispatch<EPI_APPLY_DOT>("vx_apply_dot", prec, nx, ny, nz, blocks, E, node_mask, p, nullptr,
+                                         nullptr, 0.0, q, partials, stream);
+}
+
+extern "C" int vx_true_residual(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                                const uint8_t* node_mask, const void* x, const void* b, void* res,
+                                double* partials, cudaStream_t stream) {
+    VX_CHECK_ARG(b && partials, VX_ERR_NULL_POINTER, "vx_true_residual: NULL b / partials");
+    return fused_dispatch<EPI_TRUE_RES>("vx_true_residual", prec, nx, ny, nz, blocks, E, node_mask, x, b,
+                                        nullptr, 0.0, res, partials, stream);
+}

@@ -1,0 +1,362 @@
+// Solver kernels with device-resident scalars, and a CUDA-graph WHILE loop.
+//
+// The outer Krylov loops keep every scalar (r.z, p.q, alpha, beta, |b - A x|, the iteration and
+// matvec counters, the converged flag) in a small FP64 array S on the device.  Each reduction is
+// two-stage and deterministic: the producing kernel writes one partial per CTA, a one-CTA
+// "finalize" kernel sums them in a fixed order and applies the scalar recurrence.  With the loop
+// body captured as the body of a conditional WHILE graph node, a complete solve is a single graph
+// launch with no host round trip per iteration; the condition kernel stops the loop on
+// convergence, on breakdown or at maxiter.
+#include "vx_common.cuh"
+
+namespace vx {
+
+constexpr int FT = 256;
+
+enum Slot {
+    S_RZ = 0, S_PQ = 1, S_ALPHA = 2, S_RR = 3, S_REL = 4, S_NB = 5, S_BETA = 6, S_RZN = 7, S_RZD = 8,
+    S_TOL = 9, S_DONE = 10, S_IT = 11, S_MAXIT = 12, S_MV = 13, S_BREAK = 14, S_CHECK = 15, S_COUNT = 16
+};
+
+enum FinOp {
+    FIN_PQ = 0,        // S[PQ] = sum; alpha = rz / pq (breakdown if pq == 0); it += 1; mv += 1
+    FIN_TRUE = 1,      // S[RR] = sum; rel = sqrt(rr) / nb; mv += 1; done if rel <= tol
+    FIN_BETA_PR = 2,   // rzn = sum0, rzd = sum1; beta = rzd / rz; rz = rzn      (flexible / Polak-Ribiere)
+    FIN_BETA_FR = 3,   // rzn = sum0; beta = rzn / rz; rz = rzn                  (Fletcher-Reeves)
+    FIN_NB = 4,        // nb = sqrt(sum)
+    FIN_RZ = 5,        // rz = sum0
+    FIN_RR_ONLY = 6    // rr = sum; rel = sqrt(rr) / nb (no counters, no flag)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ double block_sum_ft(double v) {
+    __shared__ double red[FT / 32];
+    v = warp_sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) s = warp_sum(threadIdx.x < FT / 32 ? red[threadIdx.x] : 0.0);
+    return s;
+}
+
+__global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const double* __restrict__ partials,
+                                                      double* __restrict__ S) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t j = threadIdx.x; j < G; j += FT) s0 += partials[j];
+    s0 = block_sum_ft(s0);
+    if (op == FIN_BETA_PR) {
+        for (int64_t j = threadIdx.x; j < G; j += FT) s1 += partials[G + j];
+        s1 = block_sum_ft(s1);
+    }
+    if (threadIdx.x != 0) return;
+    switch (op) {
+        case FIN_PQ:
+            S[S_PQ] = s0;
+            if (s0 == 0.0 || !isfinite(s0)) { S[S_BREAK] = 1.0; S[S_ALPHA] = 0.0; }
+            else S[S_ALPHA] = S[S_RZ] / s0;
+            S[S_IT] += 1.0;
+            S[S_MV] += 1.0;
+            break;
+        case FIN_TRUE:
+            S[S_RR] = s0;
+            S[S_REL] = sqrt(s0) / S[S_NB];
+            S[S_MV] += 1.0;
+            if (S[S_REL] <= S[S_TOL]) S[S_DONE] = 1.0;
+            if (!isfinite(S[S_REL])) S[S_BREAK] = 1.0;
+            break;
+        case FIN_BETA_PR:
+            S[S_RZN] = s0;
+            S[S_RZD] = s1;
+            S[S_BETA] = s1 / S[S_RZ];
+            S[S_RZ] = s0;
+            break;
+        case FIN_BETA_FR:
+            S[S_RZN] = s0;
+            S[S_BETA] = s0 / S[S_RZ];
+            S[S_RZ] = s0;
+            break;
+        case FIN_NB: S[S_NB] = sqrt(s0); break;
+        case FIN_RZ: S[S_RZ] = s0; break;
+        case FIN_RR_ONLY:
+            S[S_RR] = s0;
+            S[S_REL] = sqrt(s0) / S[S_NB];
+            break;
+    }
+}
+
+// x += alpha p; r -= alpha q (r update skipped when it is about to be replaced by b - A x).
+// Nothing moves once the loop has converged or broken down.
+template <typename T>
+__global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __restrict__ x, const T* __restrict__ p,
+                                 T* __restrict__ r, const T* __restrict__ q, int update_r) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (S[S_DONE] != 0.0 || S[S_BREAK] != 0.0) return;
+    const T a = T(S[S_ALPHA]);
+    x[i] = x[i] + a * p[i];
+    if (update_r) r[i] = r[i] - a * q[i];
+}
+
+// p = z + beta p
+template <typename T>
+__global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, const T* __restrict__ z, T* __restrict__ p) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    p[i] = z[i] + T(S[S_BETA]) * p[i];
+}
+
+// partials for r . zn and r . (zn - zo), fixed grid G (a function of n), fixed order
+template <typename T>
+__global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const T* __restrict__ zn,
+                                                     const T* __restrict__ zo, double* __restrict__ partials) {
+    const int64_t G = gridDim.x;
+    double a = 0.0, b = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
+        const double ri = double(r[i]), zi = double(zn[i]);
+        a = fma(ri, zi, a);
+        if (zo) b = fma(ri, zi - double(zo[i]), b);
+    }
+    a = block_sum_ft(a);
+    if (threadIdx.x == 0) partials[blockIdx.x] = a;
+    if (zo) {
+        b = block_sum_ft(b);
+        if (threadIdx.x == 0) partials[G + blockIdx.x] = b;
+    }
+}
+
+// z = d * r (Jacobi) with partial r . z
+template <typename T>
+__global__ void __launch_bounds__(FT) jacobi_precond_dot_kernel(int64_t n, const T* __restrict__ d, const T* __restrict__ r,
+                                                                T* __restrict__ z, double* __restrict__ partials) {
+    const int64_t G = gridDim.x;
+    double a = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
+        const T zi = d[i] * r[i];
+        z[i] = zi;
+        a = fma(double(r[i]), double(zi), a);
+    }
+    a = block_sum_ft(a);
+    if (threadIdx.x == 0) partials[blockIdx.x] = a;
+}
+
+// V-cycle entry: r_mg = (TM) r64 (skipped when r_mg is NULL), x = omega * invd * r_mg
+template <typename TM>
+__global__ void vcycle_entry_kernel(int64_t n, const double* __restrict__ r64, TM* __restrict__ rmg,
+                                    const TM* __restrict__ invd, double omega, TM* __restrict__ x) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    TM r = rmg ? TM(r64[i]) : TM(r64[i]);
+    if (rmg) rmg[i] = r;
+    x[i] = TM(omega) * invd[i] * r;
+}
+
+template <typename T>
+__global__ void scaled_product_kernel(int64_t n, double omega, const T* __restrict__ a, const T* __restrict__ b,
+                                      T* __restrict__ out) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = T(omega) * a[i] * b[i];
+}
+
+__global__ void set_scalars_kernel(double* S, int first, int count, double value) {
+    const int i = threadIdx.x;
+    if (i < count) S[first + i] = value;
+}
+
+__global__ void condition_kernel(cudaGraphConditionalHandle h, const double* __restrict__ S) {
+    if (threadIdx.x == 0) {
+        const bool go = S[S_DONE] == 0.0 && S[S_BREAK] == 0.0 && S[S_IT] < S[S_MAXIT];
+        cudaGraphSetConditional(h, go ? 1u : 0u);
+    }
+}
+
+int64_t fixed_ctas(int64_t n) {
+    int64_t g = (n + FT * 8 - 1) / (FT * 8);
+    return g < 1 ? 1 : (g > 1184 ? 1184 : g);
+}
+
+inline unsigned nb(int64_t n, int t) { return unsigned((n + t - 1) / t); }
+
+struct WhileGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle handle = 0;
+    cudaGraph_t body = nullptr;
+};
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" int vx_solver_slots(void) { return S_COUNT; }
+
+extern "C" int64_t vx_solver_partials(int64_t n) { return fixed_ctas(n); }
+
+extern "C" int vx_solver_finalize(int op, int64_t G, const double* partials, double* S, cudaStream_t stream) {
+    VX_CHECK_ARG(op >= 0 && op <= FIN_RR_ONLY && G > 0, VX_ERR_INVALID_ARGUMENT, "vx_solver_finalize: bad op/G");
+    VX_CHECK_ARG(partials && S, VX_ERR_NULL_POINTER, "vx_solver_finalize: NULL pointer");
+    finalize_kernel<<<1, FT, 0, stream>>>(op, G, partials, S);
+    VX_CHECK_LAUNCH("vx_solver_finalize");
+    return VX_OK;
+}
+
+extern "C" int vx_cg_update(int prec, int64_t n, const double* S, void* x, const void* p, void* r, const void* q,
+                            int update_r, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_update: n must be positive");
+    VX_CHECK_ARG(S && x && p && (!update_r || (r && q)), VX_ERR_NULL_POINTER, "vx_cg_update: NULL pointer");
+    if (prec == VX_F64)
+        cg_update_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, S, (double*)x, (const double*)p, (double*)r,
+                                                                 (const double*)q, update_r);
+    else if (prec == VX_F32)
+        cg_update_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, S, (float*)x, (const float*)p, (float*)r,
+                                                                (const float*)q, update_r);
+    else { set_error("vx_cg_update: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_cg_update");
+    return VX_OK;
+}
+
+extern "C" int vx_cg_direction(int prec, int64_t n, const double* S, const void* z, void* p, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction: n must be positive");
+    VX_CHECK_ARG(S && z && p, VX_ERR_NULL_POINTER, "vx_cg_direction: NULL pointer");
+    if (prec == VX_F64) cg_direction_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, S, (const double*)z, (double*)p);
+    else if (prec == VX_F32) cg_direction_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p);
+    else { set_error("vx_cg_direction: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_cg_direction");
+    return VX_OK;
+}
+
+extern "C" int vx_dots_pr(int prec, int64_t n, const void* r, const void* zn, const void* zo, double* partials,
+                          cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_dots_pr: n must be positive");
+    VX_CHECK_ARG(r && zn && partials, VX_ERR_NULL_POINTER, "vx_dots_pr: NULL pointer");
+    const unsigned G = unsigned(fixed_ctas(n));
+    if (prec == VX_F64)
+        dots_pr_kernel<double><<<G, FT, 0, stream>>>(n, (const double*)r, (const double*)zn, (const double*)zo, partials);
+    else if (prec == VX_F32)
+        dots_pr_kernel<float><<<G, FT, 0, stream>>>(n, (const float*)r, (const float*)zn, (const float*)zo, partials);
+    else { set_error("vx_dots_pr: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_dots_pr");
+    return VX_OK;
+}
+
+extern "C" int vx_jacobi_precond_dot(int prec, int64_t n, const void* d, const void* r, void* z, double* partials,
+                                     cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_jacobi_precond_dot: n must be positive");
+    VX_CHECK_ARG(d && r && z && partials, VX_ERR_NULL_POINTER, "vx_jacobi_precond_dot: NULL pointer");
+    const unsigned G = unsigned(fixed_ctas(n));
+    if (prec == VX_F64)
+        jacobi_precond_dot_kernel<double><<<G, FT, 0, stream>>>(n, (const double*)d, (const double*)r, (double*)z, partials);
+    else if (prec == VX_F32)
+        jacobi_precond_dot_kernel<float><<<G, FT, 0, stream>>>(n, (const float*)d, (const float*)r, (float*)z, partials);
+    else { set_error("vx_jacobi_precond_dot: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_jacobi_precond_dot");
+    return VX_OK;
+}
+
+extern "C" int vx_vcycle_entry(int prec, int64_t n, const double* r64, void* r_mg, const void* inv_diag, double omega,
+                               void* x, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry: n must be positive");
+    VX_CHECK_ARG(r64 && inv_diag && x, VX_ERR_NULL_POINTER, "vx_vcycle_entry: NULL pointer");
+    if (prec == VX_F64)
+        vcycle_entry_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, r64, (double*)r_mg, (const double*)inv_diag, omega, (double*)x);
+    else if (prec == VX_F32)
+        vcycle_entry_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, r64, (float*)r_mg, (const float*)inv_diag, omega, (float*)x);
+    else { set_error("vx_vcycle_entry: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_vcycle_entry");
+    return VX_OK;
+}
+
+extern "C" int vx_scaled_product(int prec, int64_t n, double omega, const void* a, const void* b, void* out,
+                                 cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_scaled_product: n must be positive");
+    VX_CHECK_ARG(a && b && out, VX_ERR_NULL_POINTER, "vx_scaled_product: NULL pointer");
+    if (prec == VX_F64)
+        scaled_product_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, omega, (const double*)a, (const double*)b, (double*)out);
+    else if (prec == VX_F32)
+        scaled_product_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, omega, (const float*)a, (const float*)b, (float*)out);
+    else { set_error("vx_scaled_product: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_scaled_product");
+    return VX_OK;
+}
+
+extern "C" int vx_set_scalars(double* S, int first, int count, double value, cudaStream_t stream) {
+    VX_CHECK_ARG(S, VX_ERR_NULL_POINTER, "vx_set_scalars: NULL S");
+    VX_CHECK_ARG(first >= 0 && count >= 1 && first + count <= S_COUNT, VX_ERR_INVALID_ARGUMENT,
+                 "vx_set_scalars: slots out of range");
+    set_scalars_kernel<<<1, 32, 0, stream>>>(S, first, count, value);
+    VX_CHECK_LAUNCH("vx_set_scalars");
+    return VX_OK;
+}
+
+// ----------------------------------------------------------------------------- WHILE graphs
+extern "C" int vx_graph_while_begin(cudaStream_t stream, void** handle) {
+    VX_CHECK_ARG(handle, VX_ERR_NULL_POINTER, "vx_graph_while_begin: NULL handle");
+    VX_CHECK_ARG(stream != nullptr, VX_ERR_INVALID_ARGUMENT, "vx_graph_while_begin: capture needs a non-default stream");
+    auto* w = new WhileGraph();
+    cudaError_t e = cudaGraphCreate(&w->graph, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&w->handle, w->graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNode_t node;
+    cudaGraphNodeParams p = {};
+    if (e == cudaSuccess) {
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = w->handle;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        e = cudaGraphAddNode(&node, w->graph, nullptr, 0, &p);
+    }
+    if (e == cudaSuccess) {
+        w->body = p.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(stream, w->body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    }
+    if (e != cudaSuccess) {
+        if (w->graph) cudaGraphDestroy(w->graph);
+        delete w;
+        set_error("vx_graph_while_begin: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    *handle = w;
+    return VX_OK;
+}
+
+extern "C" int vx_graph_while_end(void* handle, const double* S, cudaStream_t stream) {
+    VX_CHECK_ARG(handle && S, VX_ERR_NULL_POINTER, "vx_graph_while_end: NULL pointer");
+    auto* w = static_cast<WhileGraph*>(handle);
+    condition_kernel<<<1, 32, 0, stream>>>(w->handle, S);
+    cudaError_t e = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(stream, &captured);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&w->exec, w->graph, 0);
+    if (e != cudaSuccess) {
+        set_error("vx_graph_while_end: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    return VX_OK;
+}
+
+extern "C" int vx_graph_launch(void* handle, cudaStream_t stream) {
+    VX_CHECK_ARG(handle, VX_ERR_NULL_POINTER, "vx_graph_launch: NULL handle");
+    auto* w = static_cast<WhileGraph*>(handle);
+    VX_CHECK_ARG(w->exec, VX_ERR_INVALID_ARGUMENT, "vx_graph_launch: graph was not instantiated");
+    cudaError_t e = cudaGraphLaunch(w->exec, stream);
+    if (e != cudaSuccess) {
+        set_error("vx_graph_launch: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    return VX_OK;
+}
+
+extern "C" int vx_graph_destroy(void* handle) {
+    if (!handle) return VX_OK;
+    auto* w = static_cast<WhileGraph*>(handle);
+    if (w->exec) cudaGraphExecDestroy(w->exec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    delete w;
+    return VX_OK;
+}
