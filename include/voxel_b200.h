@@ -178,13 +178,64 @@ int64_t vx_partials_size(int64_t n);
 int vx_dots(int prec, int64_t n, int count, const void* const* a, const void* const* b,
             double* partials, double* out, cudaStream_t stream);
 
-/* Fused y := alpha * x + beta * y (FP64 scalars read from DEVICE memory if `dev_scalars` != 0,
- * else taken from alpha/beta) -- see vx_axpby_dev for the device-scalar form. */
+/* y := alpha * x + beta * y (host scalars; VX_F64 / VX_F32). */
 int vx_axpby(int prec, int64_t n, double alpha, const void* x, double beta, void* y, cudaStream_t stream);
 
 /* Cast between storage precisions (VX_F64 <-> VX_F32 <-> bf16), optional scale (dst = scale*src). */
 int vx_cast(int64_t n, int src_prec, const void* src, int dst_prec, void* dst, double scale,
             cudaStream_t stream);
+
+/* Operator forms fused with the outer Krylov loop (FP64/FP32, author layout, node mask optional):
+ *   vx_apply_dot:     q = A p and partials[cta] = sum p.q over the CTA's owned nodes
+ *   vx_true_residual: res = b - A x and partials[cta] = sum res^2
+ * `partials` holds vx_operator_partials(nx, ny, nz) doubles; sum them with vx_reduce_partials or
+ * vx_solver_finalize.  Replace the `apply_A(p)` + `p @ q` and `b - apply_A(x)` + `norm` pairs of
+ * src/voxel_mg.py:192-203 and donor simp_r2.py:255-270. */
+int64_t vx_operator_partials(int nx, int ny, int nz);
+int vx_apply_dot(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                 const uint8_t* node_mask, const void* p, void* q, double* partials, cudaStream_t stream);
+int vx_true_residual(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                     const uint8_t* node_mask, const void* x, const void* b, void* res, double* partials,
+                     cudaStream_t stream);
+int vx_reduce_partials(int64_t G, int count, const double* partials, double* out, cudaStream_t stream);
+
+/* ---------------------------------------------------------------------------- device-scalar solvers
+ * The Krylov loops of the reference (src/voxel_mg.py:181-217 fcg; donor simp_r2.py:187-295 pcg) with
+ * every scalar in a device array S of vx_solver_slots() doubles:
+ *   S[0] r.z  S[1] p.q  S[2] alpha  S[3] |b-Ax|^2  S[4] rel  S[5] |b|  S[6] beta  S[7] r.z_new
+ *   S[8] r.(z_new-z_old)  S[9] tol  S[10] done  S[11] iterations  S[12] maxiter  S[13] matvecs
+ *   S[14] breakdown  S[15] iterations per loop body
+ * vx_solver_finalize(op, G, partials, S) sums G partials in a fixed order and applies op:
+ *   0 p.q -> alpha = rz/pq, it++, mv++      1 |b-Ax|^2 -> rel, mv++, done if rel <= tol
+ *   2 Polak-Ribiere beta (two partial rows)  3 Fletcher-Reeves beta   4 |b|   5 r.z   6 rel only */
+int vx_solver_slots(void);
+int64_t vx_solver_partials(int64_t n);
+int vx_solver_finalize(int op, int64_t G, const double* partials, double* S, cudaStream_t stream);
+int vx_cg_update(int prec, int64_t n, const double* S, void* x, const void* p, void* r, const void* q,
+                 int update_r, cudaStream_t stream);
+int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, const void* z, void* p, void* z_old,
+                    cudaStream_t stream);
+int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const void* zn, const void* zo,
+               double* partials, cudaStream_t stream);
+int vx_jacobi_precond_dot(int prec, int64_t n, const void* d, const void* r, void* z, double* partials,
+                          cudaStream_t stream);
+/* V-cycle entry: r_mg = (prec) r64 (skipped if r_mg is NULL) and x = omega * inv_diag * r_mg;
+ * the first damped-Jacobi step of src/voxel_mg.py:165 fused with the cast of :178. */
+int vx_vcycle_entry(int prec, int64_t n, const double* r64, void* r_mg, const void* inv_diag, double omega,
+                    void* x, cudaStream_t stream);
+int vx_scaled_product(int prec, int64_t n, double omega, const void* a, const void* b, void* out,
+                      cudaStream_t stream);
+int vx_set_scalars(double* S, int first, int count, double value, cudaStream_t stream);
+
+/* A CUDA-graph WHILE loop: begin captures the loop body from `stream` (non-default); end appends
+ * the condition kernel (continue while !done && !breakdown && it + S[15] <= maxiter) and
+ * instantiates; launch runs the whole loop as one graph launch. */
+int vx_graph_while_begin(cudaStream_t stream, void** handle);
+int vx_graph_while_end(void* handle, const double* S, cudaStream_t stream);
+int vx_graph_launch(void* handle, cudaStream_t stream);
+/* Capture state of `stream`: 0 none, 1 active, 2 invalidated, -1 query failed. */
+int vx_capture_status(cudaStream_t stream);
+int vx_graph_destroy(void* handle);
 
 #ifdef __cplusplus
 }

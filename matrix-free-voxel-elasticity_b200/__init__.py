@@ -10,7 +10,12 @@ from .element import XYZ, Modal, element, quadrature
 from .layout import edof_author, element_nodes, n_elems, n_nodes, to_author, to_natural
 from .operators import (Product, VoxelOperator, cast, dofs_from_node_mask, dots, node_mask_from_dofs,
                         product, reduce_partials, simp_modulus)
+from . import problems, solver, voxel_mg  # noqa: E402
+from .solver import FCGSolver, JacobiPCG, JacobiPreconditioner, MGHierarchy, SolveResult, hierarchy_shapes
+from .api import ElasticitySolver, solve
 
 __all__ = ["XYZ", "Modal", "element", "quadrature", "edof_author", "element_nodes", "n_elems", "n_nodes",
            "to_author", "to_natural", "Product", "VoxelOperator", "cast", "dofs_from_node_mask", "dots",
-           "node_mask_from_dofs", "product", "reduce_partials", "simp_modulus"]
+           "node_mask_from_dofs", "product", "reduce_partials", "simp_modulus", "problems", "solver", "voxel_mg",
+           "FCGSolver", "JacobiPCG", "JacobiPreconditioner", "MGHierarchy", "SolveResult", "hierarchy_shapes",
+           "ElasticitySolver", "solve"]

@@ -51,6 +51,22 @@ SIGNATURES = {
     "vx_reduce_partials": (c_int, [c_int64, c_int, _P, _P, _P]),
     "vx_axpby": (c_int, [c_int, c_int64, c_double, _P, c_double, _P, _P]),
     "vx_cast": (c_int, [c_int64, c_int, _P, c_int, _P, c_double, _P]),
+    # solver kernels with device-resident scalars and WHILE graphs
+    "vx_solver_slots": (c_int, []),
+    "vx_solver_partials": (c_int64, [c_int64]),
+    "vx_solver_finalize": (c_int, [c_int, c_int64, _P, _P, _P]),
+    "vx_cg_update": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P, c_int, _P]),
+    "vx_cg_direction": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P]),
+    "vx_dots_pr": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P]),
+    "vx_jacobi_precond_dot": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P]),
+    "vx_vcycle_entry": (c_int, [c_int, c_int64, _P, _P, _P, c_double, _P, _P]),
+    "vx_scaled_product": (c_int, [c_int, c_int64, c_double, _P, _P, _P, _P]),
+    "vx_set_scalars": (c_int, [_P, c_int, c_int, c_double, _P]),
+    "vx_graph_while_begin": (c_int, [_P, ctypes.POINTER(c_void_p)]),
+    "vx_graph_while_end": (c_int, [_P, _P, _P]),
+    "vx_graph_launch": (c_int, [_P, _P]),
+    "vx_graph_destroy": (c_int, [_P]),
+    "vx_capture_status": (c_int, [_P]),
 }
 
 _lib = None
@@ -87,8 +103,16 @@ def check(status: int, what: str = "") -> None:
     raise RuntimeError(msg)
 
 
+# While a WHILE-graph body is being captured this holds the capture stream: every call then checks
+# that the capture is still valid, so the first operation that invalidates it is named.
+CAPTURE_STREAM = None
+
+
 def call(name: str, *args) -> None:
-    check(getattr(load(), name)(*args), name)
+    lib = load()
+    check(getattr(lib, name)(*args), name)
+    if CAPTURE_STREAM is not None and lib.vx_capture_status(CAPTURE_STREAM) == 2:
+        raise RuntimeError(f"{name} invalidated the stream capture")
 
 
 def dptr(a) -> _D:

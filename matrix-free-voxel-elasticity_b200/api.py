@@ -1,0 +1,93 @@
+"""Public solve API: one voxel elasticity problem resident on the device.
+
+`ElasticitySolver` owns the FP64 outer operator, the preconditioner (GMG V-cycle in FP64 or FP32,
+or Jacobi) and the graph-captured flexible-CG loop; `solve(...)` is the host-buffer entry point
+(numpy in, numpy out) a caller of the reference's `fcg(..., Multigrid(...))` path would use.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .element import quadrature
+from .operators import VoxelOperator, node_mask_from_dofs
+from .solver import FCGSolver, JacobiPreconditioner, MGHierarchy, hierarchy_shapes
+
+PRECISIONS = ("fp64", "mixed", "jacobi")
+
+
+def _dev(a, dtype=torch.float64):
+    if isinstance(a, torch.Tensor):
+        return a.to(device="cuda", dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda").to(dtype).contiguous()
+
+
+class ElasticitySolver:
+    """K(E) u = f on a (nx, ny, nz) voxel cantilever-type problem, author layout.
+
+    precision: "fp64" (FP64 V-cycle), "mixed" (FP32 V-cycle inside the FP64 outer loop; FP64 for the
+    outer residual, dots, step lengths and the coarsest solve) or "jacobi" (FP64 Jacobi-PCG via fcg).
+    omega: a float, a per-level list, or "spectral" (4 / (3 lambda_l), src/voxel_mg.py:228-244).
+    """
+
+    def __init__(self, shape, E, mask, ke=None, precision="mixed", pre=2, post=2, omega=0.6, max_coarse_x=16,
+                 levels=None, tol=1e-8, maxiter=200, check_every=1, graph=True, spectral_seed=20260923):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {PRECISIONS}")
+        self.shape = tuple(int(s) for s in shape)
+        self.ke = quadrature([1.0, 1.0, 1.0], 0.3) if ke is None else np.asarray(ke, dtype=np.float64).reshape(24, 24)
+        self.E = _dev(E)
+        m = mask if isinstance(mask, torch.Tensor) else _dev(mask)
+        self.node_mask = m.contiguous() if m.dtype == torch.uint8 else node_mask_from_dofs(m.to(torch.float64))
+        self.op64 = VoxelOperator(self.shape, self.ke, torch.float64)
+        self.precision = precision
+        if precision == "jacobi":
+            self.M = JacobiPreconditioner(self.op64, self.E, self.node_mask)
+        else:
+            shapes = hierarchy_shapes(self.shape, max_coarse_x)
+            if levels is not None:
+                if levels > len(shapes):
+                    raise ValueError(f"{self.shape} supports at most {len(shapes)} levels with max_coarse_x={max_coarse_x}")
+                shapes = shapes[:levels]
+            dt = torch.float64 if precision == "fp64" else torch.float32
+            if isinstance(omega, str) and omega == "spectral":
+                # the reference estimates lambda_l once, on the FP64 hierarchy shared by all arms
+                ref = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, torch.float64, pre, post, None,
+                                  shapes=shapes)
+                omega = ref.spectral_omegas(seed=spectral_seed)[0]
+                if dt == torch.float64:
+                    ref.set_omegas(omega)
+                    self.M = ref
+                del ref
+            if not hasattr(self, "M"):
+                self.M = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, dt, pre, post, omega, shapes=shapes)
+        self.fcg = FCGSolver(self.op64, self.E, self.node_mask, self.M, tol=tol, maxiter=maxiter,
+                             check_every=check_every, graph=graph)
+
+    @property
+    def levels(self):
+        return getattr(self.M, "shapes", [self.shape])
+
+    def footprint_bytes(self):
+        return self.fcg.footprint_bytes()
+
+    def solve(self, f):
+        """Solve with right-hand side f (CUDA tensor or array, author layout).  Returns SolveResult
+        (x, iterations, converged, rel, matvecs); x is the solver's own buffer (copy it to keep it)."""
+        return self.fcg.solve(_dev(f))
+
+    def compliance(self, f, x):
+        return float(_dev(f) @ x)
+
+
+def solve(shape, E, force, mask, *, ke=None, precision="mixed", tol=1e-8, maxiter=200, check_every=1, pre=2,
+          post=2, omega=0.6, max_coarse_x=16, levels=None):
+    """Host-buffer entry point: E (Ne), force and 0/1 DOF mask (3N), numpy, author layout.
+    Returns (u as numpy, dict(iterations, converged, rel, matvecs, compliance))."""
+    s = ElasticitySolver(shape, E, mask, ke=ke, precision=precision, pre=pre, post=post, omega=omega,
+                         max_coarse_x=max_coarse_x, levels=levels, tol=tol, maxiter=maxiter, check_every=check_every)
+    f = _dev(force)
+    res = s.solve(f)
+    u = res.x.cpu().numpy()
+    return u, dict(iterations=res.iterations, converged=res.converged, rel=res.rel, matvecs=res.matvecs,
+                   compliance=float(np.dot(np.asarray(force, dtype=np.float64), u)))

@@ -306,7 +306,10 @@ template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK,
 int launch_stream(const OpArgs<TC, TU, TE, TY>& a, cudaStream_t s, const char* what) {
     auto kern = parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
     constexpr size_t smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
-    static bool configured = false;          // once per instantiation (per process)
+    // dynamic (48 KB for FP64) + static (the block reduction) shared memory exceeds the 48 KB
+    // default: opt in once per instantiation.  The solvers run every loop body once un-captured
+    // before capturing it, so this call never happens inside a stream capture.
+    static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) {

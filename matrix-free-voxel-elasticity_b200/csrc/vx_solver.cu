@@ -58,10 +58,9 @@ __global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const d
     switch (op) {
         case FIN_PQ:
             S[S_PQ] = s0;
-            if (s0 == 0.0 || !isfinite(s0)) { S[S_BREAK] = 1.0; S[S_ALPHA] = 0.0; }
-            else S[S_ALPHA] = S[S_RZ] / s0;
-            S[S_IT] += 1.0;
             S[S_MV] += 1.0;
+            if (s0 == 0.0 || !isfinite(s0)) { S[S_BREAK] = 1.0; S[S_ALPHA] = 0.0; }   // no step is taken
+            else { S[S_ALPHA] = S[S_RZ] / s0; S[S_IT] += 1.0; }
             break;
         case FIN_TRUE:
             S[S_RR] = s0;
@@ -103,17 +102,20 @@ __global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __r
     if (update_r) r[i] = r[i] - a * q[i];
 }
 
-// p = z + beta p
-template <typename T>
-__global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, const T* __restrict__ z, T* __restrict__ p) {
+// p = z + beta p (z in the preconditioner's storage TZ), and z_old = z when z_old is given
+template <typename T, typename TZ>
+__global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, const TZ* __restrict__ z, T* __restrict__ p,
+                                    T* __restrict__ z_old) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    p[i] = z[i] + T(S[S_BETA]) * p[i];
+    const T zi = T(z[i]);
+    p[i] = zi + T(S[S_BETA]) * p[i];
+    if (z_old) z_old[i] = zi;
 }
 
 // partials for r . zn and r . (zn - zo), fixed grid G (a function of n), fixed order
-template <typename T>
-__global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const T* __restrict__ zn,
+template <typename T, typename TZ>
+__global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const TZ* __restrict__ zn,
                                                      const T* __restrict__ zo, double* __restrict__ partials) {
     const int64_t G = gridDim.x;
     double a = 0.0, b = 0.0;
@@ -151,7 +153,7 @@ __global__ void vcycle_entry_kernel(int64_t n, const double* __restrict__ r64, T
                                     const TM* __restrict__ invd, double omega, TM* __restrict__ x) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    TM r = rmg ? TM(r64[i]) : TM(r64[i]);
+    const TM r = TM(r64[i]);
     if (rmg) rmg[i] = r;
     x[i] = TM(omega) * invd[i] * r;
 }
@@ -171,7 +173,8 @@ __global__ void set_scalars_kernel(double* S, int first, int count, double value
 
 __global__ void condition_kernel(cudaGraphConditionalHandle h, const double* __restrict__ S) {
     if (threadIdx.x == 0) {
-        const bool go = S[S_DONE] == 0.0 && S[S_BREAK] == 0.0 && S[S_IT] < S[S_MAXIT];
+        // S[S_CHECK] = iterations per loop body: the next body must not pass maxiter
+        const bool go = S[S_DONE] == 0.0 && S[S_BREAK] == 0.0 && S[S_IT] + S[S_CHECK] <= S[S_MAXIT];
         cudaGraphSetConditional(h, go ? 1u : 0u);
     }
 }
@@ -221,26 +224,33 @@ extern "C" int vx_cg_update(int prec, int64_t n, const double* S, void* x, const
     return VX_OK;
 }
 
-extern "C" int vx_cg_direction(int prec, int64_t n, const double* S, const void* z, void* p, cudaStream_t stream) {
+extern "C" int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, const void* z, void* p, void* z_old,
+                               cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction: n must be positive");
     VX_CHECK_ARG(S && z && p, VX_ERR_NULL_POINTER, "vx_cg_direction: NULL pointer");
-    if (prec == VX_F64) cg_direction_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, S, (const double*)z, (double*)p);
-    else if (prec == VX_F32) cg_direction_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p);
-    else { set_error("vx_cg_direction: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    if (prec == VX_F64 && zprec == VX_F64)
+        cg_direction_kernel<double, double><<<nb(n, 256), 256, 0, stream>>>(n, S, (const double*)z, (double*)p, (double*)z_old);
+    else if (prec == VX_F64 && zprec == VX_F32)
+        cg_direction_kernel<double, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (double*)p, (double*)z_old);
+    else if (prec == VX_F32 && zprec == VX_F32)
+        cg_direction_kernel<float, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p, (float*)z_old);
+    else { set_error("vx_cg_direction: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cg_direction");
     return VX_OK;
 }
 
-extern "C" int vx_dots_pr(int prec, int64_t n, const void* r, const void* zn, const void* zo, double* partials,
-                          cudaStream_t stream) {
+extern "C" int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const void* zn, const void* zo,
+                          double* partials, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_dots_pr: n must be positive");
     VX_CHECK_ARG(r && zn && partials, VX_ERR_NULL_POINTER, "vx_dots_pr: NULL pointer");
     const unsigned G = unsigned(fixed_ctas(n));
-    if (prec == VX_F64)
-        dots_pr_kernel<double><<<G, FT, 0, stream>>>(n, (const double*)r, (const double*)zn, (const double*)zo, partials);
-    else if (prec == VX_F32)
-        dots_pr_kernel<float><<<G, FT, 0, stream>>>(n, (const float*)r, (const float*)zn, (const float*)zo, partials);
-    else { set_error("vx_dots_pr: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    if (prec == VX_F64 && zprec == VX_F64)
+        dots_pr_kernel<double, double><<<G, FT, 0, stream>>>(n, (const double*)r, (const double*)zn, (const double*)zo, partials);
+    else if (prec == VX_F64 && zprec == VX_F32)
+        dots_pr_kernel<double, float><<<G, FT, 0, stream>>>(n, (const double*)r, (const float*)zn, (const double*)zo, partials);
+    else if (prec == VX_F32 && zprec == VX_F32)
+        dots_pr_kernel<float, float><<<G, FT, 0, stream>>>(n, (const float*)r, (const float*)zn, (const float*)zo, partials);
+    else { set_error("vx_dots_pr: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_dots_pr");
     return VX_OK;
 }
@@ -298,8 +308,16 @@ extern "C" int vx_set_scalars(double* S, int first, int count, double value, cud
 extern "C" int vx_graph_while_begin(cudaStream_t stream, void** handle) {
     VX_CHECK_ARG(handle, VX_ERR_NULL_POINTER, "vx_graph_while_begin: NULL handle");
     VX_CHECK_ARG(stream != nullptr, VX_ERR_INVALID_ARGUMENT, "vx_graph_while_begin: capture needs a non-default stream");
+    // load the condition kernel now: with lazy module loading its first launch would otherwise
+    // happen inside the capture
+    cudaFuncAttributes attr;
+    cudaError_t e = cudaFuncGetAttributes(&attr, condition_kernel);
+    if (e != cudaSuccess) {
+        set_error("vx_graph_while_begin: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
     auto* w = new WhileGraph();
-    cudaError_t e = cudaGraphCreate(&w->graph, 0);
+    e = cudaGraphCreate(&w->graph, 0);
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&w->handle, w->graph, 1, cudaGraphCondAssignDefault);
     cudaGraphNode_t node;
     cudaGraphNodeParams p = {};
@@ -338,6 +356,13 @@ extern "C" int vx_graph_while_end(void* handle, const double* S, cudaStream_t st
         return VX_ERR_CUDA;
     }
     return VX_OK;
+}
+
+// 0: not capturing, 1: capture active, 2: capture invalidated, -1: query failed
+extern "C" int vx_capture_status(cudaStream_t stream) {
+    cudaStreamCaptureStatus st;
+    if (cudaStreamIsCapturing(stream, &st) != cudaSuccess) return -1;
+    return st == cudaStreamCaptureStatusNone ? 0 : (st == cudaStreamCaptureStatusActive ? 1 : 2);
 }
 
 extern "C" int vx_graph_launch(void* handle, cudaStream_t stream) {

@@ -1,0 +1,516 @@
+"""Device-resident solvers: the rediscretised GMG V-cycle, flexible (Polak-Ribiere) PCG with an
+FP64 outer loop, the donor's Jacobi-PCG (Fletcher-Reeves) and mixed-precision iterative
+refinement.
+
+Semantics follow the reference exactly -- src/voxel_mg.py:133-217 (Multigrid, fcg) and
+experiments/session_a/donor/src/gpu_fem/simp_r2.py:187-385 (pcg, pcg_ir) -- but every scalar
+lives on the device (a 16-slot FP64 array S), every reduction is deterministic, and the loop
+body is captured once as the body of a CUDA-graph WHILE node, so a whole solve is one graph
+launch with no host round trip per iteration (`graph=False` runs the same kernel sequence from
+the host, one iteration at a time).
+"""
+from __future__ import annotations
+
+import atexit
+import ctypes
+import sys
+import weakref
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .operators import PREC, VoxelOperator, _ptr, stream_ptr
+
+# scalar slots of S (csrc/vx_solver.cu)
+(S_RZ, S_PQ, S_ALPHA, S_RR, S_REL, S_NB, S_BETA, S_RZN, S_RZD, S_TOL, S_DONE, S_IT, S_MAXIT, S_MV,
+ S_BREAK, S_CHECK) = range(16)
+FIN_PQ, FIN_TRUE, FIN_BETA_PR, FIN_BETA_FR, FIN_NB, FIN_RZ, FIN_RR_ONLY = range(7)
+
+def hierarchy_shapes(shape, max_coarse_x=16):
+    """Halve every axis while x > max_coarse_x and all extents are even (src/voxel_mg.py:220-225)."""
+    shapes = [tuple(int(s) for s in shape)]
+    while shapes[-1][0] > max_coarse_x and all(s % 2 == 0 for s in shapes[-1]):
+        shapes.append(tuple(s // 2 for s in shapes[-1]))
+    return shapes
+
+
+def _s():
+    return stream_ptr()
+
+
+def all_free_mask(shape, device="cuda"):
+    nx, ny, nz = shape
+    return torch.full(((nx + 1) * (ny + 1) * (nz + 1),), 7, dtype=torch.uint8, device=device)
+
+
+class _Level:
+    __slots__ = ("shape", "op", "op64", "E64", "E", "mask", "invd", "omega", "r", "x", "xt", "n")
+
+
+class MGHierarchy:
+    """Rediscretised geometric multigrid (src/voxel_mg.py:1-21,74-178): level l has element matrix
+    ke * 2^l, modulus the 2x2x2 mean of level l-1, mask injected from level l-1; damped Jacobi
+    V(pre, post) in `dtype` (float64 or float32); the coarsest level is solved in FP64 with the
+    inverse of its dense constrained matrix (from an FP64 Cholesky factorisation)."""
+
+    def __init__(self, shape, ke, E, node_mask=None, dtype=torch.float32, pre=2, post=2, omegas=None,
+                 max_coarse_x=16, shapes=None):
+        if dtype not in (torch.float64, torch.float32):
+            raise ValueError("the V-cycle runs in float64 or float32")
+        self.shapes = [tuple(s) for s in (shapes or hierarchy_shapes(shape, max_coarse_x))]
+        self.dtype, self.prec, self.pre, self.post = dtype, PREC[dtype], int(pre), int(post)
+        self.ke = np.asarray(ke, dtype=np.float64).reshape(24, 24)
+        E64 = E.to(torch.float64).contiguous()
+        mask = node_mask if node_mask is not None else all_free_mask(self.shapes[0])
+        self.levels = []
+        for i, s in enumerate(self.shapes):
+            if i:
+                prev = self.shapes[i - 1]
+                Ec = torch.empty(s[0] * s[1] * s[2], dtype=torch.float64, device="cuda")
+                _lib.call("vx_coarsen_modulus", _lib.VX_F64, *prev, _ptr(E64, "E"), Ec.data_ptr(), _s())
+                mc = torch.empty((s[0] + 1) * (s[1] + 1) * (s[2] + 1), dtype=torch.uint8, device="cuda")
+                _lib.call("vx_coarsen_mask", *prev, _ptr(mask, "mask"), mc.data_ptr(), _s())
+                E64, mask = Ec, mc
+            L = _Level()
+            L.shape = s
+            L.op = VoxelOperator(s, self.ke * 2 ** i, dtype)
+            L.op64 = L.op if dtype == torch.float64 else VoxelOperator(s, self.ke * 2 ** i, torch.float64)
+            L.E64, L.mask = E64, mask
+            L.E = E64 if dtype == torch.float64 else E64.to(dtype)
+            inv64 = L.op64.diagonal(E64, mask, inverse=True)
+            L.invd = inv64 if dtype == torch.float64 else inv64.to(dtype)
+            L.n = L.op.ndof
+            L.r = torch.zeros(L.n, dtype=dtype, device="cuda")
+            L.x = torch.zeros(L.n, dtype=dtype, device="cuda")
+            L.xt = torch.zeros(L.n, dtype=dtype, device="cuda")
+            self.levels.append(L)
+        c = self.levels[-1]
+        A = torch.empty(c.n, c.n, dtype=torch.float64, device="cuda")
+        _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
+                  _ptr(c.E64, "E"), _ptr(c.mask, "mask"), A.data_ptr(), _s())
+        self.A_coarse = A
+        self.coarse_factor = torch.linalg.cholesky(A)
+        self.A_inv = torch.cholesky_inverse(self.coarse_factor).contiguous()
+        n_smooth = len(self.levels) - 1
+        if omegas is None:
+            self.omegas = [0.6] * n_smooth                      # the reference default (voxel_mg.py:148)
+            self.lambdas = None
+        elif isinstance(omegas, str) and omegas == "spectral":
+            self.omegas, self.lambdas = self.spectral_omegas()
+        elif np.isscalar(omegas):
+            self.omegas, self.lambdas = [float(omegas)] * n_smooth, None
+        else:
+            self.omegas, self.lambdas = [float(w) for w in omegas], None
+        self.set_omegas(self.omegas)
+
+    def set_omegas(self, omegas):
+        n_smooth = len(self.levels) - 1
+        if len(omegas) != n_smooth:
+            raise ValueError(f"need {n_smooth} omegas, got {len(omegas)}")
+        self.omegas = [float(w) for w in omegas]
+        for L, w in zip(self.levels, self.omegas + [0.0]):
+            L.omega = w
+
+    @property
+    def finest(self):
+        return self.levels[0]
+
+    def footprint_bytes(self) -> int:
+        b = 0
+        for L in self.levels:
+            es = torch.finfo(self.dtype).bits // 8
+            b += L.n * es * 4 + L.E.numel() * es + L.E64.numel() * 8 + L.mask.numel()
+        return b + self.A_inv.numel() * 8 * 3
+
+    def spectral_omegas(self, iterations=30, seed=20260923):
+        """omega_l = 4 / (3 lambda_l), lambda_l from a seeded FP64 power iteration on D^-1 A over the
+        free DOFs (src/voxel_mg.py:228-244).  Returns (omegas, lambdas)."""
+        omegas, lambdas = [], []
+        for L in self.levels[:-1]:
+            rng = np.random.default_rng(seed)
+            m = ((L.mask.to(torch.int32)[:, None] >> torch.arange(3, device="cuda")) & 1).reshape(-1).double()
+            v = torch.as_tensor(rng.standard_normal(L.n), device="cuda") * m
+            v = v / torch.linalg.vector_norm(v)
+            inv64 = L.op64.diagonal(L.E64, L.mask, inverse=True)
+            lam = 0.0
+            for _ in range(iterations):
+                w = inv64 * L.op64.matvec(v, L.E64, L.mask) * m
+                lam = float(torch.linalg.vector_norm(w))
+                v = w / lam
+            lambdas.append(lam)
+            omegas.append(4.0 / (3.0 * lam))
+        return omegas, lambdas
+
+    # ------------------------------------------------------------------ kernel emission
+    def emit(self, r64: torch.Tensor) -> torch.Tensor:
+        """Launch one V-cycle on the current stream: z = M(r64); returns the buffer holding z (in
+        the hierarchy's dtype).  r64 is the FP64 finest residual; it is read, never written."""
+        L0 = self.levels[0]
+        if len(self.levels) == 1:
+            src = r64
+            if self.dtype != torch.float64:
+                _lib.call("vx_cast", L0.n, _lib.VX_F64, _ptr(r64, "r"), self.prec, L0.r.data_ptr(), 1.0, _s())
+                src = L0.r
+            _lib.call("vx_coarse_apply", self.prec, L0.n, self.A_inv.data_ptr(), src.data_ptr(), L0.mask.data_ptr(),
+                      L0.x.data_ptr(), _s())
+            return L0.x
+        r0 = r64 if self.dtype == torch.float64 else L0.r
+        _lib.call("vx_vcycle_entry", self.prec, L0.n, _ptr(r64, "r"),
+                  None if self.dtype == torch.float64 else L0.r.data_ptr(), L0.invd.data_ptr(), L0.omega,
+                  L0.x.data_ptr(), _s())
+        return self._level(0, r0)
+
+    def _level(self, l, r):
+        L = self.levels[l]
+        if l == len(self.levels) - 1:
+            _lib.call("vx_coarse_apply", self.prec, L.n, self.A_inv.data_ptr(), r.data_ptr(), L.mask.data_ptr(),
+                      L.x.data_ptr(), _s())
+            return L.x
+        bufs = [L.x, L.xt]
+        ci = 0
+        for _ in range(self.pre - 1):
+            L.op.jacobi(bufs[ci], r, L.invd, L.E, L.mask, L.omega, out=bufs[1 - ci])
+            ci ^= 1
+        L.op.residual(bufs[ci], r, L.E, L.mask, out=bufs[1 - ci])
+        nxt = self.levels[l + 1]
+        _lib.call("vx_restrict", self.prec, *L.shape, bufs[1 - ci].data_ptr(), nxt.mask.data_ptr(), nxt.r.data_ptr(), _s())
+        if l + 1 < len(self.levels) - 1:
+            _lib.call("vx_scaled_product", self.prec, nxt.n, nxt.omega, nxt.invd.data_ptr(), nxt.r.data_ptr(),
+                      nxt.x.data_ptr(), _s())
+        xc = self._level(l + 1, nxt.r)
+        _lib.call("vx_prolong_add", self.prec, *L.shape, xc.data_ptr(), L.mask.data_ptr(), bufs[ci].data_ptr(), _s())
+        for _ in range(self.post):
+            L.op.jacobi(bufs[ci], r, L.invd, L.E, L.mask, L.omega, out=bufs[1 - ci])
+            ci ^= 1
+        return bufs[ci]
+
+    def __call__(self, r64):
+        """z = M(r) as a fresh FP64 tensor (the reference's Multigrid.__call__ casts back to r's dtype)."""
+        return self.emit(r64.contiguous()).to(torch.float64)
+
+
+class JacobiPreconditioner:
+    """z = inv_diag * r in FP64 (the `precondition=lambda r: inv * r` of a Jacobi-preconditioned fcg)."""
+
+    def __init__(self, op64: VoxelOperator, E64, node_mask):
+        self.dtype, self.prec = torch.float64, _lib.VX_F64
+        self.invd = op64.diagonal(E64, node_mask, inverse=True)
+        self.z = torch.zeros(op64.ndof, dtype=torch.float64, device="cuda")
+
+    def emit(self, r64):
+        _lib.call("vx_scaled_product", _lib.VX_F64, self.z.numel(), 1.0, self.invd.data_ptr(), r64.data_ptr(),
+                  self.z.data_ptr(), _s())
+        return self.z
+
+    def footprint_bytes(self):
+        return self.invd.numel() * 16
+
+
+@dataclass
+class SolveResult:
+    x: torch.Tensor
+    iterations: int
+    converged: bool
+    rel: float
+    matvecs: int
+
+    def __iter__(self):     # unpacks like the reference's (x, it, converged, rel, matvecs)
+        return iter((self.x, self.iterations, self.converged, self.rel, self.matvecs))
+
+
+_LIVE_GRAPHS = weakref.WeakSet()
+
+
+@atexit.register
+def _destroy_graphs():
+    # before the CUDA runtime tears down at process exit
+    for g in list(_LIVE_GRAPHS):
+        g.close()
+
+
+@dataclass
+class PCGResult:
+    x: torch.Tensor
+    iterations: int
+    converged: bool
+    rel: float
+
+    def __iter__(self):     # unpacks like the donor's (x, iters, converged, rel_resid)
+        return iter((self.x, self.iterations, self.converged, self.rel))
+
+
+class _GraphLoop:
+    """Owns a WHILE graph (csrc/vx_solver.cu) whose body is captured from `emit_body`.
+
+    The body is first run once un-captured: with CUDA's lazy module loading, a kernel's first
+    launch loads its module, which must not happen inside a capture.  Callers re-initialise the
+    solver state after building the graph."""
+
+    def __init__(self, stream: torch.cuda.Stream, S: torch.Tensor, emit_body):
+        self.handle = ctypes.c_void_p()
+        sp = ctypes.c_void_p(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            emit_body()                                     # warm-up (loads every kernel of the body)
+            _lib.call("vx_graph_while_begin", sp, ctypes.byref(self.handle))
+            _lib.CAPTURE_STREAM = sp
+            try:
+                emit_body()
+            finally:
+                _lib.CAPTURE_STREAM = None
+                _lib.call("vx_graph_while_end", self.handle, S.data_ptr(), sp)
+        _LIVE_GRAPHS.add(self)
+
+    def launch(self, stream):
+        _lib.call("vx_graph_launch", self.handle, ctypes.c_void_p(stream.cuda_stream))
+
+    def close(self):
+        if self.handle:
+            _lib.load().vx_graph_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        if not sys.is_finalizing():
+            self.close()
+
+
+class FCGSolver:
+    """Flexible PCG (Polak-Ribiere beta) in FP64 with the reference fcg's semantics
+    (src/voxel_mg.py:181-217): true residual every `check_every` iterations with residual
+    replacement, `fixed_iterations` mode, returns (x, it, converged, rel, matvecs).  The operator
+    is the Dirichlet form M K M + (I - M) in FP64; `precond.emit(r)` launches z = M(r)."""
+
+    def __init__(self, op64: VoxelOperator, E64, node_mask, precond, tol=1e-8, maxiter=200, check_every=5,
+                 fixed_iterations=None, graph=True):
+        if op64.dtype != torch.float64:
+            raise ValueError("the outer operator must be float64")
+        self.op, self.E, self.mask, self.M = op64, E64.contiguous(), node_mask, precond
+        self.tol, self.maxiter, self.fixed = float(tol), int(maxiter), fixed_iterations
+        self.check_every = max(1, int(check_every))
+        n = op64.ndof
+        self.n = n
+        f64 = dict(dtype=torch.float64, device="cuda")
+        self.b = torch.zeros(n, **f64)
+        self.x = torch.zeros(n, **f64)
+        self.r = torch.zeros(n, **f64)
+        self.p = torch.zeros(n, **f64)
+        self.q = torch.zeros(n, **f64)
+        self.z_old = torch.zeros(n, **f64)
+        self.S = torch.zeros(16, **f64)
+        self.S_host = torch.zeros(16, dtype=torch.float64, pin_memory=True)
+        self.G_op = op64.partials_size
+        self.G_vec = int(_lib.load().vx_solver_partials(n))
+        self.partials = torch.zeros(max(self.G_op, 2 * self.G_vec), **f64)
+        self.zprec = PREC[precond.dtype]
+        self.stream = torch.cuda.Stream()
+        self.use_graph = bool(graph)
+        self._graph = None
+        self._graph_k = None
+
+    def footprint_bytes(self) -> int:
+        return 6 * self.n * 8 + self.M.footprint_bytes() + self.E.numel() * 8
+
+    # ------------------------------------------------------------------ kernel emission
+    def _fin(self, op, G):
+        _lib.call("vx_solver_finalize", op, G, self.partials.data_ptr(), self.S.data_ptr(), _s())
+
+    def _iteration(self, check: bool):
+        op, S, pp = self.op, self.S.data_ptr(), self.partials.data_ptr()
+        op.apply_dot(self.p, self.E, self.mask, self.q, self.partials)          # q = A p, p.q
+        self._fin(FIN_PQ, self.G_op)
+        _lib.call("vx_cg_update", _lib.VX_F64, self.n, S, self.x.data_ptr(), self.p.data_ptr(), self.r.data_ptr(),
+                  self.q.data_ptr(), 0 if check else 1, _s())
+        if check:                                                                # r = b - A x (replacement)
+            op.true_residual(self.x, self.b, self.E, self.mask, self.r, self.partials)
+            self._fin(FIN_TRUE, self.G_op)
+        z = self.M.emit(self.r)
+        _lib.call("vx_dots_pr", _lib.VX_F64, self.zprec, self.n, self.r.data_ptr(), z.data_ptr(),
+                  self.z_old.data_ptr(), pp, _s())
+        self._fin(FIN_BETA_PR, self.G_vec)
+        _lib.call("vx_cg_direction", _lib.VX_F64, self.zprec, self.n, S, z.data_ptr(), self.p.data_ptr(),
+                  self.z_old.data_ptr(), _s())
+
+    def _body(self, k, checking):
+        for j in range(k):
+            self._iteration(checking and j == k - 1)
+
+    def _init(self, b):
+        S = self.S.data_ptr()
+        self.b.copy_(b)
+        self.x.zero_()
+        self.r.copy_(self.b)
+        self.p.zero_()
+        _lib.call("vx_set_scalars", S, 0, 16, 0.0, _s())
+        _lib.call("vx_set_scalars", S, S_TOL, 1, self.tol if self.fixed is None else -1.0, _s())
+        _lib.call("vx_dots_pr", _lib.VX_F64, _lib.VX_F64, self.n, self.b.data_ptr(), self.b.data_ptr(), None,
+                  self.partials.data_ptr(), _s())
+        self._fin(FIN_NB, self.G_vec)
+        z = self.M.emit(self.r)
+        _lib.call("vx_dots_pr", _lib.VX_F64, self.zprec, self.n, self.r.data_ptr(), z.data_ptr(), None,
+                  self.partials.data_ptr(), _s())
+        self._fin(FIN_RZ, self.G_vec)
+        _lib.call("vx_cg_direction", _lib.VX_F64, self.zprec, self.n, S, z.data_ptr(), self.p.data_ptr(),
+                  self.z_old.data_ptr(), _s())                                  # p = z (beta = 0), z_old = z
+
+    def _read(self):
+        self.S_host.copy_(self.S, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.S_host.numpy().copy()
+
+    def solve(self, b: torch.Tensor) -> SolveResult:
+        if b.numel() != self.n:
+            raise ValueError(f"b has {b.numel()} entries, expected {self.n}")
+        caller = torch.cuda.current_stream()
+        self.stream.wait_stream(caller)
+        checking = self.fixed is None
+        k = self.check_every if checking else 1
+        limit = self.fixed if self.fixed is not None else self.maxiter
+        full = limit // k
+        if full > 0 and self.use_graph and (self._graph is None or self._graph_k != (k, checking)):
+            self._graph = _GraphLoop(self.stream, self.S, lambda: self._body(k, checking))
+            self._graph_k = (k, checking)
+        with torch.cuda.stream(self.stream):
+            self._init(b)
+            S = self.S.data_ptr()
+            _lib.call("vx_set_scalars", S, S_MAXIT, 1, float(limit), _s())
+            _lib.call("vx_set_scalars", S, S_CHECK, 1, float(k), _s())
+            if full > 0:
+                if self.use_graph:
+                    self._graph.launch(self.stream)
+                else:
+                    for _ in range(full):
+                        self._body(k, checking)
+                        s = self._read()
+                        if s[S_DONE] or s[S_BREAK]:
+                            break
+            s = self._read()
+            done = bool(s[S_DONE])
+            it = int(s[S_IT])
+            while not done and not s[S_BREAK] and it < limit:                 # iterations past the last full body
+                self._iteration(checking and (it + 1) % k == 0)
+                s = self._read()
+                done, it = bool(s[S_DONE]), int(s[S_IT])
+            if not done:                                                       # final true residual (voxel_mg.py:213-216)
+                self.op.true_residual(self.x, self.b, self.E, self.mask, self.q, self.partials)
+                self._fin(FIN_TRUE, self.G_op)
+                s = self._read()
+        caller.wait_stream(self.stream)
+        rel = float(s[S_REL])
+        return SolveResult(self.x, int(s[S_IT]), bool(rel <= self.tol), rel, int(s[S_MV]))
+
+
+class JacobiPCG:
+    """The donor's Jacobi-preconditioned CG with a true-residual test and residual replacement every
+    `check_every` iterations, Fletcher-Reeves beta (experiments/session_a/donor/src/gpu_fem/
+    simp_r2.py:187-295), in FP64 or FP32 (`op.dtype`).  Returns (x, iters, converged, rel)."""
+
+    def __init__(self, op: VoxelOperator, E, node_mask, tol=1e-5, maxiter=20000, check_every=50, inv_diag=None,
+                 graph=True):
+        if op.dtype not in (torch.float64, torch.float32):
+            raise ValueError("Jacobi-PCG runs in float64 or float32")
+        self.op, self.E, self.mask = op, E.contiguous(), node_mask
+        self.dtype, self.prec = op.dtype, op.prec
+        self.tol, self.maxiter, self.k = float(tol), int(maxiter), max(1, int(check_every))
+        n = op.ndof
+        self.n = n
+        t = dict(dtype=self.dtype, device="cuda")
+        self.invd = inv_diag if inv_diag is not None else op.diagonal(self.E, node_mask, inverse=True)
+        self.b = torch.zeros(n, **t)
+        self.x = torch.zeros(n, **t)
+        self.r = torch.zeros(n, **t)
+        self.z = torch.zeros(n, **t)
+        self.p = torch.zeros(n, **t)
+        self.q = torch.zeros(n, **t)
+        self.S = torch.zeros(16, dtype=torch.float64, device="cuda")
+        self.S_host = torch.zeros(16, dtype=torch.float64, pin_memory=True)
+        self.G_op = op.partials_size
+        self.G_vec = int(_lib.load().vx_solver_partials(n))
+        self.partials = torch.zeros(max(self.G_op, 2 * self.G_vec), dtype=torch.float64, device="cuda")
+        self.stream = torch.cuda.Stream()
+        self.use_graph = bool(graph)
+        self._graph = None
+
+    def _fin(self, op, G):
+        _lib.call("vx_solver_finalize", op, G, self.partials.data_ptr(), self.S.data_ptr(), _s())
+
+    def _iteration(self, check):
+        op, S = self.op, self.S.data_ptr()
+        op.apply_dot(self.p, self.E, self.mask, self.q, self.partials)
+        self._fin(FIN_PQ, self.G_op)
+        _lib.call("vx_cg_update", self.prec, self.n, S, self.x.data_ptr(), self.p.data_ptr(), self.r.data_ptr(),
+                  self.q.data_ptr(), 0 if check else 1, _s())
+        if check:
+            op.true_residual(self.x, self.b, self.E, self.mask, self.r, self.partials)
+            self._fin(FIN_TRUE, self.G_op)
+        _lib.call("vx_jacobi_precond_dot", self.prec, self.n, self.invd.data_ptr(), self.r.data_ptr(),
+                  self.z.data_ptr(), self.partials.data_ptr(), _s())
+        self._fin(FIN_BETA_FR, self.G_vec)
+        _lib.call("vx_cg_direction", self.prec, self.prec, self.n, S, self.z.data_ptr(), self.p.data_ptr(), None, _s())
+
+    def _read(self):
+        self.S_host.copy_(self.S, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.S_host.numpy().copy()
+
+    def solve(self, b, x0=None, tol=None, maxiter=None):
+        tol = self.tol if tol is None else float(tol)
+        maxiter = self.maxiter if maxiter is None else int(maxiter)
+        caller = torch.cuda.current_stream()
+        self.stream.wait_stream(caller)
+        k = self.k
+        if self.use_graph and self._graph is None and maxiter // k > 0:
+            self._graph = _GraphLoop(self.stream, self.S, lambda: [self._iteration(j == k - 1) for j in range(k)])
+        with torch.cuda.stream(self.stream):
+            S = self.S.data_ptr()
+            m = self.mask
+            self.b.copy_(b)
+            if x0 is None:
+                self.x.zero_()
+            else:
+                self.x.copy_(x0)
+                if m is not None:                                   # x = x0 * mask
+                    bits = ((m.to(torch.int32)[:, None] >> torch.arange(3, device="cuda")) & 1).reshape(-1)
+                    self.x.mul_(bits.to(self.dtype))
+            _lib.call("vx_set_scalars", S, 0, 16, 0.0, _s())
+            _lib.call("vx_set_scalars", S, S_TOL, 1, tol, _s())
+            _lib.call("vx_dots_pr", self.prec, self.prec, self.n, self.b.data_ptr(), self.b.data_ptr(), None,
+                      self.partials.data_ptr(), _s())
+            self._fin(FIN_NB, self.G_vec)
+            self.op.true_residual(self.x, self.b, self.E, self.mask, self.r, self.partials)   # r = b - A x
+            self._fin(FIN_RR_ONLY, self.G_op)
+            _lib.call("vx_jacobi_precond_dot", self.prec, self.n, self.invd.data_ptr(), self.r.data_ptr(),
+                      self.z.data_ptr(), self.partials.data_ptr(), _s())
+            self._fin(FIN_RZ, self.G_vec)
+            _lib.call("vx_set_scalars", S, S_BETA, 1, 0.0, _s())
+            self.p.zero_()
+            _lib.call("vx_cg_direction", self.prec, self.prec, self.n, S, self.z.data_ptr(), self.p.data_ptr(), None, _s())
+            s = self._read()
+            if s[S_NB] <= 0:
+                return PCGResult(self.x, 0, True, 0.0)
+            if s[S_REL] <= tol:
+                return PCGResult(self.x, 0, True, float(s[S_REL]))
+            _lib.call("vx_set_scalars", S, S_MAXIT, 1, float(maxiter), _s())
+            _lib.call("vx_set_scalars", S, S_CHECK, 1, float(k), _s())
+            if maxiter // k > 0:
+                if self.use_graph:
+                    self._graph.launch(self.stream)
+                else:
+                    for _ in range(maxiter // k):
+                        for j in range(k):
+                            self._iteration(j == k - 1)
+                        s = self._read()
+                        if s[S_DONE] or s[S_BREAK]:
+                            break
+            s = self._read()
+            it = int(s[S_IT])
+            while not s[S_DONE] and not s[S_BREAK] and it < maxiter:          # tail: check at maxiter
+                self._iteration((it + 1) % k == 0 or it + 1 >= maxiter)
+                s = self._read()
+                it = int(s[S_IT])
+            if not s[S_DONE]:
+                self.op.true_residual(self.x, self.b, self.E, self.mask, self.q, self.partials)
+                self._fin(FIN_RR_ONLY, self.G_op)
+                s = self._read()
+        caller.wait_stream(self.stream)
+        return PCGResult(self.x, int(s[S_IT]), bool(s[S_DONE]), float(s[S_REL]))
