@@ -1,0 +1,426 @@
+"""Benchmark: time-to-1e-8 solve of the voxel elasticity cantilever on B200, mixed precision
+(FP32 GMG V-cycle inside the FP64 flexible CG) vs plain FP64, plus matvec GDOF/s and the
+roofline of the dominant kernel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload gmg_128x64x64|gmg_576x288x288|jacobi_32x16x16] [--no-large]
+
+One step = one complete solve (hierarchy already built, inputs resident) of the workload; the
+timed region is K steps bracketed by a barrier + synchronize, timed with CUDA events, max over
+ranks.  L2 (126 MB) is flushed by writing a 256 MB buffer between timed steps, outside the
+event bracket.  `e2e` is the same solve through the public host-buffer API (voxel_b200.solve):
+pinned host inputs in, host solution out, hierarchy setup included.  With N > 1 (torchrun) every
+rank solves its own replica of the workload (the path does not need a collective): weak scaling.
+
+`--impl reference` times the reference algorithm's CPU implementation -- the NumPy restatement
+of src/voxel_mg.py (oracle/voxel_oracle.py) -- on this host's cores, on the same workload
+(rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+WORKLOADS = {
+    # name: (shape, density spec, V-cycle levels, description)
+    "gmg_128x64x64": ((128, 64, 64), ("grf", 8.0, 0), 4,
+                      "cantilever 128x64x64 (1.64M DOF), GRF l=8 seed 0 -> [1e-3,1], E0=1 Emin=1e-9 p=3, "
+                      "4-level V(2,2) damped Jacobi omega=0.6, tol 1e-8"),
+    "gmg_576x288x288": ((576, 288, 288), ("grf", 16.0, 0), 6,
+                        "cantilever 576x288x288 (144.6M DOF), GRF l=16 seed 0 -> [1e-3,1], E0=1 Emin=1e-9 p=3, "
+                        "6-level V(2,2) damped Jacobi omega=0.6, tol 1e-8"),
+    "jacobi_32x16x16": ((32, 16, 16), ("uniform", 0), None,
+                        "cantilever 32x16x16 (28,611 DOF), uniform(0.01,1) seed 0, Jacobi-PCG, tol 1e-8"),
+}
+CHECK_EVERY = 5   # the reference fcg's default true-residual cadence
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="gmg_128x64x64")
+    ap.add_argument("--no-large", action="store_true", help="skip the 144.6M-DOF section")
+    ap.add_argument("--profile", action="store_true", help="short run for a profiler: no CPU baseline, no large")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------------- problems
+def build_inputs(name, device="cuda"):
+    import torch
+    import voxel_b200 as vx
+    shape, dens, levels, _ = WORKLOADS[name]
+    rho = vx.problems.density(dens, shape, device=device)
+    E = vx.problems.simp_modulus(rho, 1e-9)
+    mask, force = vx.problems.cantilever_equal_split(shape, device=device)
+    return shape, levels, rho, E, mask, force
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------------- timing
+def time_solves(solver, force, steps, warmup, flush, rank_sync):
+    import torch
+    for _ in range(warmup):
+        solver.solve(force)
+    torch.cuda.synchronize()
+    times, results = [], []
+    rank_sync()
+    for _ in range(steps):
+        flush.fill_(1.0)                                   # evict L2 (outside the timed bracket)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        res = solver.solve(force)
+        e.record()
+        e.synchronize()
+        times.append(s.elapsed_time(e) / 1e3)
+        results.append(res)
+    torch.cuda.synchronize()
+    rank_sync()
+    return times, results[-1]
+
+
+def kernel_time(fn, reps, flush):
+    """Average device time of one launch of fn (CUDA events on the launching stream), L2 flushed
+    before each launch, over `reps` launches."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(reps):
+        flush.fill_(1.0)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        e.synchronize()
+        tot += s.elapsed_time(e)
+    return tot / reps / 1e3
+
+
+def stream_bytes(nodes, elems, vec_bytes, e_bytes, n_vec_in, n_vec_out, mask=True):
+    """Algorithmic HBM bytes of one streaming-operator launch: each array crosses HBM once."""
+    return nodes * 3 * vec_bytes * (n_vec_in + n_vec_out) + elems * e_bytes + (nodes if mask else 0)
+
+
+def kernel_table(solver, vx, torch, flush, reps=10):
+    """Per-kernel device time and algorithmic bytes of the hot kernels on the solver's own data."""
+    fcg, M = solver.fcg, solver.M
+    op64 = fcg.op
+    N, Ne = op64.nodes, op64.n_elem
+    rows = {}
+    tmp = torch.zeros_like(fcg.x)
+    t = kernel_time(lambda: op64.apply_dot(fcg.p, fcg.E, fcg.mask, fcg.q, fcg.partials), reps, flush)
+    rows["apply_dot_f64"] = (t, stream_bytes(N, Ne, 8, 8, 1, 1))
+    t = kernel_time(lambda: op64.true_residual(fcg.x, fcg.b, fcg.E, fcg.mask, tmp, fcg.partials), reps, flush)
+    rows["true_residual_f64"] = (t, stream_bytes(N, Ne, 8, 8, 2, 1))
+    if hasattr(M, "levels") and len(M.levels) > 1:
+        L = M.levels[0]
+        es = 4 if M.dtype == torch.float32 else 8
+        name = "f32" if es == 4 else "f64"
+        t = kernel_time(lambda: L.op.jacobi(L.x, L.r, L.invd, L.E, L.mask, L.omega, out=L.xt), reps, flush)
+        rows[f"jacobi_sweep_{name}"] = (t, stream_bytes(N, Ne, es, es, 3, 1))
+        t = kernel_time(lambda: L.op.residual(L.x, L.r, L.E, L.mask, out=L.xt), reps, flush)
+        rows[f"residual_{name}"] = (t, stream_bytes(N, Ne, es, es, 2, 1))
+    return rows
+
+
+# ----------------------------------------------------------------------------------- arms
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    import voxel_b200 as vx
+    from voxel_b200 import _lib
+    from voxel_b200.api import ElasticitySolver
+
+    def rank_sync():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MB > L2
+    shape, levels, rho, E, mask, force = build_inputs(args.workload)
+    precision = "jacobi" if levels is None else "mixed"
+    kw = dict(tol=1e-8, maxiter=5000 if levels is None else 200, check_every=50 if levels is None else CHECK_EVERY)
+    if levels is not None:
+        kw.update(pre=2, post=2, omega=0.6, levels=levels)
+    solver = ElasticitySolver(shape, E, mask, precision=precision, **kw)
+
+    hbm, peak_kind = peaks()
+    with ClockSampler(local_rank) as clocks:
+        launches0 = _lib.launches
+        times, res = time_solves(solver, force, args.steps, args.warmup, flush, rank_sync)
+        launches = (_lib.launches - launches0)
+    launches_per_solve = launches // (args.steps + args.warmup)
+    t_local = float(np.mean(times))
+    t_max = t_local
+    if world > 1:
+        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt)
+    compliance = float(force @ res.x)
+    out = {"metric": "time-to-1e-8 solve, mixed-precision GMG-PCG (FP32 V-cycle in FP64 flexible CG)"
+                     if levels is not None else "time-to-1e-8 solve, FP64 Jacobi-PCG",
+           "value": t_max / world, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t_max * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64 outer / f32 preconditioner" if levels is not None else "f64", "data": "synthetic",
+           "config": {"workload": args.workload, "description": WORKLOADS[args.workload][3],
+                      "check_every": kw["check_every"], "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                      "l2": "flushed (256 MB write) between timed steps"},
+           "solve": {"iterations": res.iterations, "converged": res.converged, "rel_residual": res.rel,
+                     "matvecs": res.matvecs, "compliance": compliance, "step_s": times},
+           "gpu_launches": int(launches_per_solve * args.steps)}
+
+    # FP64 arm (same hierarchy shapes, FP64 V-cycle)
+    if levels is not None:
+        s64 = ElasticitySolver(shape, E, mask, precision="fp64", **kw)
+        times64, r64 = time_solves(s64, force, args.steps, args.warmup, flush, rank_sync)
+        out["fp64"] = {"value": float(np.mean(times64)), "iterations": r64.iterations,
+                       "compliance": float(force @ r64.x), "rel_residual": r64.rel}
+        out["speedup_mixed_vs_fp64"] = float(np.mean(times64)) / t_local
+        del s64
+
+    # roofline of the dominant kernel (largest share of one solve) on the solver's own data
+    table = kernel_table(solver, vx, torch, flush)
+    counts = per_solve_counts(solver, res, levels)
+    share = {k: table[k][0] * counts.get(k, 0) for k in table}
+    dom = max(share, key=share.get)
+    t_dom, b_dom = table[dom]
+    out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": b_dom / t_dom / 1e9, "peak": hbm, "unit": "GB/s",
+                       "frac": b_dom / t_dom / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind,
+                       "bytes_per_launch": b_dom, "launch_s": t_dom,
+                       "kernels": {k: {"launch_us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9,
+                                       "per_solve": counts.get(k, 0)} for k, v in table.items()}}
+    out["matvec"] = {"GDOF/s_f64_apply": 3 * solver.op64.nodes / table["apply_dot_f64"][0] / 1e9}
+    out["clocks"] = clocks.summary()
+
+    # e2e through the public host-buffer API (pinned inputs, setup + solve + result read back)
+    Eh = E.cpu().pin_memory()
+    fh = force.cpu().pin_memory()
+    mh = mask.cpu().pin_memory()
+    e2e = []
+    api_kw = dict(kw)
+    api_kw.pop("levels", None)
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, info = vx.solve(shape, Eh, fh, mh, precision=precision, levels=levels, **api_kw)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    out["e2e"] = {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(Eh.numel() * 8 + fh.numel() * 8 + mh.numel() * 8),
+                  "d2h_bytes_per_step": int(fh.numel() * 8), "includes": "H2D of E/force/mask, hierarchy setup, solve, D2H of u",
+                  "compliance": info["compliance"]}
+
+    if rank == 0 and world == 1 and not args.profile and not args.no_large and args.workload != "gmg_576x288x288":
+        del solver
+        torch.cuda.empty_cache()
+        out["large"] = large_section(args, flush, rank_sync)
+    if rank == 0 and world == 1 and not args.profile and args.workload != "gmg_576x288x288":
+        out["cpu_baseline"] = cpu_baseline(args.workload)
+    return out
+
+
+def per_solve_counts(solver, res, levels):
+    it = res.iterations
+    if levels is None:
+        return {"apply_dot_f64": it, "true_residual_f64": it // 50 + 1}
+    k = solver.fcg.check_every
+    checks = it // k + (0 if it % k == 0 else 1)
+    M = solver.M
+    n_sweeps = (M.pre - 1) + M.post
+    name = "f32" if M.dtype.itemsize == 4 else "f64"
+    return {"apply_dot_f64": it, "true_residual_f64": checks, f"jacobi_sweep_{name}": (it + 1) * n_sweeps,
+            f"residual_{name}": it + 1}
+
+
+def large_section(args, flush, rank_sync):
+    """144.6M-DOF grid: mixed vs FP64 time-to-1e-8, and the FP64/FP32 matvec bandwidth."""
+    import torch
+    import voxel_b200 as vx
+    from voxel_b200.api import ElasticitySolver
+    name = "gmg_576x288x288"
+    shape, levels, rho, E, mask, force = build_inputs(name)
+    del rho
+    kw = dict(tol=1e-8, maxiter=200, check_every=CHECK_EVERY, pre=2, post=2, omega=0.6, levels=levels)
+    hbm, _ = peaks()
+    out = {"workload": name, "description": WORKLOADS[name][3]}
+    steps, warm = max(2, min(args.steps, 3)), 1
+    for prec in ("mixed", "fp64"):
+        s = ElasticitySolver(shape, E, mask, precision=prec, **kw)
+        times, res = time_solves(s, force, steps, warm, flush, rank_sync)
+        out[prec] = {"s": float(np.mean(times)), "iterations": res.iterations, "rel": res.rel,
+                     "compliance": float(force @ res.x)}
+        if prec == "mixed":
+            table = kernel_table(s, vx, torch, flush, reps=5)
+            out["kernels"] = {k: {"launch_ms": v[0] * 1e3, "GB/s": v[1] / v[0] / 1e9, "frac_hbm": v[1] / v[0] / 1e9 / hbm}
+                              for k, v in table.items()}
+            N = s.op64.nodes
+            out["matvec_f64_GDOF/s"] = 3 * N / table["apply_dot_f64"][0] / 1e9
+        del s
+        torch.cuda.empty_cache()
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["s"] / out["mixed"]["s"]
+    # raw FP32 and BF16-storage matvecs
+    op32 = vx.VoxelOperator(shape, vx.quadrature([1, 1, 1], 0.3), torch.float32)
+    u32 = torch.randn(op32.ndof, device="cuda", dtype=torch.float32)
+    E32 = E.float()
+    y32 = torch.empty_like(u32)
+    t = kernel_time(lambda: op32.matvec(u32, E32, out=y32), 5, flush)
+    out["matvec_f32"] = {"ms": t * 1e3, "GDOF/s": op32.ndof / t / 1e9,
+                         "GB/s": stream_bytes(op32.nodes, op32.n_elem, 4, 4, 1, 1, mask=False) / t / 1e9}
+    del op32, u32, E32, y32
+    torch.cuda.empty_cache()
+    return out
+
+
+def cpu_baseline(workload, timed=True):
+    """The reference algorithm's NumPy path (oracle restatement of src/voxel_mg.py) on this host,
+    same workload: one full solve (about 10-30 s on 8 cores for the 128x64x64 case)."""
+    sys.path.insert(0, str(REPO))
+    from oracle import voxel_oracle as vo
+    shape, dens, levels, _ = WORKLOADS[workload]
+    if dens[0] == "grf":
+        rho = vo.gaussian_random_field(shape, dens[1], dens[2])
+    else:
+        rho = np.random.default_rng(dens[1]).uniform(0.01, 1.0, int(np.prod(shape)))
+    E = vo.simp_modulus(rho, 1e-9)
+    mask, force = vo.cantilever_equal_split(shape)
+    ke = vo.quadrature([1, 1, 1], 0.3)
+    A = lambda u: vo.apply_dirichlet(shape, ke, E, mask, u)
+    t0 = time.perf_counter()
+    if levels is None:
+        inv = 1 / np.where(mask != 0, vo.product_diagonal(shape, ke, E), 1.0)
+        x, it, ok, rel, mv = vo.fcg(A, force, lambda v: inv * v, 1e-8, 5000, check_every=50)
+        sample = "one full Jacobi-PCG solve (fcg, check_every 50)"
+    else:
+        shapes = vo.hierarchy_shapes(shape, 16)[:levels]
+        fac = vo.coarse_factor(shapes, ke, E, mask)
+        M = vo.Multigrid(shapes, ke, E, mask, fac, np.float32, pre=2, post=2)
+        x, it, ok, rel, mv = vo.fcg(A, force, M, 1e-8, 200, check_every=CHECK_EVERY)
+        sample = "one full mixed (FP32 V-cycle) GMG-FCG solve incl. hierarchy setup"
+    dt = time.perf_counter() - t0
+    try:
+        from threadpoolctl import threadpool_info
+        cores = max([i.get("num_threads", 1) for i in threadpool_info()] + [1])
+    except Exception:
+        cores = os.cpu_count()
+    return {"value": dt, "unit": "s", "cores": cores, "kind": "port", "sample": sample,
+            "iterations": it, "rel_residual": rel, "compliance": float(force @ x),
+            "host_cpus": os.cpu_count()}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    times = []
+    for i in range(args.warmup + args.steps):
+        if i < args.warmup:
+            continue            # the NumPy path has no warm-up state; warm-up steps are skipped
+        r = cpu_baseline(args.workload)
+        times.append(r["value"])
+    v = float(np.mean(times))
+    r["value"] = v
+    shape, _, levels, desc = WORKLOADS[args.workload]
+    return {"impl": "reference", "metric": "time-to-1e-8 solve, mixed-precision GMG-PCG (FP32 V-cycle in FP64 flexible CG)"
+            if levels is not None else "time-to-1e-8 solve, FP64 Jacobi-PCG", "value": v, "unit": "s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner",
+            "data": "synthetic", "config": {"workload": args.workload, "description": desc, "check_every": CHECK_EVERY},
+            "cpu_baseline": r, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_s": times}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_b200(args, rank, world, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

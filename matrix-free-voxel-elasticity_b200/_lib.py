@@ -107,10 +107,21 @@ def check(status: int, what: str = "") -> None:
 # that the capture is still valid, so the first operation that invalidates it is named.
 CAPTURE_STREAM = None
 
+# Kernel launches issued by each entry point (entry points not listed launch none or one:
+# host-only entry points are in HOST_ONLY).  Used to count this library's launches.
+KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1}
+HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
+             "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
+             "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch"}
+launches = 0          # kernels launched directly (graph launches are counted by the solvers)
+
 
 def call(name: str, *args) -> None:
+    global launches
     lib = load()
     check(getattr(lib, name)(*args), name)
+    if name not in HOST_ONLY:
+        launches += KERNELS_PER_CALL.get(name, 1)
     if CAPTURE_STREAM is not None and lib.vx_capture_status(CAPTURE_STREAM) == 2:
         raise RuntimeError(f"{name} invalidated the stream capture")
 

@@ -37,7 +37,7 @@ class ElasticitySolver:
         self.shape = tuple(int(s) for s in shape)
         self.ke = quadrature([1.0, 1.0, 1.0], 0.3) if ke is None else np.asarray(ke, dtype=np.float64).reshape(24, 24)
         self.E = _dev(E)
-        m = mask if isinstance(mask, torch.Tensor) else _dev(mask)
+        m = mask.to("cuda", non_blocking=True) if isinstance(mask, torch.Tensor) else _dev(mask)
         self.node_mask = m.contiguous() if m.dtype == torch.uint8 else node_mask_from_dofs(m.to(torch.float64))
         self.op64 = VoxelOperator(self.shape, self.ke, torch.float64)
         self.precision = precision

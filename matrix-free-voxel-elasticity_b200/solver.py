@@ -255,15 +255,23 @@ class _GraphLoop:
             emit_body()                                     # warm-up (loads every kernel of the body)
             _lib.call("vx_graph_while_begin", sp, ctypes.byref(self.handle))
             _lib.CAPTURE_STREAM = sp
+            before = _lib.launches
             try:
                 emit_body()
             finally:
                 _lib.CAPTURE_STREAM = None
+                # kernels per body execution, plus the condition kernel
+                self.body_kernels = _lib.launches - before + 1
+                _lib.launches = before
                 _lib.call("vx_graph_while_end", self.handle, S.data_ptr(), sp)
         _LIVE_GRAPHS.add(self)
 
     def launch(self, stream):
         _lib.call("vx_graph_launch", self.handle, ctypes.c_void_p(stream.cuda_stream))
+
+    def account(self, bodies: int):
+        """Add the kernels of `bodies` executions of the loop body to the launch counter."""
+        _lib.launches += int(bodies) * self.body_kernels
 
     def close(self):
         if self.handle:
@@ -387,6 +395,8 @@ class FCGSolver:
             s = self._read()
             done = bool(s[S_DONE])
             it = int(s[S_IT])
+            if full > 0 and self.use_graph:
+                self._graph.account(max(1, -(-it // k)))
             while not done and not s[S_BREAK] and it < limit:                 # iterations past the last full body
                 self._iteration(checking and (it + 1) % k == 0)
                 s = self._read()
@@ -504,6 +514,8 @@ class JacobiPCG:
                             break
             s = self._read()
             it = int(s[S_IT])
+            if maxiter // k > 0 and self.use_graph:
+                self._graph.account(max(1, -(-it // k)))
             while not s[S_DONE] and not s[S_BREAK] and it < maxiter:          # tail: check at maxiter
                 self._iteration((it + 1) % k == 0 or it + 1 >= maxiter)
                 s = self._read()
