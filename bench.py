@@ -40,6 +40,9 @@ WORKLOADS = {
     "gmg_576x288x288": ((576, 288, 288), ("grf", 16.0, 0), 6,
                         "cantilever 576x288x288 (144.6M DOF), GRF l=16 seed 0 -> [1e-3,1], E0=1 Emin=1e-9 p=3, "
                         "6-level V(2,2) damped Jacobi omega=0.6, tol 1e-8"),
+    "gmg_256x128x128": ((256, 128, 128), ("grf", 8.0, 0), 5,
+                        "cantilever 256x128x128 (12.7M DOF), GRF l=8 seed 0 -> [1e-3,1], E0=1 Emin=1e-9 p=3, "
+                        "5-level V(2,2) damped Jacobi omega=0.6, tol 1e-8"),
     "jacobi_32x16x16": ((32, 16, 16), ("uniform", 0), None,
                         "cantilever 32x16x16 (28,611 DOF), uniform(0.01,1) seed 0, Jacobi-PCG, tol 1e-8"),
 }
@@ -55,6 +58,8 @@ def parse():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="gmg_128x64x64")
     ap.add_argument("--no-large", action="store_true", help="skip the 144.6M-DOF section")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler: no CPU baseline, no large")
+    ap.add_argument("--kernels", action="store_true",
+                    help="only launch the hot kernels on the workload's data (for an ncu capture); prints their times")
     return ap.parse_args()
 
 
@@ -132,6 +137,7 @@ def time_solves(solver, force, steps, warmup, flush, rank_sync):
     torch.cuda.synchronize()
     times, results = [], []
     rank_sync()
+    torch.cuda.nvtx.range_push("timed")                   # ncu --nvtx --nvtx-include timed/
     for _ in range(steps):
         flush.fill_(1.0)                                   # evict L2 (outside the timed bracket)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -141,6 +147,7 @@ def time_solves(solver, force, steps, warmup, flush, rank_sync):
         e.synchronize()
         times.append(s.elapsed_time(e) / 1e3)
         results.append(res)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     rank_sync()
     return times, results[-1]
@@ -397,8 +404,25 @@ def run_reference(args, rank):
             "step_s": times}
 
 
+def run_kernels(args):
+    """Hot kernels only, on the workload's solver data: 3 launches each (for ncu -k/-c captures)."""
+    import torch
+    import voxel_b200 as vx
+    from voxel_b200.api import ElasticitySolver
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    shape, levels, rho, E, mask, force = build_inputs(args.workload)
+    s = ElasticitySolver(shape, E, mask, precision="mixed", levels=levels, pre=2, post=2, omega=0.6)
+    # launch order of the streaming operator: apply_dot f64 x4, true_residual f64 x4, jacobi f32 x4,
+    # residual f32 x4 (one warm-up + 3 timed each)
+    table = kernel_table(s, vx, torch, flush, reps=3)
+    print(json.dumps({k: {"us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9} for k, v in table.items()}))
+
+
 def main():
     args = parse()
+    if args.kernels:
+        run_kernels(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

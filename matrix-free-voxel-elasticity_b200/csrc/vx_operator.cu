@@ -26,7 +26,7 @@ namespace vx {
 constexpr int NW = 16;          // warps per CTA (node rows incl. 2 halo rows)
 constexpr int TYR = NW - 2;     // owned node rows per CTA
 constexpr int TZ = 30;          // owned node columns per CTA
-constexpr int CX = 32;          // owned node planes per CTA (x chunk)
+constexpr int CX_MAX = 32;      // owned node planes per CTA (x chunk), upper bound
 
 enum Epi { EPI_RAW = 0, EPI_JACOBI = 1, EPI_RESIDUAL = 2, EPI_TRUE_RES = 3, EPI_APPLY_DOT = 4 };
 enum MaskKind { MASK_NONE = 0, MASK_NODE = 1, MASK_DOF = 2 };
@@ -44,6 +44,7 @@ struct OpArgs {
     TC omega;
     double* partials;         // TRUE_RES (|res|^2) / APPLY_DOT (p.q): one double per CTA
     double emin, de, penal;   // SIMP modulus E = emin + de * rho^penal
+    int cx;                   // owned node planes per CTA (x chunk)
     BlocksT<TC> C;
 };
 
@@ -86,8 +87,8 @@ parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
     const Grid g = a.g;
     const int iz = blockIdx.x * TZ - 1 + lane;
     const int iy = blockIdx.y * TYR - 1 + row;
-    const int x0 = blockIdx.z * CX;
-    const int x1 = min(x0 + CX, g.nx + 1);                 // owned node planes [x0, x1)
+    const int x0 = blockIdx.z * a.cx;
+    const int x1 = min(x0 + a.cx, g.nx + 1);               // owned node planes [x0, x1)
     const bool in_node = iy >= 0 && iy <= g.ny && iz >= 0 && iz <= g.nz;
     const bool owner = in_node && lane >= 1 && lane <= TZ && row >= 1 && row <= TYR;
     const bool elem_ok = iy >= 0 && iy < g.ny && iz >= 0 && iz < g.nz && lane < 31 && row < NW - 1;
@@ -293,17 +294,27 @@ parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
 #undef HS
 }
 
-inline dim3 stream_grid(const Grid& g) {
-    return dim3((g.nz + 1 + TZ - 1) / TZ, (g.ny + 1 + TYR - 1) / TYR, (g.nx + 1 + CX - 1) / CX);
+// x-chunk: the longest chunk (least halo recomputation) that still gives >= 4 CTAs per SM
+inline int stream_cx(const Grid& g) {
+    const int64_t yz = int64_t((g.nz + 1 + TZ - 1) / TZ) * ((g.ny + 1 + TYR - 1) / TYR);
+    int cx = CX_MAX;
+    while (cx > 4 && yz * ((g.nx + 1 + cx - 1) / cx) < 4 * 148) cx /= 2;
+    return cx;
+}
+
+inline dim3 stream_grid(const Grid& g, int cx) {
+    return dim3((g.nz + 1 + TZ - 1) / TZ, (g.ny + 1 + TYR - 1) / TYR, (g.nx + 1 + cx - 1) / cx);
 }
 
 int64_t stream_ctas(const Grid& g) {
-    dim3 d = stream_grid(g);
+    dim3 d = stream_grid(g, stream_cx(g));
     return int64_t(d.x) * d.y * d.z;
 }
 
 template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP>
-int launch_stream(const OpArgs<TC, TU, TE, TY>& a, cudaStream_t s, const char* what) {
+int launch_stream(const OpArgs<TC, TU, TE, TY>& a_in, cudaStream_t s, const char* what) {
+    OpArgs<TC, TU, TE, TY> a = a_in;
+    a.cx = stream_cx(a.g);
     auto kern = parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
     constexpr size_t smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
     // dynamic (48 KB for FP64) + static (the block reduction) shared memory exceeds the 48 KB
@@ -318,7 +329,7 @@ int launch_stream(const OpArgs<TC, TU, TE, TY>& a, cudaStream_t s, const char* w
         }
         configured = true;
     }
-    kern<<<stream_grid(a.g), NW * 32, smem, s>>>(a);
+    kern<<<stream_grid(a.g, a.cx), NW * 32, smem, s>>>(a);
     VX_CHECK_LAUNCH(what);
     return VX_OK;
 }
