@@ -199,6 +199,21 @@ int vx_true_residual(int prec, int nx, int ny, int nz, const double* blocks, con
                      cudaStream_t stream);
 int vx_reduce_partials(int64_t G, int count, const double* partials, double* out, cudaStream_t stream);
 
+/* res = b - A x and *norm2 = sum res^2 (a device double), like vx_true_residual followed by
+ * vx_reduce_partials, but needing no scratch buffer from the caller: for code that may not
+ * allocate device memory (a request loop that must never call cudaMalloc mid-flight, a plugin
+ * inside another framework's memory arena, a process under a hard memory cap).  The partial sums
+ * live in a fixed array compiled into the library: 16384 doubles (128 KiB) on every device that
+ * loads it, kept until the process exits.  Grids that need more than 16384 CTA partials
+ * (vx_operator_partials) are rejected with VX_ERR_INVALID_ARGUMENT.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the one array: calls whose executions overlap on the GPU
+ * (different streams, concurrent host threads) race and must be serialised by the caller.
+ * No counterpart in the reference (it allocates every temporary through CuPy). */
+int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                             const uint8_t* node_mask, const void* x, const void* b, void* res,
+                             double* norm2, cudaStream_t stream);
+
 /* ---------------------------------------------------------------------------- device-scalar solvers
  * The Krylov loops of the reference (src/voxel_mg.py:181-217 fcg; donor simp_r2.py:187-295 pcg) with
  * every scalar in a device array S of vx_solver_slots() doubles:

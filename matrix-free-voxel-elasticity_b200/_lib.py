@@ -49,6 +49,7 @@ SIGNATURES = {
     "vx_partials_size": (c_int64, [c_int64]),
     "vx_dots": (c_int, [c_int, c_int64, c_int, POINTER(c_void_p), POINTER(c_void_p), _P, _P, _P]),
     "vx_reduce_partials": (c_int, [c_int64, c_int, _P, _P, _P]),
+    "vx_true_residual_noalloc": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
     "vx_axpby": (c_int, [c_int, c_int64, c_double, _P, c_double, _P, _P]),
     "vx_cast": (c_int, [c_int64, c_int, _P, c_int, _P, c_double, _P]),
     # solver kernels with device-resident scalars and WHILE graphs
@@ -109,7 +110,7 @@ CAPTURE_STREAM = None
 
 # Kernel launches issued by each entry point (entry points not listed launch none or one:
 # host-only entry points are in HOST_ONLY).  Used to count this library's launches.
-KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1}
+KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2}
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch"}

@@ -677,3 +677,69 @@ extern "C" int vx_true_residual(int prec, int nx, int ny, int nz, const double* 
     return fused_dispatch<EPI_TRUE_RES>("vx_true_residual", prec, nx, ny, nz, blocks, E, node_mask, x, b,
                                         nullptr, 0.0, res, partials, stream);
 }
+
+// ----------------------------------------------------------------------------- allocation-free form
+// Callers that cannot allocate device memory -- a serving loop that must not call cudaMalloc while
+// requests are in flight, a plugin living inside another framework's memory arena, a process under
+// a hard device-memory cap -- get one entry point that needs no scratch buffer from them:
+// vx_true_residual_noalloc keeps the per-CTA partial sums of |b - A x|^2 in a fixed device array
+// compiled into this library (NOALLOC_MAX_CTAS doubles = 128 KiB, resident on every device that
+// loads the library until the process exits).
+#include <mutex>
+
+namespace vx {
+constexpr int64_t NOALLOC_MAX_CTAS = 16384;
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_CTAS];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_noalloc_mutex;
+
+// Device address of g_noalloc_partials on the current device, looked up once per device.  In host
+// code the array's name is only a host-side stand-in, so kernels must be given this address.
+static int noalloc_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("vx_true_residual_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        set_error("vx_true_residual_noalloc: device %d is beyond the %d supported", dev, NOALLOC_MAX_DEVICES);
+        return VX_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || p == nullptr) {
+            set_error("vx_true_residual_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            return VX_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return VX_OK;
+}
+}  // namespace vx
+
+extern "C" int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                                        const uint8_t* node_mask, const void* x, const void* b, void* res,
+                                        double* norm2, cudaStream_t stream) {
+    int st = check_grid(nx, ny, nz);
+    if (st) return st;
+    VX_CHECK_ARG(blocks && E && x && b && res && norm2, VX_ERR_NULL_POINTER,
+                 "vx_true_residual_noalloc: NULL pointer");
+    const int64_t G = stream_ctas(Grid{nx, ny, nz});
+    VX_CHECK_ARG(G <= NOALLOC_MAX_CTAS, VX_ERR_INVALID_ARGUMENT,
+                 "vx_true_residual_noalloc: grid (%d, %d, %d) needs %lld partial sums but the built-in scratch "
+                 "holds %lld; use vx_true_residual with a caller-provided buffer",
+                 nx, ny, nz, (long long)G, (long long)NOALLOC_MAX_CTAS);
+    double* scratch = nullptr;
+    st = noalloc_scratch(&scratch);
+    if (st) return st;
+    // every CTA overwrites its own slot before the reduction reads it: nothing needs clearing
+    st = fused_dispatch<EPI_TRUE_RES>("vx_true_residual_noalloc", prec, nx, ny, nz, blocks, E, node_mask, x, b,
+                                      nullptr, 0.0, res, scratch, stream);
+    if (st) return st;
+    return vx_reduce_partials(G, 1, scratch, norm2, stream);
+}
