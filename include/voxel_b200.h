@@ -188,10 +188,10 @@ int vx_cast(int64_t n, int src_prec, const void* src, int dst_prec, void* dst, d
 /* Operator forms fused with the outer Krylov loop (FP64/FP32, author layout, node mask optional):
  *   vx_apply_dot:     q = A p and partials[cta] = sum p.q over the CTA's owned nodes
  *   vx_true_residual: res = b - A x and partials[cta] = sum res^2
- * `partials` holds vx_operator_partials(nx, ny, nz) doubles; sum them with vx_reduce_partials or
+ * `partials` holds vx_operator_partials(prec, nx, ny, nz) doubles; sum them with vx_reduce_partials or
  * vx_solver_finalize.  Replace the `apply_A(p)` + `p @ q` and `b - apply_A(x)` + `norm` pairs of
  * src/voxel_mg.py:192-203 and donor simp_r2.py:255-270. */
-int64_t vx_operator_partials(int nx, int ny, int nz);
+int64_t vx_operator_partials(int prec, int nx, int ny, int nz);
 int vx_apply_dot(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
                  const uint8_t* node_mask, const void* p, void* q, double* partials, cudaStream_t stream);
 int vx_true_residual(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
@@ -205,7 +205,7 @@ int vx_reduce_partials(int64_t G, int count, const double* partials, double* out
  * inside another framework's memory arena, a process under a hard memory cap).  The partial sums
  * live in a fixed array compiled into the library: 16384 doubles (128 KiB) on every device that
  * loads it, kept until the process exits.  Grids that need more than 16384 CTA partials
- * (vx_operator_partials) are rejected with VX_ERR_INVALID_ARGUMENT.  The first call on each device
+ * (vx_operator_partials(prec, ...)) are rejected with VX_ERR_INVALID_ARGUMENT.  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress); make that first call before any
  * stream capture.  All calls share the one array: calls whose executions overlap on the GPU
  * (different streams, concurrent host threads) race and must be serialised by the caller.

@@ -36,7 +36,7 @@ SIGNATURES = {
     "vx_simp_modulus": (c_int, [c_int, c_int64, _P, c_double, c_double, c_double, _P, _P]),
     "vx_jacobi_sweep": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, c_double, _P, _P]),
     "vx_residual": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P]),
-    "vx_operator_partials": (c_int64, [c_int, c_int, c_int]),
+    "vx_operator_partials": (c_int64, [c_int, c_int, c_int, c_int]),
     "vx_apply_dot": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P]),
     "vx_true_residual": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
     "vx_restrict": (c_int, [c_int, c_int, c_int, c_int, _P, _P, _P, _P]),

@@ -51,16 +51,26 @@ int check_grid(int nx, int ny, int nz);
 
 // ---------------------------------------------------------------------------- storage conversion
 template <typename S> struct Storage;
+// load: value in arithmetic type; raw/cvt: load without touching the value, convert at use
 template <> struct Storage<double> {
+    using raw_t = double;
     __device__ static double load(const double* p) { return *p; }
+    __device__ static double raw(const double* p) { return *p; }
+    __device__ static double cvt(double v) { return v; }
     __device__ static void store(double* p, double v) { *p = v; }
 };
 template <> struct Storage<float> {
+    using raw_t = float;
     __device__ static float load(const float* p) { return *p; }
+    __device__ static float raw(const float* p) { return *p; }
+    __device__ static float cvt(float v) { return v; }
     __device__ static void store(float* p, float v) { *p = v; }
 };
 template <> struct Storage<__nv_bfloat16> {
+    using raw_t = __nv_bfloat16;
     __device__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ static __nv_bfloat16 raw(const __nv_bfloat16* p) { return *p; }
+    __device__ static float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
     __device__ static void store(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 

@@ -17,8 +17,10 @@
 // dense_gather: the reference's node-owned dense 24x24 mapping (independent control path).
 // diag / energy / coarse-grid helpers.
 #include "vx_common.cuh"
+#include "vx_pair.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 
 namespace vx {
@@ -294,32 +296,638 @@ parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
 #undef HS
 }
 
-// x-chunk: the longest chunk (least halo recomputation) that still gives >= 4 CTAs per SM
-inline int stream_cx(const Grid& g) {
-    const int64_t yz = int64_t((g.nz + 1 + TZ - 1) / TZ) * ((g.ny + 1 + TYR - 1) / TYR);
+
+// ============================================================================= parity_stream2
+// Second-generation streaming operator: each thread owns TWO consecutive z node columns and the two
+// elements starting at them, processed as a pair (packed f32x2 arithmetic in FP32).  A warp covers
+// 64 z columns (62 owned), so the z-direction shuffle exchange is halved per element and addressing
+// and loop overheads are shared by two elements.  The plane loop is unrolled by two with two
+// prefetch register sets, so every plane's loads are issued two steps before they are used.  The
+// halo warp (last row) only supplies its x-stage to the row above it and skips all element work.
+// Same algebra, ownership and determinism as parity_stream.
+template <typename TC> struct Stream2Cfg;
+template <> struct Stream2Cfg<float> { static constexpr int NW = 12; };
+template <> struct Stream2Cfg<double> { static constexpr int NW = 8; };
+constexpr int TZ2 = 62;                        // owned node columns per CTA (64 per warp, 2 per lane)
+
+template <typename TC> struct Blocks2 { typename Coef<TC>::type c[72]; };
+
+template <typename TC, typename TU, typename TE, typename TY>
+struct OpArgs2 {
+    OpArgs<TC, TU, TE, TY> a;
+    Blocks2<TC> C2;
+};
+
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
+struct Stream2 {
+    static constexpr int NWS = Stream2Cfg<TC>::NW;
+    static constexpr int TYS = NWS - 2;
+    using P = V2<TC>;
+    using Raw = typename Storage<TY>::raw_t;
+    // raw loads of one node plane (two columns) and the element plane after it
+    struct Plane {
+        typename Storage<TU>::raw_t u0[3], u1[3];
+        typename Storage<TE>::raw_t e0, e1;
+        uint8_t m0, m1;
+    };
+};
+
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
+__global__ void __launch_bounds__(Stream2Cfg<TC>::NW * 32, 1)
+parity_stream2(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
+    using S2 = Stream2<TC, TU, TE, TY, EPI, MASK>;
+    constexpr int NWS = S2::NWS;
+    constexpr int TYS = S2::TYS;
+    using P = typename S2::P;
+    using Plane = typename S2::Plane;
+    const auto& a = args.a;
+    const int lane = threadIdx.x & 31;
+    const int row = threadIdx.x >> 5;
+    const Grid g = a.g;
+    const int jz = 2 * lane;                                   // tile column of this thread's column 0
+    const int iz0 = blockIdx.x * TZ2 - 1 + jz;
+    const int iy = blockIdx.y * TYS - 1 + row;
+    const int x0 = blockIdx.z * a.cx;
+    const int x1 = min(x0 + a.cx, g.nx + 1);
+    const bool row_in = iy >= 0 && iy <= g.ny;
+    const bool in0 = row_in && iz0 >= 0 && iz0 <= g.nz;
+    const bool in1 = row_in && iz0 + 1 >= 0 && iz0 + 1 <= g.nz;
+    const bool own_row = row >= 1 && row <= TYS;
+    const bool own0 = own_row && in0 && jz >= 1 && jz <= TZ2;
+    const bool own1 = own_row && in1 && jz + 1 >= 1 && jz + 1 <= TZ2;
+    const bool erow = iy >= 0 && iy < g.ny && row < NWS - 1;
+    const bool el0 = erow && iz0 >= 0 && iz0 < g.nz;                       // element at column 0
+    const bool el1 = erow && iz0 + 1 >= 0 && iz0 + 1 < g.nz && jz + 1 < 63;  // element at column 1
+    const bool compute = row < NWS - 1;                                    // warp-uniform
+    const int rown = row + 1 < NWS ? row + 1 : row;
+    const int rowp = row > 0 ? row - 1 : 0;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P* xs = reinterpret_cast<P*>(smem_raw);
+    P* hs = xs + NWS * 6 * 32;
+#define XS2(r, k) xs[((r) * 6 + (k)) * 32 + lane]
+#define HS2(r, k) hs[((r) * 6 + (k)) * 32 + lane]
+
+    // Per-thread base pointers at CLAMPED (always in-bounds) positions.  Loads are issued two plane
+    // steps ahead into registers that nothing touches until the step that consumes them: validity,
+    // Dirichlet masking and pair packing are applied there, so no instruction waits on a load early.
+    const int64_t plane_nodes = int64_t(g.ny + 1) * (g.nz + 1);
+    const int64_t plane_elems = int64_t(g.ny) * g.nz;
+    const int iyc = min(max(iy, 0), g.ny), iye = min(max(iy, 0), g.ny - 1);
+    const int izc0 = min(max(iz0, 0), g.nz), izc1 = min(max(iz0 + 1, 0), g.nz);
+    const int ize0 = min(max(iz0, 0), g.nz - 1), ize1 = min(max(iz0 + 1, 0), g.nz - 1);
+    const int64_t c0 = int64_t(iyc) * (g.nz + 1) + izc0, c1 = int64_t(iyc) * (g.nz + 1) + izc1;
+    const TU* ub0 = a.u + 3 * c0;
+    const TU* ub1 = a.u + 3 * c1;
+    const TE* eb0 = a.E + int64_t(iye) * g.nz + ize0;
+    const TE* eb1 = a.E + int64_t(iye) * g.nz + ize1;
+    const uint8_t* mb0 = a.node_mask + c0;
+    const uint8_t* mb1 = a.node_mask + c1;
+    const int64_t col = int64_t(iy) * (g.nz + 1) + iz0;          // unclamped: owners only
+
+    auto load_plane = [&](int ix, Plane& pl) {
+        const int ixc = min(max(ix, 0), g.nx), exc = min(max(ix, 0), g.nx - 1);
+        const int64_t on = 3 * plane_nodes * ixc, oe = plane_elems * exc;
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) { pl.u0[k] = Storage<TU>::raw(ub0 + on + k); pl.u1[k] = Storage<TU>::raw(ub1 + on + k); }
+        pl.e0 = Storage<TE>::raw(eb0 + oe);
+        pl.e1 = Storage<TE>::raw(eb1 + oe);
+        if constexpr (MASK == MASK_NODE) { pl.m0 = mb0[plane_nodes * ixc]; pl.m1 = mb1[plane_nodes * ixc]; }
+    };
+
+    P up[3], uprev_raw[3], carry[3];
+    #pragma unroll
+    for (int k = 0; k < 3; ++k) { up[k] = mk2(TC(0), TC(0)); uprev_raw[k] = up[k]; carry[k] = up[k]; }
+    unsigned bits_prev = 077u;
+    P Eprev = mk2(TC(0), TC(0));                  // modulus of element plane ix - 1
+    double acc = 0.0;
+
+    // one plane step; `cur` holds the raw loads of plane ix and is refilled with plane ix + 2
+    auto step = [&](int ix, Plane& cur) {
+        const int64_t nout = int64_t(ix - 1) * plane_nodes + col;   // node plane ix - 1, column 0
+        const bool out_now = ix - 1 >= x0 && (own0 || own1);
+        // epilogue operands of node plane ix - 1, from clamped addresses (used by owners only)
+        typename S2::Raw rr0[3], rr1[3], dd0[3], dd1[3];
+        if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
+            const int64_t oo = 3 * plane_nodes * min(max(ix - 1, 0), g.nx);
+            const TY* r0 = a.r + 3 * c0 + oo;
+            const TY* r1 = a.r + 3 * c1 + oo;
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) { rr0[k] = Storage<TY>::raw(r0 + k); rr1[k] = Storage<TY>::raw(r1 + k); }
+            if constexpr (EPI == EPI_JACOBI) {
+                const TY* d0 = a.invd + 3 * c0 + oo;
+                const TY* d1 = a.invd + 3 * c1 + oo;
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) { dd0[k] = Storage<TY>::raw(d0 + k); dd1[k] = Storage<TY>::raw(d1 + k); }
+            }
+        }
+        // consume plane ix
+        const bool vplane = ix >= 0 && ix <= g.nx, veplane = ix >= 0 && ix < g.nx;
+        const bool v0 = vplane && in0, v1 = vplane && in1;
+        unsigned bits_cur = 077u;
+        if constexpr (MASK == MASK_NODE) bits_cur = (v0 ? unsigned(cur.m0) : 7u) | ((v1 ? unsigned(cur.m1) : 7u) << 3);
+        P ucur[3], uraw[3];
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const TC a0 = v0 ? TC(Storage<TU>::cvt(cur.u0[k])) : TC(0);
+            const TC a1 = v1 ? TC(Storage<TU>::cvt(cur.u1[k])) : TC(0);
+            uraw[k] = mk2(a0, a1);
+            ucur[k] = mk2(((bits_cur >> k) & 1u) ? a0 : TC(0), ((bits_cur >> (3 + k)) & 1u) ? a1 : TC(0));
+        }
+        const P Ecur = mk2(veplane && el0 ? TC(Storage<TE>::cvt(cur.e0)) : TC(0),
+                           veplane && el1 ? TC(Storage<TE>::cvt(cur.e1)) : TC(0));
+        if (ix + 2 <= x1) load_plane(ix + 2, cur);
+
+        if (ix >= x0) {
+            // ---- X stage (edge ix-1 -> ix) for both columns
+            P X0[3], X1[3];
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) { X0[k] = add2(up[k], ucur[k]); X1[k] = sub2(up[k], ucur[k]); }
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) { XS2(row, k) = X0[k]; XS2(row, 3 + k) = X1[k]; }
+            __syncthreads();
+            P H0[3][2];
+            if (compute) {
+                // ---- Y stage for columns 0 and 1
+                P Y[3][2][2];
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const P b0 = XS2(rown, k), b1 = XS2(rown, 3 + k);
+                    Y[k][0][0] = add2(X0[k], b0); Y[k][0][1] = sub2(X0[k], b0);
+                    Y[k][1][0] = add2(X1[k], b1); Y[k][1][1] = sub2(X1[k], b1);
+                }
+                // ---- Z stage for the element pair A = (col0, col1), B = (col1, col2), modulus folded
+                const P E = Eprev;
+                const P nE = mk2(-E.lo(), -E.hi());
+                P v[3][8];
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    #pragma unroll
+                    for (int px = 0; px < 2; ++px) {
+                        #pragma unroll
+                        for (int py = 0; py < 2; ++py) {
+                            const P ya = Y[k][px][py];                                        // (Y0, Y1)
+                            const P yb = mk2(ya.hi(), __shfl_down_sync(0xffffffffu, ya.lo(), 1)); // (Y1, Y2)
+                            const P ea = mul2(E, ya);
+                            const int p = px + 2 * py;
+                            if (p != 0) v[k][p] = fma2(E, yb, ea);
+                            v[k][p + 4] = fma2(nE, yb, ea);
+                        }
+                    }
+                    v[k][0] = mk2(TC(0), TC(0));
+                }
+                // ---- parity-block product (coefficients from the parameter bank)
+                #pragma unroll
+                for (int gi = 0; gi < 8; ++gi) {
+                    const int pa[3] = {gi ^ 1, gi ^ 2, gi ^ 4};
+                    const P in[3] = {v[0][pa[0]], v[1][pa[1]], v[2][pa[2]]};
+                    #pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        if (pa[r] == 0) continue;
+                        P sacc = mk2(TC(0), TC(0));
+                        bool first = true;
+                        #pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) {
+                            if (!parity_nonzero(gi, r, cc)) continue;
+                            const auto coef = args.C2.c[9 * gi + 3 * r + cc];
+                            sacc = first ? cmul2(coef, in[cc]) : cfma2(coef, in[cc], sacc);
+                            first = false;
+                        }
+                        v[r][pa[r]] = sacc;
+                    }
+                }
+                // ---- inverse Z: faces of columns 0 and 1 (column 2's share goes to lane + 1)
+                P FY[3][2][2];
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    #pragma unroll
+                    for (int px = 0; px < 2; ++px) {
+                        #pragma unroll
+                        for (int py = 0; py < 2; ++py) {
+                            const int p = px + 2 * py;
+                            const P f1 = v[k][p + 4];
+                            if (p == 0) {
+                                const TC from = __shfl_up_sync(0xffffffffu, f1.hi(), 1);
+                                FY[k][px][py] = sub2(f1, mk2(from, f1.lo()));
+                            } else {
+                                const P f0 = v[k][p];
+                                const P g0 = add2(f0, f1), g1 = sub2(f0, f1);    // (G0_A, G0_B), (G1_A, G1_B)
+                                const TC from = __shfl_up_sync(0xffffffffu, g1.hi(), 1);
+                                FY[k][px][py] = add2(mk2(g0.lo(), g1.lo()), mk2(from, g0.hi()));
+                            }
+                        }
+                    }
+                }
+                // ---- inverse Y
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    #pragma unroll
+                    for (int px = 0; px < 2; ++px) {
+                        H0[k][px] = add2(FY[k][px][0], FY[k][px][1]);
+                        HS2(row, 3 * px + k) = sub2(FY[k][px][0], FY[k][px][1]);
+                    }
+                }
+            }
+            __syncthreads();
+            if (compute) {
+                P yout[3];
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const P zero = mk2(TC(0), TC(0));
+                    const P fx0 = add2(H0[k][0], row > 0 ? HS2(rowp, k) : zero);
+                    const P fx1 = add2(H0[k][1], row > 0 ? HS2(rowp, 3 + k) : zero);
+                    yout[k] = add2(carry[k], add2(fx0, fx1));
+                    carry[k] = sub2(fx0, fx1);
+                }
+                if (out_now) {
+                    #pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        if (!(c == 0 ? own0 : own1)) continue;
+                        TY* yo = a.y + 3 * (nout + c);
+                        #pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            const TC yv = c == 0 ? yout[k].lo() : yout[k].hi();
+                            const TC xr = c == 0 ? uprev_raw[k].lo() : uprev_raw[k].hi();
+                            const bool fr = (bits_prev >> (3 * c + k)) & 1u;
+                            const TC ax = (MASK == MASK_NONE || fr) ? yv : xr;
+                            TC o;
+                            if constexpr (EPI == EPI_RAW) {
+                                o = ax;
+                            } else if constexpr (EPI == EPI_APPLY_DOT) {
+                                o = ax;
+                                acc += double(xr) * double(ax);
+                            } else if constexpr (EPI == EPI_JACOBI) {
+                                const TC r_ = TC(Storage<TY>::cvt(c == 0 ? rr0[k] : rr1[k]));
+                                const TC d_ = TC(Storage<TY>::cvt(c == 0 ? dd0[k] : dd1[k]));
+                                o = xr + a.omega * d_ * (r_ - ax);
+                            } else if constexpr (EPI == EPI_RESIDUAL) {
+                                const TC r_ = TC(Storage<TY>::cvt(c == 0 ? rr0[k] : rr1[k]));
+                                o = fr ? r_ - ax : TC(0);
+                            } else {
+                                const TC r_ = TC(Storage<TY>::cvt(c == 0 ? rr0[k] : rr1[k]));
+                                o = r_ - ax;
+                                acc += double(o) * double(o);
+                            }
+                            Storage<TY>::store(yo + k, o);
+                        }
+                    }
+                }
+            }
+        }
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) { up[k] = ucur[k]; uprev_raw[k] = uraw[k]; }
+        bits_prev = bits_cur;
+        Eprev = Ecur;
+    };
+
+    Plane pa_, pb_;                               // planes ix (even steps) and ix + 1 (odd steps)
+    load_plane(x0 - 1, pa_);
+    load_plane(x0, pb_);
+    int ix = x0 - 1;
+    for (; ix + 1 <= x1; ix += 2) {
+        step(ix, pa_);
+        step(ix + 1, pb_);
+    }
+    if (ix <= x1) step(ix, pa_);
+    if constexpr (EPI == EPI_TRUE_RES || EPI == EPI_APPLY_DOT) {
+        const int64_t bid = (int64_t(blockIdx.z) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        block_sum_store<NWS * 32>(acc, a.partials + bid);
+    }
+#undef XS2
+#undef HS2
+}
+
+// ============================================================================= parity_stream_xp
+// Third-generation streaming operator: one z node column per thread, TWO consecutive element
+// planes per step, processed as a pair (packed f32x2 in FP32).  Because both halves of a pair sit at
+// the same (y, z) position, the y exchange (shared memory) and the z exchange (shuffles) move whole
+// pairs with no repacking, and there are two block barriers per two element planes.  Each step
+// consumes the loads issued one step (two planes) earlier and refills the same registers after use;
+// validity, masking and packing happen at consumption.  Ownership, halo recomputation and
+// determinism as in parity_stream.
+template <typename TC> struct XpCfg;
+template <> struct XpCfg<float> { static constexpr int NW = 16; };
+template <> struct XpCfg<double> { static constexpr int NW = 12; };
+
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
+struct XpPlane {
+    typename Storage<TU>::raw_t u1[3], u2[3];       // node planes e+1, e+2
+    typename Storage<TE>::raw_t e0, e1;             // element planes e, e+1
+    uint8_t m1, m2;
+    typename Storage<TY>::raw_t r0[3], r1[3], d0[3], d1[3];   // epilogue operands, node planes e, e+1
+};
+
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
+__global__ void __launch_bounds__(XpCfg<TC>::NW * 32, 1)
+parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
+    constexpr int NWS = XpCfg<TC>::NW;
+    constexpr int TYS = NWS - 2;
+    using P = V2<TC>;
+    using Plane = XpPlane<TC, TU, TE, TY, EPI, MASK>;
+    const auto& a = args.a;
+    const int lane = threadIdx.x & 31;
+    const int row = threadIdx.x >> 5;
+    const Grid g = a.g;
+    const int iz = blockIdx.x * TZ - 1 + lane;
+    const int iy = blockIdx.y * TYS - 1 + row;
+    const int x0 = blockIdx.z * a.cx;
+    const int x1 = min(x0 + a.cx, g.nx + 1);                 // owned node planes [x0, x1)
+    const bool in_node = iy >= 0 && iy <= g.ny && iz >= 0 && iz <= g.nz;
+    const bool owner = in_node && lane >= 1 && lane <= TZ && row >= 1 && row <= TYS;
+    const bool elem_ok = iy >= 0 && iy < g.ny && iz >= 0 && iz < g.nz && lane < 31 && row < NWS - 1;
+    const bool compute = row < NWS - 1;                      // warp-uniform
+    const int rown = row + 1 < NWS ? row + 1 : row;
+    const int rowp = row > 0 ? row - 1 : 0;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    P* xs = reinterpret_cast<P*>(smem_raw);
+    P* hs = xs + NWS * 6 * 32;
+#define XSP(r, k) xs[((r) * 6 + (k)) * 32 + lane]
+#define HSP(r, k) hs[((r) * 6 + (k)) * 32 + lane]
+
+    // clamped (always in-bounds) addresses; values are validated when consumed
+    const int64_t plane_nodes = int64_t(g.ny + 1) * (g.nz + 1);
+    const int64_t plane_elems = int64_t(g.ny) * g.nz;
+    const int iyc = min(max(iy, 0), g.ny), izc = min(max(iz, 0), g.nz);
+    const int iye = min(max(iy, 0), g.ny - 1), ize = min(max(iz, 0), g.nz - 1);
+    const int64_t cn = int64_t(iyc) * (g.nz + 1) + izc;
+    const TU* ub = a.u + 3 * cn;
+    const TE* eb = a.E + int64_t(iye) * g.nz + ize;
+    const uint8_t* mb = a.node_mask + cn;
+    const int64_t col = int64_t(iy) * (g.nz + 1) + iz;      // unclamped: owners only
+
+    auto nplane = [&](int ix) { return int64_t(min(max(ix, 0), g.nx)); };
+    auto eplane = [&](int ex) { return int64_t(min(max(ex, 0), g.nx - 1)); };
+    auto load_step = [&](int e, Plane& pl) {
+        const int64_t n1 = 3 * plane_nodes * nplane(e + 1), n2 = 3 * plane_nodes * nplane(e + 2);
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) { pl.u1[k] = Storage<TU>::raw(ub + n1 + k); pl.u2[k] = Storage<TU>::raw(ub + n2 + k); }
+        pl.e0 = Storage<TE>::raw(eb + plane_elems * eplane(e));
+        pl.e1 = Storage<TE>::raw(eb + plane_elems * eplane(e + 1));
+        if constexpr (MASK == MASK_NODE) {
+            pl.m1 = mb[plane_nodes * nplane(e + 1)];
+            pl.m2 = mb[plane_nodes * nplane(e + 2)];
+        }
+        if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
+            const TY* r0 = a.r + 3 * cn + 3 * plane_nodes * nplane(e);
+            const TY* r1 = a.r + 3 * cn + 3 * plane_nodes * nplane(e + 1);
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) { pl.r0[k] = Storage<TY>::raw(r0 + k); pl.r1[k] = Storage<TY>::raw(r1 + k); }
+            if constexpr (EPI == EPI_JACOBI) {
+                const TY* d0 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e);
+                const TY* d1 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e + 1);
+                #pragma unroll
+                for (int k = 0; k < 3; ++k) { pl.d0[k] = Storage<TY>::raw(d0 + k); pl.d1[k] = Storage<TY>::raw(d1 + k); }
+            }
+        }
+    };
+
+    // node plane e (x0 - 1 initially): masked and raw operand, mask bits
+    TC up[3], upraw[3];
+    unsigned bits_up;
+    {
+        const int e = x0 - 1;
+        const bool v = in_node && e >= 0 && e <= g.nx;
+        const int64_t n = 3 * plane_nodes * nplane(e);
+        unsigned b = 7u;
+        if constexpr (MASK == MASK_NODE) b = v ? unsigned(mb[plane_nodes * nplane(e)]) : 7u;
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            upraw[k] = v ? TC(Storage<TU>::load(ub + n + k)) : TC(0);
+            up[k] = ((b >> k) & 1u) ? upraw[k] : TC(0);
+        }
+        bits_up = b;
+    }
+    TC carry[3] = {TC(0), TC(0), TC(0)};
+    double acc = 0.0;
+    Plane cur;
+    load_step(x0 - 1, cur);
+
+    for (int e = x0 - 1; e <= x1 - 1; e += 2) {               // element planes e, e + 1
+        // ---- consume the loads of this step
+        const bool v1 = in_node && e + 1 >= 0 && e + 1 <= g.nx;
+        const bool v2 = in_node && e + 2 >= 0 && e + 2 <= g.nx;
+        unsigned b1 = 7u, b2 = 7u;
+        if constexpr (MASK == MASK_NODE) { b1 = v1 ? unsigned(cur.m1) : 7u; b2 = v2 ? unsigned(cur.m2) : 7u; }
+        TC u1r[3], u1m[3], u2m[3], u2r[3];
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            u1r[k] = v1 ? TC(Storage<TU>::cvt(cur.u1[k])) : TC(0);
+            u2r[k] = v2 ? TC(Storage<TU>::cvt(cur.u2[k])) : TC(0);
+            u1m[k] = ((b1 >> k) & 1u) ? u1r[k] : TC(0);
+            u2m[k] = ((b2 >> k) & 1u) ? u2r[k] : TC(0);
+        }
+        const P E = mk2(elem_ok && e >= 0 && e < g.nx ? TC(Storage<TE>::cvt(cur.e0)) : TC(0),
+                        elem_ok && e + 1 >= 0 && e + 1 < g.nx ? TC(Storage<TE>::cvt(cur.e1)) : TC(0));
+        TC rr0[3], rr1[3], dd0[3], dd1[3];
+        if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                rr0[k] = TC(Storage<TY>::cvt(cur.r0[k]));
+                rr1[k] = TC(Storage<TY>::cvt(cur.r1[k]));
+                if constexpr (EPI == EPI_JACOBI) { dd0[k] = TC(Storage<TY>::cvt(cur.d0[k])); dd1[k] = TC(Storage<TY>::cvt(cur.d1[k])); }
+            }
+        }
+        if (e + 2 <= x1 - 1) load_step(e + 2, cur);          // refill: next step's planes
+
+        // ---- X stage: pair (edge e -> e+1, edge e+1 -> e+2)
+        P X0[3], X1[3];
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const P lo = mk2(up[k], u1m[k]), hi = mk2(u1m[k], u2m[k]);
+            X0[k] = add2(lo, hi);
+            X1[k] = sub2(lo, hi);
+        }
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) { XSP(row, k) = X0[k]; XSP(row, 3 + k) = X1[k]; }
+        __syncthreads();
+        P H0[3][2];
+        if (compute) {
+            P Y[3][2][2];
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const P b0 = XSP(rown, k), b1_ = XSP(rown, 3 + k);
+                Y[k][0][0] = add2(X0[k], b0); Y[k][0][1] = sub2(X0[k], b0);
+                Y[k][1][0] = add2(X1[k], b1_); Y[k][1][1] = sub2(X1[k], b1_);
+            }
+            // ---- Z stage, modulus folded: v = E (Y(iz) +- Y(iz+1)) for both elements of the pair
+            const P nE = mk2(-E.lo(), -E.hi());
+            P v[3][8];
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                #pragma unroll
+                for (int px = 0; px < 2; ++px) {
+                    #pragma unroll
+                    for (int py = 0; py < 2; ++py) {
+                        const P ya = Y[k][px][py];
+                        const P yb = mk2(__shfl_down_sync(0xffffffffu, ya.lo(), 1), __shfl_down_sync(0xffffffffu, ya.hi(), 1));
+                        const P ea = mul2(E, ya);
+                        const int p = px + 2 * py;
+                        if (p != 0) v[k][p] = fma2(E, yb, ea);
+                        v[k][p + 4] = fma2(nE, yb, ea);
+                    }
+                }
+                v[k][0] = mk2(TC(0), TC(0));
+            }
+            #pragma unroll
+            for (int gi = 0; gi < 8; ++gi) {
+                const int pa[3] = {gi ^ 1, gi ^ 2, gi ^ 4};
+                const P in[3] = {v[0][pa[0]], v[1][pa[1]], v[2][pa[2]]};
+                #pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    if (pa[r] == 0) continue;
+                    P sacc = mk2(TC(0), TC(0));
+                    bool first = true;
+                    #pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        if (!parity_nonzero(gi, r, cc)) continue;
+                        const auto coef = args.C2.c[9 * gi + 3 * r + cc];
+                        sacc = first ? cmul2(coef, in[cc]) : cfma2(coef, in[cc], sacc);
+                        first = false;
+                    }
+                    v[r][pa[r]] = sacc;
+                }
+            }
+            // ---- inverse Z: face iz gets G0 (own) + G1 of lane - 1
+            P FY[3][2][2];
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                #pragma unroll
+                for (int px = 0; px < 2; ++px) {
+                    #pragma unroll
+                    for (int py = 0; py < 2; ++py) {
+                        const int p = px + 2 * py;
+                        const P f1 = v[k][p + 4];
+                        if (p == 0) {
+                            const P from = mk2(__shfl_up_sync(0xffffffffu, f1.lo(), 1), __shfl_up_sync(0xffffffffu, f1.hi(), 1));
+                            FY[k][px][py] = sub2(f1, from);
+                        } else {
+                            const P f0 = v[k][p];
+                            const P g1 = sub2(f0, f1);
+                            const P from = mk2(__shfl_up_sync(0xffffffffu, g1.lo(), 1), __shfl_up_sync(0xffffffffu, g1.hi(), 1));
+                            FY[k][px][py] = add2(add2(f0, f1), from);
+                        }
+                    }
+                }
+            }
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                #pragma unroll
+                for (int px = 0; px < 2; ++px) {
+                    H0[k][px] = add2(FY[k][px][0], FY[k][px][1]);
+                    HSP(row, 3 * px + k) = sub2(FY[k][px][0], FY[k][px][1]);
+                }
+            }
+        }
+        __syncthreads();
+        if (compute) {
+            // ---- edge totals, inverse X: node e <- carry + sA, node e+1 <- dA + sB, carry <- dB
+            TC y0[3], y1[3];
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const P zero = mk2(TC(0), TC(0));
+                const P fx0 = add2(H0[k][0], row > 0 ? HSP(rowp, k) : zero);
+                const P fx1 = add2(H0[k][1], row > 0 ? HSP(rowp, 3 + k) : zero);
+                const P sm = add2(fx0, fx1), df = sub2(fx0, fx1);
+                y0[k] = carry[k] + sm.lo();
+                y1[k] = df.lo() + sm.hi();
+                carry[k] = df.hi();
+            }
+            if (owner) {
+                #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int ixo = e + h;                       // node plane written by this half
+                    if (ixo < x0 || ixo >= x1) continue;
+                    const unsigned bb = h == 0 ? bits_up : b1;
+                    TY* yo = a.y + 3 * (int64_t(ixo) * plane_nodes + col);
+                    #pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const TC yv = h == 0 ? y0[k] : y1[k];
+                        const TC xr = h == 0 ? upraw[k] : u1r[k];
+                        const bool fr = (bb >> k) & 1u;
+                        const TC ax = (MASK == MASK_NONE || fr) ? yv : xr;
+                        TC o;
+                        if constexpr (EPI == EPI_RAW) {
+                            o = ax;
+                        } else if constexpr (EPI == EPI_APPLY_DOT) {
+                            o = ax;
+                            acc += double(xr) * double(ax);
+                        } else if constexpr (EPI == EPI_JACOBI) {
+                            const TC r_ = h == 0 ? rr0[k] : rr1[k], d_ = h == 0 ? dd0[k] : dd1[k];
+                            o = xr + a.omega * d_ * (r_ - ax);
+                        } else if constexpr (EPI == EPI_RESIDUAL) {
+                            const TC r_ = h == 0 ? rr0[k] : rr1[k];
+                            o = fr ? r_ - ax : TC(0);
+                        } else {
+                            const TC r_ = h == 0 ? rr0[k] : rr1[k];
+                            o = r_ - ax;
+                            acc += double(o) * double(o);
+                        }
+                        Storage<TY>::store(yo + k, o);
+                    }
+                }
+            }
+        }
+        // ---- the step's last node plane (e + 2) becomes the next step's first
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) { up[k] = u2m[k]; upraw[k] = u2r[k]; }
+        bits_up = b2;
+    }
+    if constexpr (EPI == EPI_TRUE_RES || EPI == EPI_APPLY_DOT) {
+        const int64_t bid = (int64_t(blockIdx.z) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        block_sum_store<NWS * 32>(acc, a.partials + bid);
+    }
+#undef XSP
+#undef HSP
+}
+
+// CTA tiling of the streaming operators: parity_stream2 (author layout, node or no mask) tiles
+// (y, z) node columns as (NW-2) x 62; parity_stream (natural-layout / SIMP / DOF-mask product) as
+// 14 x 30.  x-chunk: the longest chunk (least halo recomputation) with >= 4 CTAs per SM.
+struct Tiling { int tz, ty; };
+inline Tiling tiling(int prec, bool v2) {
+    if (!v2) return {TZ, TYR};
+    return {TZ, (prec == VX_F64 ? XpCfg<double>::NW : XpCfg<float>::NW) - 2};
+}
+
+inline int stream_cx(const Grid& g, Tiling t) {
+    const int64_t yz = int64_t((g.nz + 1 + t.tz - 1) / t.tz) * ((g.ny + 1 + t.ty - 1) / t.ty);
     int cx = CX_MAX;
     while (cx > 4 && yz * ((g.nx + 1 + cx - 1) / cx) < 4 * 148) cx /= 2;
     return cx;
 }
 
-inline dim3 stream_grid(const Grid& g, int cx) {
-    return dim3((g.nz + 1 + TZ - 1) / TZ, (g.ny + 1 + TYR - 1) / TYR, (g.nx + 1 + cx - 1) / cx);
+inline dim3 stream_grid(const Grid& g, Tiling t, int cx) {
+    return dim3((g.nz + 1 + t.tz - 1) / t.tz, (g.ny + 1 + t.ty - 1) / t.ty, (g.nx + 1 + cx - 1) / cx);
 }
 
-int64_t stream_ctas(const Grid& g) {
-    dim3 d = stream_grid(g, stream_cx(g));
+// CTAs (= partial sums) of a fused reducing launch of precision `prec` on grid g
+int64_t stream_ctas(const Grid& g, int prec) {
+    const Tiling t = tiling(prec, true);
+    dim3 d = stream_grid(g, t, stream_cx(g, t));
     return int64_t(d.x) * d.y * d.z;
 }
 
 template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP>
 int launch_stream(const OpArgs<TC, TU, TE, TY>& a_in, cudaStream_t s, const char* what) {
+    constexpr bool v2 = !REV && !SIMP && MASK != MASK_DOF;
     OpArgs<TC, TU, TE, TY> a = a_in;
-    a.cx = stream_cx(a.g);
-    auto kern = parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
-    constexpr size_t smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
-    // dynamic (48 KB for FP64) + static (the block reduction) shared memory exceeds the 48 KB
-    // default: opt in once per instantiation.  The solvers run every loop body once un-captured
-    // before capturing it, so this call never happens inside a stream capture.
+    const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
+    a.cx = stream_cx(a.g, t);
+    size_t smem, threads;
+    const void* kern;
+    if constexpr (v2) {
+        kern = (const void*)parity_stream_xp<TC, TU, TE, TY, EPI, MASK>;
+        threads = XpCfg<TC>::NW * 32;
+        smem = size_t(2) * XpCfg<TC>::NW * 6 * 32 * sizeof(V2<TC>);
+    } else {
+        kern = (const void*)parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
+        threads = NW * 32;
+        smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
+    }
+    // dynamic + static shared memory exceeds the 48 KB default: opt in once per instantiation.  The
+    // solvers run every loop body once un-captured before capturing it, so this call never happens
+    // inside a stream capture.
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -329,7 +937,17 @@ int launch_stream(const OpArgs<TC, TU, TE, TY>& a_in, cudaStream_t s, const char
         }
         configured = true;
     }
-    kern<<<stream_grid(a.g, a.cx), NW * 32, smem, s>>>(a);
+    if constexpr (v2) {
+        OpArgs2<TC, TU, TE, TY> a2;
+        a2.a = a;
+        for (int i = 0; i < 72; ++i) {
+            if constexpr (std::is_same<TC, float>::value) a2.C2.c[i] = make_float2(a.C.c[i], a.C.c[i]);
+            else a2.C2.c[i] = a.C.c[i];
+        }
+        parity_stream_xp<TC, TU, TE, TY, EPI, MASK><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+    } else {
+        parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a);
+    }
     VX_CHECK_LAUNCH(what);
     return VX_OK;
 }
@@ -657,9 +1275,9 @@ extern "C" int vx_residual(int prec, int nx, int ny, int nz, const double* block
                                         nullptr, 0.0, res, nullptr, stream);
 }
 
-extern "C" int64_t vx_operator_partials(int nx, int ny, int nz) {
-    if (check_grid(nx, ny, nz)) return -1;
-    return stream_ctas(Grid{nx, ny, nz});
+extern "C" int64_t vx_operator_partials(int prec, int nx, int ny, int nz) {
+    if (check_grid(nx, ny, nz) || (prec != VX_F64 && prec != VX_F32)) return -1;
+    return stream_ctas(Grid{nx, ny, nz}, prec);
 }
 
 extern "C" int vx_apply_dot(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
@@ -729,7 +1347,9 @@ extern "C" int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const 
     if (st) return st;
     VX_CHECK_ARG(blocks && E && x && b && res && norm2, VX_ERR_NULL_POINTER,
                  "vx_true_residual_noalloc: NULL pointer");
-    const int64_t G = stream_ctas(Grid{nx, ny, nz});
+    VX_CHECK_ARG(prec == VX_F64 || prec == VX_F32, VX_ERR_INVALID_ARGUMENT,
+                 "vx_true_residual_noalloc: unsupported precision %d", prec);
+    const int64_t G = stream_ctas(Grid{nx, ny, nz}, prec);
     VX_CHECK_ARG(G <= NOALLOC_MAX_CTAS, VX_ERR_INVALID_ARGUMENT,
                  "vx_true_residual_noalloc: grid (%d, %d, %d) needs %lld partial sums but the built-in scratch "
                  "holds %lld; use vx_true_residual with a caller-provided buffer",

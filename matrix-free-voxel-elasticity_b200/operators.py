@@ -82,7 +82,7 @@ class VoxelOperator:
     @property
     def partials_size(self) -> int:
         """doubles of scratch the fused reducing forms (apply_dot / true_residual) need"""
-        return int(_lib.load().vx_operator_partials(*self.shape))
+        return int(_lib.load().vx_operator_partials(self.prec, *self.shape))
 
     def _vec(self, t, what, dtype=None):
         return _ptr(t, what, dtype or self.dtype, self.ndof)

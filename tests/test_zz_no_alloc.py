@@ -58,7 +58,7 @@ def test_noalloc_matches_existing_entry_point_on_two_calls(shape):
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
     shape = (2047, 400, 400)                     # needs far more than 16384 CTA partial sums
-    assert _lib.load().vx_operator_partials(*shape) > 16384
+    assert _lib.load().vx_operator_partials(_lib.VX_F64, *shape) > 16384
     dummy = torch.zeros(8, dtype=torch.float64, device="cuda")
     blocks = np.ascontiguousarray(vx.Modal(KE).blocks.reshape(72))
     st = _lib.load().vx_true_residual_noalloc(_lib.VX_F64, *shape, _lib.dptr(blocks), dummy.data_ptr(), None,
