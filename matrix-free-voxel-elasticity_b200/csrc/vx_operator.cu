@@ -607,7 +607,7 @@ parity_stream2(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
 // determinism as in parity_stream.
 template <typename TC> struct XpCfg;
 template <> struct XpCfg<float> { static constexpr int NW = 16; };
-template <> struct XpCfg<double> { static constexpr int NW = 12; };
+template <> struct XpCfg<double> { static constexpr int NW = 8; };
 
 template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
 struct XpPlane {
@@ -760,7 +760,7 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
                     #pragma unroll
                     for (int py = 0; py < 2; ++py) {
                         const P ya = Y[k][px][py];
-                        const P yb = mk2(__shfl_down_sync(0xffffffffu, ya.lo(), 1), __shfl_down_sync(0xffffffffu, ya.hi(), 1));
+                        const P yb = shfl_down2(ya, 1);
                         const P ea = mul2(E, ya);
                         const int p = px + 2 * py;
                         if (p != 0) v[k][p] = fma2(E, yb, ea);
@@ -799,12 +799,12 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
                         const int p = px + 2 * py;
                         const P f1 = v[k][p + 4];
                         if (p == 0) {
-                            const P from = mk2(__shfl_up_sync(0xffffffffu, f1.lo(), 1), __shfl_up_sync(0xffffffffu, f1.hi(), 1));
+                            const P from = shfl_up2(f1, 1);
                             FY[k][px][py] = sub2(f1, from);
                         } else {
                             const P f0 = v[k][p];
                             const P g1 = sub2(f0, f1);
-                            const P from = mk2(__shfl_up_sync(0xffffffffu, g1.lo(), 1), __shfl_up_sync(0xffffffffu, g1.hi(), 1));
+                            const P from = shfl_up2(g1, 1);
                             FY[k][px][py] = add2(add2(f0, f1), from);
                         }
                     }

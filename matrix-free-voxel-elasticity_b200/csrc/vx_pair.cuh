@@ -48,4 +48,21 @@ __device__ __forceinline__ V2<double> cfma2(double c, V2<double> a, V2<double> a
 __device__ __forceinline__ V2<float> cmul2(float2 c, V2<float> a) { return {__fmul2_rn(c, a.v)}; }
 __device__ __forceinline__ V2<float> cfma2(float2 c, V2<float> a, V2<float> acc) { return {__ffma2_rn(c, a.v, acc.v)}; }
 
+// whole-pair shuffles: an FP32 pair moves as one 64-bit value, so both halves land in an aligned
+// register pair; an FP64 pair is two 64-bit shuffles
+__device__ __forceinline__ V2<float> shfl_down2(V2<float> a, int d) {
+    const unsigned long long b = __shfl_down_sync(0xffffffffu, *reinterpret_cast<const unsigned long long*>(&a.v), d);
+    return {*reinterpret_cast<const float2*>(&b)};
+}
+__device__ __forceinline__ V2<float> shfl_up2(V2<float> a, int d) {
+    const unsigned long long b = __shfl_up_sync(0xffffffffu, *reinterpret_cast<const unsigned long long*>(&a.v), d);
+    return {*reinterpret_cast<const float2*>(&b)};
+}
+__device__ __forceinline__ V2<double> shfl_down2(V2<double> a, int d) {
+    return {__shfl_down_sync(0xffffffffu, a.x, d), __shfl_down_sync(0xffffffffu, a.y, d)};
+}
+__device__ __forceinline__ V2<double> shfl_up2(V2<double> a, int d) {
+    return {__shfl_up_sync(0xffffffffu, a.x, d), __shfl_up_sync(0xffffffffu, a.y, d)};
+}
+
 }  // namespace vx
