@@ -185,6 +185,29 @@ int vx_axpby(int prec, int64_t n, double alpha, const void* x, double beta, void
 int vx_cast(int64_t n, int src_prec, const void* src, int dst_prec, void* dst, double scale,
             cudaStream_t stream);
 
+/* ---------------------------------------------------------------------------- SIMP */
+
+/* Matrix-free hat density filter on the element grid (author layout), weights max(0, rmin - |d|),
+ * support ceil(rmin) - 1 (rmin <= 4): mode 0 y = H x; mode 1 y = (H x) / s; mode 2 y = H (x / s),
+ * s = H 1 the row sums.  Replaces: experiments/session_a/donor/src/gpu_fem/filter_r2.py:40-76,
+ * 93-171 (cone stencil, forward, transpose); the CSR filter of experiments/session_h/run_w1b.py:97-125. */
+int vx_cone_filter(int nx, int ny, int nz, double rmin, const double* x, const double* s, int mode,
+                   double* y, cudaStream_t stream);
+
+/* top88 optimality-criteria update with the bisection on the multiplier on the device
+ * (experiments/session_h/run_w1b.py:46-62, 82-94).  State S (16 doubles): S[0] l1, S[1] l2,
+ * S[2] last lmid, S[3] last volume, S[4] volfrac, S[5] tol, S[6] element count, S[10] done,
+ * S[11] probes, S[12] max probes, S[15] = 1.  A probe: lmid = (l1 + l2) / 2,
+ * x_new = clip(x sqrt(max(-dc / dv / lmid, 0)), max(x - move, 0), min(x + move, 1)), volume =
+ * sum w x_new / n with w = H (1 / s) (= mean of the filtered x_new); vx_oc_finalize moves l1 or l2 and
+ * sets done when (l2 - l1) / (l1 + l2) <= tol.  vx_oc_apply writes x_new for the last lmid. */
+int64_t vx_oc_partials(int64_t n);
+int vx_oc_probe(int64_t n, const double* x, const double* dc, const double* dv, const double* w, double move,
+                const double* S, double* partials, cudaStream_t stream);
+int vx_oc_finalize(int64_t n, const double* partials, double* S, cudaStream_t stream);
+int vx_oc_apply(int64_t n, const double* x, const double* dc, const double* dv, double move, const double* S,
+                double* x_new, cudaStream_t stream);
+
 /* Operator forms fused with the outer Krylov loop (FP64/FP32, author layout, node mask optional):
  *   vx_apply_dot:     q = A p and partials[cta] = sum p.q over the CTA's owned nodes
  *   vx_true_residual: res = b - A x and partials[cta] = sum res^2

@@ -68,6 +68,12 @@ SIGNATURES = {
     "vx_graph_launch": (c_int, [_P, _P]),
     "vx_graph_destroy": (c_int, [_P]),
     "vx_capture_status": (c_int, [_P]),
+    # SIMP
+    "vx_cone_filter": (c_int, [c_int, c_int, c_int, c_double, _P, _P, c_int, _P, _P]),
+    "vx_oc_partials": (c_int64, [c_int64]),
+    "vx_oc_probe": (c_int, [c_int64, _P, _P, _P, _P, c_double, _P, _P, _P]),
+    "vx_oc_finalize": (c_int, [c_int64, _P, _P, _P]),
+    "vx_oc_apply": (c_int, [c_int64, _P, _P, _P, c_double, _P, _P, _P]),
 }
 
 _lib = None
@@ -113,7 +119,8 @@ CAPTURE_STREAM = None
 KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2}
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
-             "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch"}
+             "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",
+             "vx_oc_partials"}
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 

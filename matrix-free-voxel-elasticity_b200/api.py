@@ -36,7 +36,7 @@ class ElasticitySolver:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         self.shape = tuple(int(s) for s in shape)
         self.ke = quadrature([1.0, 1.0, 1.0], 0.3) if ke is None else np.asarray(ke, dtype=np.float64).reshape(24, 24)
-        self.E = _dev(E)
+        self.E = _dev(E).clone()          # owned: update_modulus rewrites it in place
         m = mask.to("cuda", non_blocking=True) if isinstance(mask, torch.Tensor) else _dev(mask)
         self.node_mask = m.contiguous() if m.dtype == torch.uint8 else node_mask_from_dofs(m.to(torch.float64))
         self.op64 = VoxelOperator(self.shape, self.ke, torch.float64)
@@ -50,19 +50,23 @@ class ElasticitySolver:
                     raise ValueError(f"{self.shape} supports at most {len(shapes)} levels with max_coarse_x={max_coarse_x}")
                 shapes = shapes[:levels]
             dt = torch.float64 if precision == "fp64" else torch.float32
-            if isinstance(omega, str) and omega == "spectral":
-                # the reference estimates lambda_l once, on the FP64 hierarchy shared by all arms
-                ref = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, torch.float64, pre, post, None,
-                                  shapes=shapes)
-                omega = ref.spectral_omegas(seed=spectral_seed)[0]
-                if dt == torch.float64:
-                    ref.set_omegas(omega)
-                    self.M = ref
-                del ref
-            if not hasattr(self, "M"):
-                self.M = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, dt, pre, post, omega, shapes=shapes)
+            spectral = isinstance(omega, str) and omega == "spectral"
+            self.M = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, dt, pre, post,
+                                 None if spectral else omega, shapes=shapes)
+            self.spectral_seed = spectral_seed
+            if spectral:
+                # lambda_l from the FP64 level operators, as the reference estimates it once on the
+                # FP64 hierarchy shared by all arms (experiments/session_i/run_gpu.py:287-288)
+                self.refresh_omegas()
         self.fcg = FCGSolver(self.op64, self.E, self.node_mask, self.M, tol=tol, maxiter=maxiter,
                              check_every=check_every, graph=graph)
+
+    def refresh_omegas(self, iterations=30):
+        """Re-estimate omega_l = 4 / (3 lambda_l) for the current moduli (spectral damping)."""
+        om, lam = self.M.spectral_omegas(iterations=iterations, seed=self.spectral_seed)
+        self.M.set_omegas(om)
+        self.lambdas = lam
+        return om, lam
 
     @property
     def levels(self):
@@ -71,10 +75,18 @@ class ElasticitySolver:
     def footprint_bytes(self):
         return self.fcg.footprint_bytes()
 
-    def solve(self, f):
-        """Solve with right-hand side f (CUDA tensor or array, author layout).  Returns SolveResult
-        (x, iterations, converged, rel, matvecs); x is the solver's own buffer (copy it to keep it)."""
-        return self.fcg.solve(_dev(f))
+    def solve(self, f, x0=None):
+        """Solve with right-hand side f (CUDA tensor or array, author layout), optionally warm-started
+        at x0.  Returns SolveResult (x, iterations, converged, rel, matvecs); x is the solver's own
+        buffer (copy it to keep it)."""
+        return self.fcg.solve(_dev(f), None if x0 is None else _dev(x0))
+
+    def update_modulus(self, E):
+        """New element moduli on the same grid: refreshes the hierarchy in place (graphs stay valid)."""
+        E = _dev(E)
+        if E.data_ptr() != self.E.data_ptr():
+            self.E.copy_(E)
+        self.M.update_modulus(self.E)
 
     def compliance(self, f, x):
         return float(_dev(f) @ x)

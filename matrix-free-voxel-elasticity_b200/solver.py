@@ -117,6 +117,26 @@ class MGHierarchy:
     def finest(self):
         return self.levels[0]
 
+    def update_modulus(self, E):
+        """New finest modulus (FP64, same grid): refresh every level's moduli, inverse diagonal and
+        the coarsest inverse IN PLACE, so captured graphs that use this hierarchy stay valid."""
+        L0 = self.levels[0]
+        if E.data_ptr() != L0.E64.data_ptr():
+            L0.E64.copy_(E)
+        for i, L in enumerate(self.levels):
+            if i:
+                prev = self.levels[i - 1]
+                _lib.call("vx_coarsen_modulus", _lib.VX_F64, *prev.shape, prev.E64.data_ptr(), L.E64.data_ptr(), _s())
+            if L.E.data_ptr() != L.E64.data_ptr():
+                L.E.copy_(L.E64)
+            inv64 = L.op64.diagonal(L.E64, L.mask, inverse=True)
+            L.invd.copy_(inv64)
+        c = self.levels[-1]
+        _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
+                  c.E64.data_ptr(), c.mask.data_ptr(), self.A_coarse.data_ptr(), _s())
+        self.coarse_factor = torch.linalg.cholesky(self.A_coarse)
+        self.A_inv.copy_(torch.cholesky_inverse(self.coarse_factor))
+
     def footprint_bytes(self) -> int:
         b = 0
         for L in self.levels:
@@ -196,6 +216,7 @@ class JacobiPreconditioner:
 
     def __init__(self, op64: VoxelOperator, E64, node_mask):
         self.dtype, self.prec = torch.float64, _lib.VX_F64
+        self.op64, self.mask = op64, node_mask
         self.invd = op64.diagonal(E64, node_mask, inverse=True)
         self.z = torch.zeros(op64.ndof, dtype=torch.float64, device="cuda")
 
@@ -203,6 +224,9 @@ class JacobiPreconditioner:
         _lib.call("vx_scaled_product", _lib.VX_F64, self.z.numel(), 1.0, self.invd.data_ptr(), r64.data_ptr(),
                   self.z.data_ptr(), _s())
         return self.z
+
+    def update_modulus(self, E):
+        self.invd.copy_(self.op64.diagonal(E, self.mask, inverse=True))
 
     def footprint_bytes(self):
         return self.invd.numel() * 16
@@ -343,17 +367,22 @@ class FCGSolver:
         for j in range(k):
             self._iteration(checking and j == k - 1)
 
-    def _init(self, b):
+    def _init(self, b, x0=None):
         S = self.S.data_ptr()
         self.b.copy_(b)
-        self.x.zero_()
-        self.r.copy_(self.b)
         self.p.zero_()
         _lib.call("vx_set_scalars", S, 0, 16, 0.0, _s())
         _lib.call("vx_set_scalars", S, S_TOL, 1, self.tol if self.fixed is None else -1.0, _s())
         _lib.call("vx_dots_pr", _lib.VX_F64, _lib.VX_F64, self.n, self.b.data_ptr(), self.b.data_ptr(), None,
                   self.partials.data_ptr(), _s())
         self._fin(FIN_NB, self.G_vec)
+        if x0 is None:
+            self.x.zero_()
+            self.r.copy_(self.b)
+        else:                                                   # warm start: r = b - A x0
+            self.x.copy_(x0)
+            self.op.true_residual(self.x, self.b, self.E, self.mask, self.r, self.partials)
+            self._fin(FIN_TRUE, self.G_op)
         z = self.M.emit(self.r)
         _lib.call("vx_dots_pr", _lib.VX_F64, self.zprec, self.n, self.r.data_ptr(), z.data_ptr(), None,
                   self.partials.data_ptr(), _s())
@@ -366,7 +395,9 @@ class FCGSolver:
         torch.cuda.current_stream().synchronize()
         return self.S_host.numpy().copy()
 
-    def solve(self, b: torch.Tensor) -> SolveResult:
+    def solve(self, b: torch.Tensor, x0: torch.Tensor | None = None) -> SolveResult:
+        """Solve A x = b (optionally warm-started at x0: then r0 = b - A x0 and a converged x0
+        returns after 0 iterations).  x is the solver's own buffer."""
         if b.numel() != self.n:
             raise ValueError(f"b has {b.numel()} entries, expected {self.n}")
         caller = torch.cuda.current_stream()
@@ -379,10 +410,15 @@ class FCGSolver:
             self._graph = _GraphLoop(self.stream, self.S, lambda: self._body(k, checking))
             self._graph_k = (k, checking)
         with torch.cuda.stream(self.stream):
-            self._init(b)
+            self._init(b, x0)
             S = self.S.data_ptr()
             _lib.call("vx_set_scalars", S, S_MAXIT, 1, float(limit), _s())
             _lib.call("vx_set_scalars", S, S_CHECK, 1, float(k), _s())
+            if x0 is not None and self.fixed is None:
+                s0 = self._read()
+                if s0[S_DONE]:
+                    caller.wait_stream(self.stream)
+                    return SolveResult(self.x, 0, True, float(s0[S_REL]), int(s0[S_MV]))
             if full > 0:
                 if self.use_graph:
                     self._graph.launch(self.stream)

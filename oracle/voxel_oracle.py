@@ -566,3 +566,26 @@ def gaussian_random_field(shape, ell, seed):
     g = np.real(np.fft.ifftn(np.fft.fftn(w) * np.exp(-2 * np.pi ** 2 * ell ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))))
     g = (g - g.mean()) / g.std()
     return (1e-3 + (1 - 1e-3) / (1 + np.exp(-g))).ravel()
+
+
+def simp_top88(shape, x, steps, volfrac, rmin, move, emin=1e-9, penal=3.0, oc_tol=1e-6, solve=None):
+    """Density-filtered SIMP with the top88 OC (experiments/session_h/run_w1b.py:163-205, update
+    'top88'): rho = H x / s; solve K(E(rho)) u = f; dc = -p rho^(p-1)(1-emin) u_e^T ke u_e;
+    dc_x = H(dc / s), dv_x = H(1 / s); x <- oc_top88(x, dc_x, dv_x, volfrac, move, density).
+    `solve(E) -> u` must return the displacement for modulus E.  Returns (x, rho, compliances)."""
+    ke = quadrature([1, 1, 1], 0.3)
+    filt = ConeFilter(shape, rmin)
+    mask, force = cantilever_equal_split(shape)
+    rho = filt.forward(x)
+    dv_x = filt.transpose(np.ones_like(x))
+    comps = []
+    for _ in range(steps):
+        E = simp_modulus(rho, emin, 1.0, penal)
+        u = solve(E)
+        comps.append(float(force @ u))
+        ce = element_energy(shape, ke, u)
+        dc = -penal * rho ** (penal - 1) * (1 - emin) * ce
+        dc_x = filt.transpose(dc)
+        x = oc_top88(x, dc_x, dv_x, volfrac, move, density=filt.forward, tol=oc_tol)
+        rho = filt.forward(x)
+    return x, rho, comps
