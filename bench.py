@@ -43,6 +43,10 @@ WORKLOADS = {
     "gmg_256x128x128": ((256, 128, 128), ("grf", 8.0, 0), 5,
                         "cantilever 256x128x128 (12.7M DOF), GRF l=8 seed 0 -> [1e-3,1], E0=1 Emin=1e-9 p=3, "
                         "5-level V(2,2) damped Jacobi omega=0.6, tol 1e-8"),
+    "serving": ((256, 128, 128), ("grf", 8.0, 0), None,
+                "256 solve requests, Poisson arrivals (seeded, offered load 1.2x the serial FP64 capacity), "
+                "grids uniform from 48x24x24/96x48x48/160x80x80/256x128x128, seeded GRF densities l=8, "
+                "tol uniform from {1e-6, 1e-8}, mixed GMG-PCG V(2,2) omega=0.6, HBM budget 150 GB"),
     "jacobi_32x16x16": ((32, 16, 16), ("uniform", 0), None,
                         "cantilever 32x16x16 (28,611 DOF), uniform(0.01,1) seed 0, Jacobi-PCG, tol 1e-8"),
 }
@@ -418,10 +422,60 @@ def run_kernels(args):
     print(json.dumps({k: {"us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9} for k, v in table.items()}))
 
 
+def run_serving(args):
+    """Continuous-batching server vs serial plain-FP64 solving on the same request stream."""
+    import torch
+    import voxel_b200 as vx
+    from voxel_b200 import serving
+    shapes = ((48, 24, 24), (96, 48, 48), (160, 80, 80), (256, 128, 128))
+    # serial FP64 service time per shape (after warm-up) sets the arrival rate
+    svc = {}
+    for s_ in shapes:
+        rho = vx.problems.gaussian_random_field(s_, 8.0, 7)
+        mask, force = vx.problems.cantilever_equal_split(s_)
+        sol = vx.ElasticitySolver(s_, vx.problems.simp_modulus(rho, 1e-9), mask, precision="fp64", tol=1e-8,
+                                  check_every=1)
+        sol.solve(force)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = sol.solve(force)
+        torch.cuda.synchronize()
+        svc[s_] = time.perf_counter() - t0
+        if not r.converged:
+            raise RuntimeError(f"serial FP64 reference solve on {s_} did not converge: {r}")
+        del sol
+    mean_service = float(np.mean(list(svc.values())))
+    n = 256 if not args.profile else 32
+    reqs = serving.request_stream(n=n, shapes=shapes, load=1.2, mean_service=mean_service, seed=0)
+    warm = serving.request_stream(n=8, shapes=shapes, rate=1e6, seed=99)
+    for r in warm:
+        r.arrival = 0.0
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        backend = serving.CudaBackend(precision="mixed")
+        sched = serving.Scheduler(serving._PoolCharge(backend), budget_bytes=150e9, max_slots=16)
+        sched.run(warm)                                          # populate the solver pool (untimed)
+        sched.peak_inflight = 0
+        done, makespan = sched.run(reqs)
+    mixed = serving.summarize(done, makespan)
+    mixed.update(peak_inflight=sched.peak_inflight,
+                 not_converged=[(c.rid, c.shape, c.iterations, c.rel) for c in done if not c.converged][:10])
+    serial_done, serial_summary = serving.serve(reqs, precision="fp64", max_slots=1)
+    serial_summary["not_converged"] = [(c.rid, c.shape, c.iterations, c.rel) for c in serial_done if not c.converged][:10]
+    return {"metric": "serving p99 latency, mixed-size stream (continuous batching, mixed GMG-PCG)",
+            "value": mixed["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": n, "warmup": len(warm),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner",
+            "data": "synthetic", "config": {"workload": "serving", "description": WORKLOADS["serving"][3]},
+            "serving": mixed, "serial_fp64": serial_summary, "serial_fp64_service_s": {str(k): v for k, v in svc.items()},
+            "clocks": clocks.summary()}
+
+
 def main():
     args = parse()
     if args.kernels:
         run_kernels(args)
+        return
+    if args.workload == "serving" and args.impl == "b200":
+        print(json.dumps(run_serving(args)))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -271,6 +271,8 @@ int vx_set_scalars(double* S, int first, int count, double value, cudaStream_t s
 int vx_graph_while_begin(cudaStream_t stream, void** handle);
 int vx_graph_while_end(void* handle, const double* S, cudaStream_t stream);
 int vx_graph_launch(void* handle, cudaStream_t stream);
+/* Number of nodes in a WHILE graph's captured body (-1 on error). */
+int64_t vx_graph_body_nodes(void* handle);
 /* Capture state of `stream`: 0 none, 1 active, 2 invalidated, -1 query failed. */
 int vx_capture_status(cudaStream_t stream);
 int vx_graph_destroy(void* handle);

@@ -13,7 +13,7 @@ from .operators import (Product, VoxelOperator, cast, dofs_from_node_mask, dots,
 from . import problems, solver, voxel_mg  # noqa: E402
 from .solver import FCGSolver, JacobiPCG, JacobiPreconditioner, MGHierarchy, SolveResult, hierarchy_shapes
 from .api import ElasticitySolver, solve
-from . import simp  # noqa: E402
+from . import serving, simp  # noqa: E402
 from .simp import Compliance, ConeFilter, OCUpdater, compliance, oc_top88, run_simp
 
 __all__ = ["XYZ", "Modal", "element", "quadrature", "edof_author", "element_nodes", "n_elems", "n_nodes",
@@ -21,4 +21,4 @@ __all__ = ["XYZ", "Modal", "element", "quadrature", "edof_author", "element_node
            "node_mask_from_dofs", "product", "reduce_partials", "simp_modulus", "problems", "solver", "voxel_mg",
            "FCGSolver", "JacobiPCG", "JacobiPreconditioner", "MGHierarchy", "SolveResult", "hierarchy_shapes",
            "ElasticitySolver", "solve", "simp", "Compliance", "ConeFilter", "OCUpdater", "compliance", "oc_top88",
-           "run_simp"]
+           "run_simp", "serving"]

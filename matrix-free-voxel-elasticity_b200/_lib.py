@@ -68,6 +68,7 @@ SIGNATURES = {
     "vx_graph_launch": (c_int, [_P, _P]),
     "vx_graph_destroy": (c_int, [_P]),
     "vx_capture_status": (c_int, [_P]),
+    "vx_graph_body_nodes": (c_int64, [_P]),
     # SIMP
     "vx_cone_filter": (c_int, [c_int, c_int, c_int, c_double, _P, _P, c_int, _P, _P]),
     "vx_oc_partials": (c_int64, [c_int64]),
@@ -120,7 +121,7 @@ KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noal
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",
-             "vx_oc_partials"}
+             "vx_oc_partials", "vx_graph_body_nodes"}
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 

@@ -57,12 +57,14 @@ __global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const d
     if (threadIdx.x != 0) return;
     switch (op) {
         case FIN_PQ:
+            if (S[S_DONE] != 0.0) break;            // a converged warm start: the body is a no-op
             S[S_PQ] = s0;
             S[S_MV] += 1.0;
             if (s0 == 0.0 || !isfinite(s0)) { S[S_BREAK] = 1.0; S[S_ALPHA] = 0.0; }   // no step is taken
             else { S[S_ALPHA] = S[S_RZ] / s0; S[S_IT] += 1.0; }
             break;
         case FIN_TRUE:
+            if (S[S_DONE] != 0.0) break;
             S[S_RR] = s0;
             S[S_REL] = sqrt(s0) / S[S_NB];
             S[S_MV] += 1.0;
@@ -375,6 +377,15 @@ extern "C" int vx_graph_launch(void* handle, cudaStream_t stream) {
         return VX_ERR_CUDA;
     }
     return VX_OK;
+}
+
+// Number of nodes in the captured loop body (introspection for tests).
+extern "C" int64_t vx_graph_body_nodes(void* handle) {
+    if (!handle) return -1;
+    auto* w = static_cast<WhileGraph*>(handle);
+    size_t n = 0;
+    if (cudaGraphGetNodes(w->body, nullptr, &n) != cudaSuccess) return -1;
+    return int64_t(n);
 }
 
 extern "C" int vx_graph_destroy(void* handle) {

@@ -1,0 +1,274 @@
+"""Continuous-batching solve server.
+
+Requests (elasticity solves on grids of different sizes, each with its own density and tolerance)
+arrive over time.  The scheduler admits a request as soon as a slot is free and its device memory
+footprint (vectors + multigrid hierarchy + coarsest dense inverse) fits the HBM budget, so work
+that arrives while other solves run starts immediately and overlaps with them on the GPU: every
+in-flight job owns a CUDA stream, its density, its hierarchy and its captured whole-solve graph,
+and the host only polls completion events.  Solvers are pooled per grid shape: a new request on a
+shape whose solver is free refreshes the moduli in place (the captured graph stays valid) instead
+of rebuilding.  Kernels are deterministic, so a result does not depend on what else ran with it.
+
+The scheduling core (`Scheduler`) is independent of CUDA; `CudaBackend` runs jobs on the device.
+There is no counterpart in the reference (it has no serving loop).
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    shape: tuple
+    density: object            # author-layout element densities (numpy or CUDA tensor)
+    tol: float
+    arrival: float             # seconds after the stream starts
+
+
+@dataclass
+class Completion:
+    rid: int
+    shape: tuple
+    tol: float
+    arrival: float
+    admitted: float
+    finished: float
+    iterations: int
+    converged: bool
+    rel: float
+    compliance: float
+    x: object = None
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+def footprint_estimate(shape, precision="mixed", levels=None, max_coarse_x=16) -> int:
+    """Device bytes of one resident job: FP64 outer vectors, moduli, hierarchy, coarsest inverse."""
+    from .solver import hierarchy_shapes
+    shapes = hierarchy_shapes(shape, max_coarse_x)
+    if levels is not None:
+        shapes = shapes[:levels]
+    es = 8 if precision == "fp64" else 4
+    total = 0
+    for i, (nx, ny, nz) in enumerate(shapes):
+        nodes, elems = (nx + 1) * (ny + 1) * (nz + 1), nx * ny * nz
+        if i == 0:
+            total += 6 * 24 * nodes + 2 * 8 * elems        # b x r p q z_old; E and its owned copy
+        total += 4 * 3 * es * nodes + elems * (8 + es) + nodes
+    nx, ny, nz = shapes[-1]
+    nc = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    return int(total + 3 * 8 * nc * nc + (64 << 20))   # A, its factor, its inverse; workspace margin
+
+
+def percentile(values, q):
+    return float(np.percentile(np.asarray(values, dtype=np.float64), q)) if len(values) else float("nan")
+
+
+def summarize(completions, makespan):
+    lat = [c.latency for c in completions]
+    return {"requests": len(completions), "makespan_s": makespan,
+            "solves_per_s": len(completions) / makespan if makespan > 0 else float("nan"),
+            "p50_ms": 1e3 * percentile(lat, 50), "p99_ms": 1e3 * percentile(lat, 99),
+            "mean_ms": 1e3 * float(np.mean(lat)) if lat else float("nan"),
+            "all_converged": all(c.converged for c in completions)}
+
+
+class Scheduler:
+    """FIFO admission by slots and memory budget; completion by polling.  `backend` provides
+    footprint(req), start(req) -> handle, done(handle) -> bool, finish(handle, req) -> dict,
+    release(handle) and reclaim(bytes_needed) -> bytes freed from idle pooled state."""
+
+    def __init__(self, backend, budget_bytes=150e9, max_slots=16, clock=time.perf_counter, poll_s=50e-6):
+        self.backend, self.budget, self.max_slots = backend, float(budget_bytes), int(max_slots)
+        self.clock, self.poll_s = clock, poll_s
+        self.peak_inflight = 0
+        self.peak_bytes = 0.0
+
+    def run(self, requests):
+        pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
+        active = []            # (req, handle, bytes, admitted)
+        done = []
+        used = 0.0
+        t0 = self.clock()
+        while pending or active:
+            now = self.clock() - t0
+            progressed = False
+            while pending and pending[0].arrival <= now and len(active) < self.max_slots:
+                req = pending[0]
+                need = float(self.backend.footprint(req))
+                if need > self.budget:
+                    raise ValueError(f"request {req.rid} needs {need / 1e9:.1f} GB, over the whole budget")
+                if used + need > self.budget:
+                    used -= self.backend.reclaim(used + need - self.budget)
+                    if used + need > self.budget:
+                        break                                   # wait for a running job to finish
+                pending.popleft()
+                handle = self.backend.start(req)
+                used += need
+                active.append((req, handle, need, self.clock() - t0))
+                self.peak_inflight = max(self.peak_inflight, len(active))
+                self.peak_bytes = max(self.peak_bytes, used)
+                progressed = True
+            still = []
+            for req, handle, need, adm in active:
+                if self.backend.done(handle):
+                    info = self.backend.finish(handle, req)
+                    fin = self.clock() - t0
+                    self.backend.release(handle)
+                    used -= need
+                    done.append(Completion(req.rid, tuple(req.shape), req.tol, req.arrival, adm, fin, **info))
+                    progressed = True
+                else:
+                    still.append((req, handle, need, adm))
+            active = still
+            if not progressed:
+                if not active and pending:
+                    wait = pending[0].arrival - (self.clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.01))
+                else:
+                    time.sleep(self.poll_s)
+        return done, self.clock() - t0
+
+
+class CudaBackend:
+    """Runs each request on a pooled ElasticitySolver with its own stream."""
+
+    def __init__(self, precision="mixed", pre=2, post=2, omega=0.6, max_coarse_x=16, keep_solution=False,
+                 maxiter=200, check_every=1):
+        import torch
+        self.torch = torch
+        self.precision, self.pre, self.post, self.omega = precision, pre, post, omega
+        self.max_coarse_x, self.keep, self.maxiter, self.check_every = max_coarse_x, keep_solution, maxiter, check_every
+        self.free = {}              # shape -> [solver, ...] idle, resident
+        self.free_bytes = {}        # id(solver) -> footprint
+        self.forces = {}
+
+    def footprint(self, req):
+        return footprint_estimate(req.shape, self.precision, max_coarse_x=self.max_coarse_x)
+
+    def _force(self, shape):
+        from .problems import cantilever_equal_split
+        if shape not in self.forces:
+            self.forces[shape] = cantilever_equal_split(shape)
+        return self.forces[shape]
+
+    def start(self, req):
+        from .api import ElasticitySolver
+        from .problems import simp_modulus
+        torch = self.torch
+        shape = tuple(req.shape)
+        mask, force = self._force(shape)
+        rho = req.density if isinstance(req.density, torch.Tensor) else torch.as_tensor(req.density)
+        rho = rho.to("cuda", torch.float64, non_blocking=True)
+        pool = self.free.get(shape, [])
+        if pool:
+            s = pool.pop()
+            self.free_bytes.pop(id(s), None)
+            s.fcg.stream.wait_stream(torch.cuda.current_stream())    # rho was produced there
+            with torch.cuda.stream(s.fcg.stream):
+                s.update_modulus(simp_modulus(rho, 1e-9))
+        else:
+            s = ElasticitySolver(shape, simp_modulus(rho, 1e-9), mask, precision=self.precision, pre=self.pre,
+                                 post=self.post, omega=self.omega, max_coarse_x=self.max_coarse_x, tol=req.tol,
+                                 maxiter=self.maxiter, check_every=self.check_every)
+        s.fcg.tol = float(req.tol)
+        s.fcg.launch(force)
+        return s
+
+    def done(self, s):
+        return s.fcg.done()
+
+    def finish(self, s, req):
+        res = s.fcg.finish()
+        _, force = self._force(tuple(req.shape))
+        x = res.x.clone() if self.keep else None
+        return {"iterations": res.iterations, "converged": res.converged, "rel": res.rel,
+                "compliance": float(force @ res.x), "x": x}
+
+    def release(self, s):
+        self.free.setdefault(s.shape, []).append(s)
+        self.free_bytes[id(s)] = footprint_estimate(s.shape, self.precision, max_coarse_x=self.max_coarse_x)
+
+    def reclaim(self, need):
+        """Drop idle pooled solvers (largest first) until `need` bytes are freed; returns bytes freed."""
+        freed = 0.0
+        order = sorted(((self.free_bytes.get(id(s), 0), shape, s) for shape, lst in self.free.items() for s in lst),
+                       key=lambda t: -t[0])
+        for b, shape, s in order:
+            if freed >= need:
+                break
+            self.free[shape].remove(s)
+            self.free_bytes.pop(id(s), None)
+            freed += b
+        if freed:
+            self.torch.cuda.empty_cache()
+        return freed
+
+    def resident_bytes(self):
+        return sum(self.free_bytes.values())
+
+
+def serve(requests, precision="mixed", budget_bytes=150e9, max_slots=16, keep_solution=False, **kw):
+    """Run a request stream through the continuous-batching server; returns (completions, summary).
+    Pooled idle solvers are charged to the budget (they stay resident for reuse)."""
+    backend = CudaBackend(precision=precision, keep_solution=keep_solution, **kw)
+    sched = Scheduler(_PoolCharge(backend), budget_bytes=budget_bytes, max_slots=max_slots)
+    done, makespan = sched.run(requests)
+    out = summarize(done, makespan)
+    out.update(peak_inflight=sched.peak_inflight, peak_budget_gb=sched.peak_bytes / 1e9)
+    return sorted(done, key=lambda c: c.rid), out
+
+
+class _PoolCharge:
+    """Adapter: idle pooled solvers are charged to the budget until reclaimed, so the budget bounds
+    everything resident (running and pooled)."""
+
+    def __init__(self, backend):
+        self.b = backend
+
+    def footprint(self, req):
+        pool = self.b.free.get(tuple(req.shape), [])
+        return 0.0 if pool else self.b.footprint(req)      # a pooled solver is already charged
+
+    def start(self, req):
+        return self.b.start(req)
+
+    def done(self, h):
+        return self.b.done(h)
+
+    def finish(self, h, req):
+        return self.b.finish(h, req)
+
+    def release(self, h):
+        self.b.release(h)
+
+    def reclaim(self, need):
+        return self.b.reclaim(need)
+
+
+def request_stream(n=256, shapes=((48, 24, 24), (96, 48, 48), (160, 80, 80), (256, 128, 128)), tols=(1e-6, 1e-8),
+                   rate=None, mean_service=None, load=1.2, seed=0, densities_per_shape=4, ell=8.0, device="cuda"):
+    """The mixed-size request stream: Poisson arrivals (seeded), shapes uniform from `shapes`,
+    seeded GRF densities (l = ell, a few per shape, reused), tolerances uniform from `tols`.  The
+    arrival rate is `rate`, or load / mean_service."""
+    from .problems import gaussian_random_field
+    rng = np.random.default_rng(seed)
+    dens = {s: [gaussian_random_field(s, ell, 1000 + 17 * k + i, device=device) for i in range(densities_per_shape)]
+            for k, s in enumerate(shapes)}
+    if rate is None:
+        rate = load / float(mean_service)
+    t = 0.0
+    reqs = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        s = shapes[rng.integers(len(shapes))]
+        reqs.append(Request(i, s, dens[s][rng.integers(densities_per_shape)], float(tols[rng.integers(len(tols))]), t))
+    return reqs

@@ -91,7 +91,11 @@ class MGHierarchy:
         _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
                   _ptr(c.E64, "E"), _ptr(c.mask, "mask"), A.data_ptr(), _s())
         self.A_coarse = A
-        self.coarse_factor = torch.linalg.cholesky(A)
+        # the same factorisation call as update_modulus, so a refreshed pooled hierarchy and a fresh
+        # one are bitwise identical; checked once here (the check synchronises)
+        self.coarse_factor, info = torch.linalg.cholesky_ex(A)
+        if int(info) != 0:
+            raise ValueError(f"coarsest-level matrix is not positive definite (cholesky info {int(info)})")
         self.A_inv = torch.cholesky_inverse(self.coarse_factor).contiguous()
         n_smooth = len(self.levels) - 1
         if omegas is None:
@@ -134,7 +138,9 @@ class MGHierarchy:
         c = self.levels[-1]
         _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
                   c.E64.data_ptr(), c.mask.data_ptr(), self.A_coarse.data_ptr(), _s())
-        self.coarse_factor = torch.linalg.cholesky(self.A_coarse)
+        # no error check here (it would synchronise the stream); a non-SPD coarse matrix shows up as a
+        # non-finite residual and a non-converged solve
+        self.coarse_factor = torch.linalg.cholesky_ex(self.A_coarse)[0]
         self.A_inv.copy_(torch.cholesky_inverse(self.coarse_factor))
 
     def footprint_bytes(self) -> int:
@@ -269,12 +275,16 @@ class _GraphLoop:
     """Owns a WHILE graph (csrc/vx_solver.cu) whose body is captured from `emit_body`.
 
     The body is first run once un-captured: with CUDA's lazy module loading, a kernel's first
-    launch loads its module, which must not happen inside a capture.  Callers re-initialise the
-    solver state after building the graph."""
+    launch loads its module, which must not happen inside a capture.  That warm-up writes the
+    solver's buffers on `stream`, so it is ordered after all work already queued on the caller's
+    stream: the caching allocator may have handed those buffers memory that kernels still queued
+    there (temporaries of the set-up, e.g. the coarse factorisation) are using.  Callers
+    re-initialise the solver state after building the graph."""
 
     def __init__(self, stream: torch.cuda.Stream, S: torch.Tensor, emit_body):
         self.handle = ctypes.c_void_p()
         sp = ctypes.c_void_p(stream.cuda_stream)
+        stream.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(stream):
             emit_body()                                     # warm-up (loads every kernel of the body)
             _lib.call("vx_graph_while_begin", sp, ctypes.byref(self.handle))
@@ -339,6 +349,8 @@ class FCGSolver:
         self.use_graph = bool(graph)
         self._graph = None
         self._graph_k = None
+        self._pending = None
+        self._event = None
 
     def footprint_bytes(self) -> int:
         return 6 * self.n * 8 + self.M.footprint_bytes() + self.E.numel() * 8
@@ -395,44 +407,58 @@ class FCGSolver:
         torch.cuda.current_stream().synchronize()
         return self.S_host.numpy().copy()
 
-    def solve(self, b: torch.Tensor, x0: torch.Tensor | None = None) -> SolveResult:
-        """Solve A x = b (optionally warm-started at x0: then r0 = b - A x0 and a converged x0
-        returns after 0 iterations).  x is the solver's own buffer."""
+    def launch(self, b: torch.Tensor, x0: torch.Tensor | None = None, stream: torch.cuda.Stream | None = None):
+        """Enqueue a solve of A x = b on `stream` (default: the solver's own) without waiting: the
+        initialisation, the whole-loop graph and an asynchronous read-back of the scalars.  Call
+        finish() for the result; done() polls without blocking."""
         if b.numel() != self.n:
             raise ValueError(f"b has {b.numel()} entries, expected {self.n}")
-        caller = torch.cuda.current_stream()
-        self.stream.wait_stream(caller)
+        st = stream or self.stream
         checking = self.fixed is None
         k = self.check_every if checking else 1
         limit = self.fixed if self.fixed is not None else self.maxiter
         full = limit // k
+        caller = torch.cuda.current_stream()
+        st.wait_stream(caller)
+        if st != caller:                 # b and x0 are read on st: keep their memory until it is done
+            b.record_stream(st)
+            if x0 is not None:
+                x0.record_stream(st)
         if full > 0 and self.use_graph and (self._graph is None or self._graph_k != (k, checking)):
-            self._graph = _GraphLoop(self.stream, self.S, lambda: self._body(k, checking))
+            self._graph = _GraphLoop(st, self.S, lambda: self._body(k, checking))
             self._graph_k = (k, checking)
-        with torch.cuda.stream(self.stream):
+        with torch.cuda.stream(st):
             self._init(b, x0)
             S = self.S.data_ptr()
             _lib.call("vx_set_scalars", S, S_MAXIT, 1, float(limit), _s())
             _lib.call("vx_set_scalars", S, S_CHECK, 1, float(k), _s())
-            if x0 is not None and self.fixed is None:
-                s0 = self._read()
-                if s0[S_DONE]:
-                    caller.wait_stream(self.stream)
-                    return SolveResult(self.x, 0, True, float(s0[S_REL]), int(s0[S_MV]))
-            if full > 0:
-                if self.use_graph:
-                    self._graph.launch(self.stream)
-                else:
-                    for _ in range(full):
-                        self._body(k, checking)
-                        s = self._read()
-                        if s[S_DONE] or s[S_BREAK]:
-                            break
-            s = self._read()
-            done = bool(s[S_DONE])
-            it = int(s[S_IT])
             if full > 0 and self.use_graph:
-                self._graph.account(max(1, -(-it // k)))
+                self._graph.launch(st)
+            self.S_host.copy_(self.S, non_blocking=True)
+            self._event = torch.cuda.Event()
+            self._event.record(st)
+        self._pending = (st, k, checking, limit, full, x0 is not None)
+
+    def done(self) -> bool:
+        return self._pending is None or self._event.query()
+
+    def finish(self) -> SolveResult:
+        """Wait for the launched solve and return its result (host work only for the rare tails:
+        iterations past the last full loop body, the host-driven loop, or non-convergence)."""
+        st, k, checking, limit, full, warm = self._pending
+        self._pending = None
+        self._event.synchronize()
+        with torch.cuda.stream(st):
+            s = self.S_host.numpy().copy()
+            if full > 0 and self.use_graph:
+                self._graph.account(max(1, -(-int(s[S_IT]) // k)))
+            if not self.use_graph and not (warm and s[S_DONE]):
+                for _ in range(full):
+                    self._body(k, checking)
+                    s = self._read()
+                    if s[S_DONE] or s[S_BREAK]:
+                        break
+            done, it = bool(s[S_DONE]), int(s[S_IT])
             while not done and not s[S_BREAK] and it < limit:                 # iterations past the last full body
                 self._iteration(checking and (it + 1) % k == 0)
                 s = self._read()
@@ -441,9 +467,15 @@ class FCGSolver:
                 self.op.true_residual(self.x, self.b, self.E, self.mask, self.q, self.partials)
                 self._fin(FIN_TRUE, self.G_op)
                 s = self._read()
-        caller.wait_stream(self.stream)
+        torch.cuda.current_stream().wait_stream(st)
         rel = float(s[S_REL])
         return SolveResult(self.x, int(s[S_IT]), bool(rel <= self.tol), rel, int(s[S_MV]))
+
+    def solve(self, b: torch.Tensor, x0: torch.Tensor | None = None) -> SolveResult:
+        """Solve A x = b (optionally warm-started at x0: then r0 = b - A x0 and a converged x0
+        returns after 0 iterations).  x is the solver's own buffer."""
+        self.launch(b, x0)
+        return self.finish()
 
 
 class JacobiPCG:
