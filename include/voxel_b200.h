@@ -38,11 +38,22 @@ enum {
     VX_ERR_CUDA = 7              /* another CUDA runtime error                                  */
 };
 
-/* Precision / storage selectors */
+/* Precision / storage selectors.  The multigrid kernels see two kinds of vector: ITERATES (the
+ * smoother's x and x_out, the operand u of a product, the coarse solve's z, both sides of the
+ * prolongation, the V-cycle output) and AUXILIARY vectors (right-hand sides r, residuals res, the
+ * inverse diagonal, both sides of the restriction).  Storage per selector:
+ *                     iterate   auxiliary   modulus E   arithmetic
+ *   VX_F64            double    double      double      FP64
+ *   VX_F32            float     float       float       FP32
+ *   VX_BF16_F32       bf16      bf16        bf16        FP32  (vx_matvec writes y in float)
+ *   VX_F32_BF16AUX    float     bf16        bf16        FP32
+ * VX_F32_BF16AUX keeps only the iterate in FP32: rounding the iterate to bf16 after every sweep
+ * adds rough noise that costs outer iterations, rounding the rest does not. */
 enum {
-    VX_F64 = 0,       /* FP64 storage, FP64 arithmetic                                  */
-    VX_F32 = 1,       /* FP32 storage, FP32 arithmetic                                  */
-    VX_BF16_F32 = 2   /* operand u and modulus E stored in BF16, FP32 arithmetic/output */
+    VX_F64 = 0,
+    VX_F32 = 1,
+    VX_BF16_F32 = 2,
+    VX_F32_BF16AUX = 3
 };
 
 const char* vx_last_error(void);

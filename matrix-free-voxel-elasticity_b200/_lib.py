@@ -15,7 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libvoxel_b200.so"
 
 VX_OK, VX_ERR_INVALID_ARGUMENT, VX_ERR_NULL_POINTER, VX_ERR_ALIGNMENT = 0, 1, 2, 3
 VX_ERR_LAUNCH, VX_ERR_UNSUPPORTED, VX_ERR_TIMEOUT, VX_ERR_CUDA = 4, 5, 6, 7
-VX_F64, VX_F32, VX_BF16_F32 = 0, 1, 2
+VX_F64, VX_F32, VX_BF16_F32, VX_F32_BF16AUX = 0, 1, 2, 3
 
 _P = c_void_p          # device or host pointer
 _D = POINTER(c_double)  # host double array

@@ -13,7 +13,10 @@ from .element import quadrature
 from .operators import VoxelOperator, node_mask_from_dofs
 from .solver import FCGSolver, JacobiPreconditioner, MGHierarchy, hierarchy_shapes
 
-PRECISIONS = ("fp64", "mixed", "jacobi")
+PRECISIONS = ("fp64", "mixed", "bf16", "bf16-all", "jacobi")
+# V-cycle storage: (iterate dtype, auxiliary-vector and modulus dtype)
+_MG_STORAGE = {"fp64": (torch.float64, torch.float64), "mixed": (torch.float32, torch.float32),
+               "bf16": (torch.float32, torch.bfloat16), "bf16-all": (torch.bfloat16, torch.bfloat16)}
 
 
 def _dev(a, dtype=torch.float64):
@@ -26,7 +29,10 @@ class ElasticitySolver:
     """K(E) u = f on a (nx, ny, nz) voxel cantilever-type problem, author layout.
 
     precision: "fp64" (FP64 V-cycle), "mixed" (FP32 V-cycle inside the FP64 outer loop; FP64 for the
-    outer residual, dots, step lengths and the coarsest solve) or "jacobi" (FP64 Jacobi-PCG via fcg).
+    outer residual, dots, step lengths and the coarsest solve), "bf16" (as mixed, with the V-cycle's
+    moduli, right-hand sides, residuals and inverse diagonals stored in bf16, iterates in FP32),
+    "bf16-all" (the iterates in bf16 as well; costs outer iterations) or "jacobi" (FP64 Jacobi-PCG
+    via fcg).
     omega: a float, a per-level list, or "spectral" (4 / (3 lambda_l), src/voxel_mg.py:228-244).
     """
 
@@ -49,10 +55,10 @@ class ElasticitySolver:
                 if levels > len(shapes):
                     raise ValueError(f"{self.shape} supports at most {len(shapes)} levels with max_coarse_x={max_coarse_x}")
                 shapes = shapes[:levels]
-            dt = torch.float64 if precision == "fp64" else torch.float32
+            dt, aux = _MG_STORAGE[precision]
             spectral = isinstance(omega, str) and omega == "spectral"
             self.M = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, dt, pre, post,
-                                 None if spectral else omega, shapes=shapes)
+                                 None if spectral else omega, shapes=shapes, aux_dtype=aux)
             self.spectral_seed = spectral_seed
             if spectral:
                 # lambda_l from the FP64 level operators, as the reference estimates it once on the

@@ -51,9 +51,11 @@ int check_grid(int nx, int ny, int nz);
 
 // ---------------------------------------------------------------------------- storage conversion
 template <typename S> struct Storage;
-// load: value in arithmetic type; raw/cvt: load without touching the value, convert at use
+// load: value in arithmetic type; raw/cvt: load without touching the value, convert at use;
+// round: the arithmetic value that storing v would leave in memory
 template <> struct Storage<double> {
     using raw_t = double;
+    __device__ static double round(double v) { return v; }
     __device__ static double load(const double* p) { return *p; }
     __device__ static double raw(const double* p) { return *p; }
     __device__ static double cvt(double v) { return v; }
@@ -61,6 +63,7 @@ template <> struct Storage<double> {
 };
 template <> struct Storage<float> {
     using raw_t = float;
+    __device__ static float round(float v) { return v; }
     __device__ static float load(const float* p) { return *p; }
     __device__ static float raw(const float* p) { return *p; }
     __device__ static float cvt(float v) { return v; }
@@ -68,11 +71,34 @@ template <> struct Storage<float> {
 };
 template <> struct Storage<__nv_bfloat16> {
     using raw_t = __nv_bfloat16;
+    __device__ static float round(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
     __device__ static float load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     __device__ static __nv_bfloat16 raw(const __nv_bfloat16* p) { return *p; }
     __device__ static float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
     __device__ static void store(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 };
+// arithmetic type of a storage type (bf16 -> float)
+template <typename S> using arith_t = decltype(Storage<S>::load(static_cast<const S*>(nullptr)));
+
+// ---------------------------------------------------------------------------- storage selectors
+// Iterate (X), auxiliary-vector (R) and modulus (M) storage of each VX_* selector.
+template <int P> struct PrecT;
+template <> struct PrecT<VX_F64> { using X = double; using R = double; using M = double; };
+template <> struct PrecT<VX_F32> { using X = float; using R = float; using M = float; };
+template <> struct PrecT<VX_BF16_F32> { using X = __nv_bfloat16; using R = __nv_bfloat16; using M = __nv_bfloat16; };
+template <> struct PrecT<VX_F32_BF16AUX> { using X = float; using R = __nv_bfloat16; using M = __nv_bfloat16; };
+
+// Calls f(PrecT<P>{}) for the runtime selector `prec`; false if it is not a selector.
+template <typename F>
+bool dispatch_prec(int prec, F&& f) {
+    switch (prec) {
+        case VX_F64: f(PrecT<VX_F64>{}); return true;
+        case VX_F32: f(PrecT<VX_F32>{}); return true;
+        case VX_BF16_F32: f(PrecT<VX_BF16_F32>{}); return true;
+        case VX_F32_BF16AUX: f(PrecT<VX_F32_BF16AUX>{}); return true;
+        default: return false;
+    }
+}
 
 // ---------------------------------------------------------------------------- parity blocks
 // The parity (Walsh-Hadamard) form of an affine-brick Hex8 element matrix: T ke T^T / 64 is block

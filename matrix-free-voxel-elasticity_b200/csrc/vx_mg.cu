@@ -13,39 +13,42 @@ __device__ __forceinline__ void node_coords(const Grid& g, int64_t n, int& ix, i
     ix = int(n / (int64_t(g.nz + 1) * (g.ny + 1)));
 }
 
-// coarse node (I,J,K) of fine grid f: rc = sum w(a) w(b) w(d) f(2I+a, 2J+b, 2K+d), w(0)=1, w(+-1)=1/2
+// coarse node (I,J,K) of fine grid f: rc = sum w(a) w(b) w(d) f(2I+a, 2J+b, 2K+d), w(0)=1, w(+-1)=1/2.
+// Arithmetic in arith_t<T> (bf16 storage: FP32).
 template <typename T>
 __global__ void restrict_kernel(Grid f, Grid c, const T* __restrict__ fine, const uint8_t* __restrict__ cmask,
                                 T* __restrict__ coarse) {
+    using A = arith_t<T>;
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= c.nodes()) return;
     int I, J, K;
     node_coords(c, n, I, J, K);
     const unsigned bits = cmask ? unsigned(cmask[n]) : 7u;
+    auto ld = [&](int64_t i) { return Storage<T>::load(fine + i); };
     for (int comp = 0; comp < 3; ++comp) {
-        T ty[3][3];   // after the x pass, at fine (y = 2J + b - 1, z = 2K + d - 1)
+        A ty[3][3];   // after the x pass, at fine (y = 2J + b - 1, z = 2K + d - 1)
         for (int b = 0; b < 3; ++b)
             for (int d = 0; d < 3; ++d) {
                 const int fy = 2 * J + b - 1, fz = 2 * K + d - 1;
-                T v = T(0);
+                A v = A(0);
                 if (fy >= 0 && fy <= f.ny && fz >= 0 && fz <= f.nz) {
-                    v = fine[3 * f.node(2 * I, fy, fz) + comp];
-                    if (2 * I + 1 <= f.nx) v = v + T(0.5) * fine[3 * f.node(2 * I + 1, fy, fz) + comp];
-                    if (I >= 1) v = v + T(0.5) * fine[3 * f.node(2 * I - 1, fy, fz) + comp];
+                    v = ld(3 * f.node(2 * I, fy, fz) + comp);
+                    if (2 * I + 1 <= f.nx) v = v + A(0.5) * ld(3 * f.node(2 * I + 1, fy, fz) + comp);
+                    if (I >= 1) v = v + A(0.5) * ld(3 * f.node(2 * I - 1, fy, fz) + comp);
                 }
                 ty[b][d] = v;
             }
-        T tz[3];
+        A tz[3];
         for (int d = 0; d < 3; ++d) {
-            T v = ty[1][d];
-            if (2 * J + 1 <= f.ny) v = v + T(0.5) * ty[2][d];
-            if (J >= 1) v = v + T(0.5) * ty[0][d];
+            A v = ty[1][d];
+            if (2 * J + 1 <= f.ny) v = v + A(0.5) * ty[2][d];
+            if (J >= 1) v = v + A(0.5) * ty[0][d];
             tz[d] = v;
         }
-        T v = tz[1];
-        if (2 * K + 1 <= f.nz) v = v + T(0.5) * tz[2];
-        if (K >= 1) v = v + T(0.5) * tz[0];
-        coarse[3 * n + comp] = ((bits >> comp) & 1u) ? v : T(0);
+        A v = tz[1];
+        if (2 * K + 1 <= f.nz) v = v + A(0.5) * tz[2];
+        if (K >= 1) v = v + A(0.5) * tz[0];
+        Storage<T>::store(coarse + 3 * n + comp, ((bits >> comp) & 1u) ? v : A(0));
     }
 }
 
@@ -53,6 +56,7 @@ __global__ void restrict_kernel(Grid f, Grid c, const T* __restrict__ fine, cons
 template <typename T>
 __global__ void prolong_add_kernel(Grid f, Grid c, const T* __restrict__ coarse, const uint8_t* __restrict__ fmask,
                                    T* __restrict__ x) {
+    using A = arith_t<T>;
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= f.nodes()) return;
     int i, j, k;
@@ -61,17 +65,18 @@ __global__ void prolong_add_kernel(Grid f, Grid c, const T* __restrict__ coarse,
     const int I0 = i >> 1, J0 = j >> 1, K0 = k >> 1;
     const bool ox = i & 1, oy = j & 1, oz = k & 1;
     for (int comp = 0; comp < 3; ++comp) {
-        T py[2];
+        A py[2];
         for (int d = 0; d <= int(oz); ++d) {
-            T px[2];
+            A px[2];
             for (int b = 0; b <= int(oy); ++b) {
                 const int64_t a0 = 3 * c.node(I0, J0 + b, K0 + d) + comp;
-                px[b] = ox ? T(0.5) * (coarse[a0] + coarse[a0 + 3 * int64_t(c.ny + 1) * (c.nz + 1)]) : coarse[a0];
+                const A c0 = Storage<T>::load(coarse + a0);
+                px[b] = ox ? A(0.5) * (c0 + Storage<T>::load(coarse + a0 + 3 * int64_t(c.ny + 1) * (c.nz + 1))) : c0;
             }
-            py[d] = oy ? T(0.5) * (px[0] + px[1]) : px[0];
+            py[d] = oy ? A(0.5) * (px[0] + px[1]) : px[0];
         }
-        const T v = oz ? T(0.5) * (py[0] + py[1]) : py[0];
-        if ((bits >> comp) & 1u) x[3 * n + comp] = x[3 * n + comp] + v;
+        const A v = oz ? A(0.5) * (py[0] + py[1]) : py[0];
+        if ((bits >> comp) & 1u) Storage<T>::store(x + 3 * n + comp, Storage<T>::load(x + 3 * n + comp) + v);
     }
 }
 
@@ -133,20 +138,21 @@ __global__ void assemble_dense_kernel(Grid g, const __grid_constant__ Ke576 ke, 
 }
 
 // z = (Ainv r) * mask, one warp per row, FP64 accumulation
-template <typename T>
-__global__ void coarse_apply_kernel(int n, const double* __restrict__ Ainv, const T* __restrict__ r,
+template <typename TR, typename T>
+__global__ void coarse_apply_kernel(int n, const double* __restrict__ Ainv, const TR* __restrict__ r,
                                     const uint8_t* __restrict__ mask, T* __restrict__ z) {
+    using A = arith_t<T>;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
     const double* row = Ainv + int64_t(warp) * n;
     double s = 0.0;
-    for (int j = lane; j < n; j += 32) s = fma(row[j], double(r[j]), s);
+    for (int j = lane; j < n; j += 32) s = fma(row[j], double(Storage<TR>::load(r + j)), s);
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) {
         const bool fr = mask ? ((mask[warp / 3] >> (warp % 3)) & 1u) : true;
-        z[warp] = fr ? T(s) : T(0);
+        Storage<T>::store(z + warp, fr ? A(s) : A(0));
     }
 }
 
@@ -178,11 +184,11 @@ extern "C" int vx_restrict(int prec, int nx, int ny, int nz, const void* fine, c
     if (st) return st;
     VX_CHECK_ARG(fine && coarse, VX_ERR_NULL_POINTER, "vx_restrict: NULL pointer");
     Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
-    if (prec == VX_F64)
-        restrict_kernel<double><<<blocks_for(c.nodes(), 128), 128, 0, stream>>>(f, c, (const double*)fine, coarse_mask, (double*)coarse);
-    else if (prec == VX_F32)
-        restrict_kernel<float><<<blocks_for(c.nodes(), 128), 128, 0, stream>>>(f, c, (const float*)fine, coarse_mask, (float*)coarse);
-    else { set_error("vx_restrict: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    const bool ok = dispatch_prec(prec, [&](auto t) {             // auxiliary vectors on both sides
+        using R = typename decltype(t)::R;
+        restrict_kernel<R><<<blocks_for(c.nodes(), 128), 128, 0, stream>>>(f, c, (const R*)fine, coarse_mask, (R*)coarse);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_restrict: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_restrict");
     return VX_OK;
 }
@@ -193,11 +199,11 @@ extern "C" int vx_prolong_add(int prec, int nx, int ny, int nz, const void* coar
     if (st) return st;
     VX_CHECK_ARG(coarse && x, VX_ERR_NULL_POINTER, "vx_prolong_add: NULL pointer");
     Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
-    if (prec == VX_F64)
-        prolong_add_kernel<double><<<blocks_for(f.nodes(), 256), 256, 0, stream>>>(f, c, (const double*)coarse, fine_mask, (double*)x);
-    else if (prec == VX_F32)
-        prolong_add_kernel<float><<<blocks_for(f.nodes(), 256), 256, 0, stream>>>(f, c, (const float*)coarse, fine_mask, (float*)x);
-    else { set_error("vx_prolong_add: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    const bool ok = dispatch_prec(prec, [&](auto t) {             // iterates on both sides
+        using X = typename decltype(t)::X;
+        prolong_add_kernel<X><<<blocks_for(f.nodes(), 256), 256, 0, stream>>>(f, c, (const X*)coarse, fine_mask, (X*)x);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_prolong_add: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_prolong_add");
     return VX_OK;
 }
@@ -209,11 +215,11 @@ extern "C" int vx_coarsen_modulus(int prec, int nx, int ny, int nz, const void* 
     VX_CHECK_ARG(E_fine && E_coarse, VX_ERR_NULL_POINTER, "vx_coarsen_modulus: NULL pointer");
     Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
     const unsigned gb = blocks_for(c.elems(), 256);
-    if (prec == VX_F64) coarsen_modulus_kernel<double><<<gb, 256, 0, stream>>>(f, c, (const double*)E_fine, (double*)E_coarse);
-    else if (prec == VX_F32) coarsen_modulus_kernel<float><<<gb, 256, 0, stream>>>(f, c, (const float*)E_fine, (float*)E_coarse);
-    else if (prec == VX_BF16_F32)
-        coarsen_modulus_kernel<__nv_bfloat16><<<gb, 256, 0, stream>>>(f, c, (const __nv_bfloat16*)E_fine, (__nv_bfloat16*)E_coarse);
-    else { set_error("vx_coarsen_modulus: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using M = typename decltype(t)::M;
+        coarsen_modulus_kernel<M><<<gb, 256, 0, stream>>>(f, c, (const M*)E_fine, (M*)E_coarse);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarsen_modulus: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarsen_modulus");
     return VX_OK;
 }
@@ -252,9 +258,12 @@ extern "C" int vx_coarse_apply(int prec, int n, const double* Ainv, const void* 
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply: n must be positive");
     VX_CHECK_ARG(Ainv && r && z, VX_ERR_NULL_POINTER, "vx_coarse_apply: NULL pointer");
     const unsigned gb = blocks_for(int64_t(n) * 32, 256);
-    if (prec == VX_F64) coarse_apply_kernel<double><<<gb, 256, 0, stream>>>(n, Ainv, (const double*)r, node_mask, (double*)z);
-    else if (prec == VX_F32) coarse_apply_kernel<float><<<gb, 256, 0, stream>>>(n, Ainv, (const float*)r, node_mask, (float*)z);
-    else { set_error("vx_coarse_apply: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
+        using R = typename decltype(t)::R;
+        using X = typename decltype(t)::X;
+        coarse_apply_kernel<R, X><<<gb, 256, 0, stream>>>(n, Ainv, (const R*)r, node_mask, (X*)z);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarse_apply");
     return VX_OK;
 }

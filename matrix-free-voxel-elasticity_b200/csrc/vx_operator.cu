@@ -33,7 +33,9 @@ constexpr int CX_MAX = 32;      // owned node planes per CTA (x chunk), upper bo
 enum Epi { EPI_RAW = 0, EPI_JACOBI = 1, EPI_RESIDUAL = 2, EPI_TRUE_RES = 3, EPI_APPLY_DOT = 4 };
 enum MaskKind { MASK_NONE = 0, MASK_NODE = 1, MASK_DOF = 2 };
 
-template <typename TC, typename TU, typename TE, typename TY>
+// TR: type of the auxiliary vectors r and invd (the output type TY unless a storage mode keeps
+// them narrower than the iterate)
+template <typename TC, typename TU, typename TE, typename TY, typename TR = TY>
 struct OpArgs {
     Grid g;
     const TU* u;              // operand (smoother: current iterate x)
@@ -41,8 +43,8 @@ struct OpArgs {
     TY* y;                    // output
     const uint8_t* node_mask; // MASK_NODE: bit c set <=> DOF c free
     const double* dof_mask;   // MASK_DOF: 3 doubles per node, non-zero = free
-    const TY* r;              // JACOBI / RESIDUAL / TRUE_RES right-hand side
-    const TY* invd;           // JACOBI inverse diagonal
+    const TR* r;              // JACOBI / RESIDUAL / TRUE_RES right-hand side
+    const TR* invd;           // JACOBI inverse diagonal
     TC omega;
     double* partials;         // TRUE_RES (|res|^2) / APPLY_DOT (p.q): one double per CTA
     double emin, de, penal;   // SIMP modulus E = emin + de * rho^penal
@@ -297,305 +299,14 @@ parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
 }
 
 
-// ============================================================================= parity_stream2
-// Second-generation streaming operator: each thread owns TWO consecutive z node columns and the two
-// elements starting at them, processed as a pair (packed f32x2 arithmetic in FP32).  A warp covers
-// 64 z columns (62 owned), so the z-direction shuffle exchange is halved per element and addressing
-// and loop overheads are shared by two elements.  The plane loop is unrolled by two with two
-// prefetch register sets, so every plane's loads are issued two steps before they are used.  The
-// halo warp (last row) only supplies its x-stage to the row above it and skips all element work.
-// Same algebra, ownership and determinism as parity_stream.
-template <typename TC> struct Stream2Cfg;
-template <> struct Stream2Cfg<float> { static constexpr int NW = 12; };
-template <> struct Stream2Cfg<double> { static constexpr int NW = 8; };
-constexpr int TZ2 = 62;                        // owned node columns per CTA (64 per warp, 2 per lane)
-
+// ============================================================================= packed coefficients
 template <typename TC> struct Blocks2 { typename Coef<TC>::type c[72]; };
 
-template <typename TC, typename TU, typename TE, typename TY>
+template <typename TC, typename TU, typename TE, typename TY, typename TR = TY>
 struct OpArgs2 {
-    OpArgs<TC, TU, TE, TY> a;
+    OpArgs<TC, TU, TE, TY, TR> a;
     Blocks2<TC> C2;
 };
-
-template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
-struct Stream2 {
-    static constexpr int NWS = Stream2Cfg<TC>::NW;
-    static constexpr int TYS = NWS - 2;
-    using P = V2<TC>;
-    using Raw = typename Storage<TY>::raw_t;
-    // raw loads of one node plane (two columns) and the element plane after it
-    struct Plane {
-        typename Storage<TU>::raw_t u0[3], u1[3];
-        typename Storage<TE>::raw_t e0, e1;
-        uint8_t m0, m1;
-    };
-};
-
-template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
-__global__ void __launch_bounds__(Stream2Cfg<TC>::NW * 32, 1)
-parity_stream2(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
-    using S2 = Stream2<TC, TU, TE, TY, EPI, MASK>;
-    constexpr int NWS = S2::NWS;
-    constexpr int TYS = S2::TYS;
-    using P = typename S2::P;
-    using Plane = typename S2::Plane;
-    const auto& a = args.a;
-    const int lane = threadIdx.x & 31;
-    const int row = threadIdx.x >> 5;
-    const Grid g = a.g;
-    const int jz = 2 * lane;                                   // tile column of this thread's column 0
-    const int iz0 = blockIdx.x * TZ2 - 1 + jz;
-    const int iy = blockIdx.y * TYS - 1 + row;
-    const int x0 = blockIdx.z * a.cx;
-    const int x1 = min(x0 + a.cx, g.nx + 1);
-    const bool row_in = iy >= 0 && iy <= g.ny;
-    const bool in0 = row_in && iz0 >= 0 && iz0 <= g.nz;
-    const bool in1 = row_in && iz0 + 1 >= 0 && iz0 + 1 <= g.nz;
-    const bool own_row = row >= 1 && row <= TYS;
-    const bool own0 = own_row && in0 && jz >= 1 && jz <= TZ2;
-    const bool own1 = own_row && in1 && jz + 1 >= 1 && jz + 1 <= TZ2;
-    const bool erow = iy >= 0 && iy < g.ny && row < NWS - 1;
-    const bool el0 = erow && iz0 >= 0 && iz0 < g.nz;                       // element at column 0
-    const bool el1 = erow && iz0 + 1 >= 0 && iz0 + 1 < g.nz && jz + 1 < 63;  // element at column 1
-    const bool compute = row < NWS - 1;                                    // warp-uniform
-    const int rown = row + 1 < NWS ? row + 1 : row;
-    const int rowp = row > 0 ? row - 1 : 0;
-
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    P* xs = reinterpret_cast<P*>(smem_raw);
-    P* hs = xs + NWS * 6 * 32;
-#define XS2(r, k) xs[((r) * 6 + (k)) * 32 + lane]
-#define HS2(r, k) hs[((r) * 6 + (k)) * 32 + lane]
-
-    // Per-thread base pointers at CLAMPED (always in-bounds) positions.  Loads are issued two plane
-    // steps ahead into registers that nothing touches until the step that consumes them: validity,
-    // Dirichlet masking and pair packing are applied there, so no instruction waits on a load early.
-    const int64_t plane_nodes = int64_t(g.ny + 1) * (g.nz + 1);
-    const int64_t plane_elems = int64_t(g.ny) * g.nz;
-    const int iyc = min(max(iy, 0), g.ny), iye = min(max(iy, 0), g.ny - 1);
-    const int izc0 = min(max(iz0, 0), g.nz), izc1 = min(max(iz0 + 1, 0), g.nz);
-    const int ize0 = min(max(iz0, 0), g.nz - 1), ize1 = min(max(iz0 + 1, 0), g.nz - 1);
-    const int64_t c0 = int64_t(iyc) * (g.nz + 1) + izc0, c1 = int64_t(iyc) * (g.nz + 1) + izc1;
-    const TU* ub0 = a.u + 3 * c0;
-    const TU* ub1 = a.u + 3 * c1;
-    const TE* eb0 = a.E + int64_t(iye) * g.nz + ize0;
-    const TE* eb1 = a.E + int64_t(iye) * g.nz + ize1;
-    const uint8_t* mb0 = a.node_mask + c0;
-    const uint8_t* mb1 = a.node_mask + c1;
-    const int64_t col = int64_t(iy) * (g.nz + 1) + iz0;          // unclamped: owners only
-
-    auto load_plane = [&](int ix, Plane& pl) {
-        const int ixc = min(max(ix, 0), g.nx), exc = min(max(ix, 0), g.nx - 1);
-        const int64_t on = 3 * plane_nodes * ixc, oe = plane_elems * exc;
-        #pragma unroll
-        for (int k = 0; k < 3; ++k) { pl.u0[k] = Storage<TU>::raw(ub0 + on + k); pl.u1[k] = Storage<TU>::raw(ub1 + on + k); }
-        pl.e0 = Storage<TE>::raw(eb0 + oe);
-        pl.e1 = Storage<TE>::raw(eb1 + oe);
-        if constexpr (MASK == MASK_NODE) { pl.m0 = mb0[plane_nodes * ixc]; pl.m1 = mb1[plane_nodes * ixc]; }
-    };
-
-    P up[3], uprev_raw[3], carry[3];
-    #pragma unroll
-    for (int k = 0; k < 3; ++k) { up[k] = mk2(TC(0), TC(0)); uprev_raw[k] = up[k]; carry[k] = up[k]; }
-    unsigned bits_prev = 077u;
-    P Eprev = mk2(TC(0), TC(0));                  // modulus of element plane ix - 1
-    double acc = 0.0;
-
-    // one plane step; `cur` holds the raw loads of plane ix and is refilled with plane ix + 2
-    auto step = [&](int ix, Plane& cur) {
-        const int64_t nout = int64_t(ix - 1) * plane_nodes + col;   // node plane ix - 1, column 0
-        const bool out_now = ix - 1 >= x0 && (own0 || own1);
-        // epilogue operands of node plane ix - 1, from clamped addresses (used by owners only)
-        typename S2::Raw rr0[3], rr1[3], dd0[3], dd1[3];
-        if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
-            const int64_t oo = 3 * plane_nodes * min(max(ix - 1, 0), g.nx);
-            const TY* r0 = a.r + 3 * c0 + oo;
-            const TY* r1 = a.r + 3 * c1 + oo;
-            #pragma unroll
-            for (int k = 0; k < 3; ++k) { rr0[k] = Storage<TY>::raw(r0 + k); rr1[k] = Storage<TY>::raw(r1 + k); }
-            if constexpr (EPI == EPI_JACOBI) {
-                const TY* d0 = a.invd + 3 * c0 + oo;
-                const TY* d1 = a.invd + 3 * c1 + oo;
-                #pragma unroll
-                for (int k = 0; k < 3; ++k) { dd0[k] = Storage<TY>::raw(d0 + k); dd1[k] = Storage<TY>::raw(d1 + k); }
-            }
-        }
-        // consume plane ix
-        const bool vplane = ix >= 0 && ix <= g.nx, veplane = ix >= 0 && ix < g.nx;
-        const bool v0 = vplane && in0, v1 = vplane && in1;
-        unsigned bits_cur = 077u;
-        if constexpr (MASK == MASK_NODE) bits_cur = (v0 ? unsigned(cur.m0) : 7u) | ((v1 ? unsigned(cur.m1) : 7u) << 3);
-        P ucur[3], uraw[3];
-        #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const TC a0 = v0 ? TC(Storage<TU>::cvt(cur.u0[k])) : TC(0);
-            const TC a1 = v1 ? TC(Storage<TU>::cvt(cur.u1[k])) : TC(0);
-            uraw[k] = mk2(a0, a1);
-            ucur[k] = mk2(((bits_cur >> k) & 1u) ? a0 : TC(0), ((bits_cur >> (3 + k)) & 1u) ? a1 : TC(0));
-        }
-        const P Ecur = mk2(veplane && el0 ? TC(Storage<TE>::cvt(cur.e0)) : TC(0),
-                           veplane && el1 ? TC(Storage<TE>::cvt(cur.e1)) : TC(0));
-        if (ix + 2 <= x1) load_plane(ix + 2, cur);
-
-        if (ix >= x0) {
-            // ---- X stage (edge ix-1 -> ix) for both columns
-            P X0[3], X1[3];
-            #pragma unroll
-            for (int k = 0; k < 3; ++k) { X0[k] = add2(up[k], ucur[k]); X1[k] = sub2(up[k], ucur[k]); }
-            #pragma unroll
-            for (int k = 0; k < 3; ++k) { XS2(row, k) = X0[k]; XS2(row, 3 + k) = X1[k]; }
-            __syncthreads();
-            P H0[3][2];
-            if (compute) {
-                // ---- Y stage for columns 0 and 1
-                P Y[3][2][2];
-                #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const P b0 = XS2(rown, k), b1 = XS2(rown, 3 + k);
-                    Y[k][0][0] = add2(X0[k], b0); Y[k][0][1] = sub2(X0[k], b0);
-                    Y[k][1][0] = add2(X1[k], b1); Y[k][1][1] = sub2(X1[k], b1);
-                }
-                // ---- Z stage for the element pair A = (col0, col1), B = (col1, col2), modulus folded
-                const P E = Eprev;
-                const P nE = mk2(-E.lo(), -E.hi());
-                P v[3][8];
-                #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    #pragma unroll
-                    for (int px = 0; px < 2; ++px) {
-                        #pragma unroll
-                        for (int py = 0; py < 2; ++py) {
-                            const P ya = Y[k][px][py];                                        // (Y0, Y1)
-                            const P yb = mk2(ya.hi(), __shfl_down_sync(0xffffffffu, ya.lo(), 1)); // (Y1, Y2)
-                            const P ea = mul2(E, ya);
-                            const int p = px + 2 * py;
-                            if (p != 0) v[k][p] = fma2(E, yb, ea);
-                            v[k][p + 4] = fma2(nE, yb, ea);
-                        }
-                    }
-                    v[k][0] = mk2(TC(0), TC(0));
-                }
-                // ---- parity-block product (coefficients from the parameter bank)
-                #pragma unroll
-                for (int gi = 0; gi < 8; ++gi) {
-                    const int pa[3] = {gi ^ 1, gi ^ 2, gi ^ 4};
-                    const P in[3] = {v[0][pa[0]], v[1][pa[1]], v[2][pa[2]]};
-                    #pragma unroll
-                    for (int r = 0; r < 3; ++r) {
-                        if (pa[r] == 0) continue;
-                        P sacc = mk2(TC(0), TC(0));
-                        bool first = true;
-                        #pragma unroll
-                        for (int cc = 0; cc < 3; ++cc) {
-                            if (!parity_nonzero(gi, r, cc)) continue;
-                            const auto coef = args.C2.c[9 * gi + 3 * r + cc];
-                            sacc = first ? cmul2(coef, in[cc]) : cfma2(coef, in[cc], sacc);
-                            first = false;
-                        }
-                        v[r][pa[r]] = sacc;
-                    }
-                }
-                // ---- inverse Z: faces of columns 0 and 1 (column 2's share goes to lane + 1)
-                P FY[3][2][2];
-                #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    #pragma unroll
-                    for (int px = 0; px < 2; ++px) {
-                        #pragma unroll
-                        for (int py = 0; py < 2; ++py) {
-                            const int p = px + 2 * py;
-                            const P f1 = v[k][p + 4];
-                            if (p == 0) {
-                                const TC from = __shfl_up_sync(0xffffffffu, f1.hi(), 1);
-                                FY[k][px][py] = sub2(f1, mk2(from, f1.lo()));
-                            } else {
-                                const P f0 = v[k][p];
-                                const P g0 = add2(f0, f1), g1 = sub2(f0, f1);    // (G0_A, G0_B), (G1_A, G1_B)
-                                const TC from = __shfl_up_sync(0xffffffffu, g1.hi(), 1);
-                                FY[k][px][py] = add2(mk2(g0.lo(), g1.lo()), mk2(from, g0.hi()));
-                            }
-                        }
-                    }
-                }
-                // ---- inverse Y
-                #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    #pragma unroll
-                    for (int px = 0; px < 2; ++px) {
-                        H0[k][px] = add2(FY[k][px][0], FY[k][px][1]);
-                        HS2(row, 3 * px + k) = sub2(FY[k][px][0], FY[k][px][1]);
-                    }
-                }
-            }
-            __syncthreads();
-            if (compute) {
-                P yout[3];
-                #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const P zero = mk2(TC(0), TC(0));
-                    const P fx0 = add2(H0[k][0], row > 0 ? HS2(rowp, k) : zero);
-                    const P fx1 = add2(H0[k][1], row > 0 ? HS2(rowp, 3 + k) : zero);
-                    yout[k] = add2(carry[k], add2(fx0, fx1));
-                    carry[k] = sub2(fx0, fx1);
-                }
-                if (out_now) {
-                    #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
-                        if (!(c == 0 ? own0 : own1)) continue;
-                        TY* yo = a.y + 3 * (nout + c);
-                        #pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            const TC yv = c == 0 ? yout[k].lo() : yout[k].hi();
-                            const TC xr = c == 0 ? uprev_raw[k].lo() : uprev_raw[k].hi();
-                            const bool fr = (bits_prev >> (3 * c + k)) & 1u;
-                            const TC ax = (MASK == MASK_NONE || fr) ? yv : xr;
-                            TC o;
-                            if constexpr (EPI == EPI_RAW) {
-                                o = ax;
-                            } else if constexpr (EPI == EPI_APPLY_DOT) {
-                                o = ax;
-                                acc += double(xr) * double(ax);
-                            } else if constexpr (EPI == EPI_JACOBI) {
-                                const TC r_ = TC(Storage<TY>::cvt(c == 0 ? rr0[k] : rr1[k]));
-                                const TC d_ = TC(Storage<TY>::cvt(c == 0 ? dd0[k] : dd1[k]));
-                                o = xr + a.omega * d_ * (r_ - ax);
-                            } else if constexpr (EPI == EPI_RESIDUAL) {
-                                const TC r_ = TC(Storage<TY>::cvt(c == 0 ? rr0[k] : rr1[k]));
-                                o = fr ? r_ - ax : TC(0);
-                            } else {
-                                const TC r_ = TC(Storage<TY>::cvt(c == 0 ? rr0[k] : rr1[k]));
-                                o = r_ - ax;
-                                acc += double(o) * double(o);
-                            }
-                            Storage<TY>::store(yo + k, o);
-                        }
-                    }
-                }
-            }
-        }
-        #pragma unroll
-        for (int k = 0; k < 3; ++k) { up[k] = ucur[k]; uprev_raw[k] = uraw[k]; }
-        bits_prev = bits_cur;
-        Eprev = Ecur;
-    };
-
-    Plane pa_, pb_;                               // planes ix (even steps) and ix + 1 (odd steps)
-    load_plane(x0 - 1, pa_);
-    load_plane(x0, pb_);
-    int ix = x0 - 1;
-    for (; ix + 1 <= x1; ix += 2) {
-        step(ix, pa_);
-        step(ix + 1, pb_);
-    }
-    if (ix <= x1) step(ix, pa_);
-    if constexpr (EPI == EPI_TRUE_RES || EPI == EPI_APPLY_DOT) {
-        const int64_t bid = (int64_t(blockIdx.z) * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-        block_sum_store<NWS * 32>(acc, a.partials + bid);
-    }
-#undef XS2
-#undef HS2
-}
 
 // ============================================================================= parity_stream_xp
 // Third-generation streaming operator: one z node column per thread, TWO consecutive element
@@ -609,21 +320,21 @@ template <typename TC> struct XpCfg;
 template <> struct XpCfg<float> { static constexpr int NW = 16; };
 template <> struct XpCfg<double> { static constexpr int NW = 8; };
 
-template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
+template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK>
 struct XpPlane {
     typename Storage<TU>::raw_t u1[3], u2[3];       // node planes e+1, e+2
     typename Storage<TE>::raw_t e0, e1;             // element planes e, e+1
     uint8_t m1, m2;
-    typename Storage<TY>::raw_t r0[3], r1[3], d0[3], d1[3];   // epilogue operands, node planes e, e+1
+    typename Storage<TR>::raw_t r0[3], r1[3], d0[3], d1[3];   // epilogue operands, node planes e, e+1
 };
 
-template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK>
+template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK>
 __global__ void __launch_bounds__(XpCfg<TC>::NW * 32, 1)
-parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
+parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
     constexpr int NWS = XpCfg<TC>::NW;
     constexpr int TYS = NWS - 2;
     using P = V2<TC>;
-    using Plane = XpPlane<TC, TU, TE, TY, EPI, MASK>;
+    using Plane = XpPlane<TC, TU, TE, TY, TR, EPI, MASK>;
     const auto& a = args.a;
     const int lane = threadIdx.x & 31;
     const int row = threadIdx.x >> 5;
@@ -669,15 +380,15 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
             pl.m2 = mb[plane_nodes * nplane(e + 2)];
         }
         if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
-            const TY* r0 = a.r + 3 * cn + 3 * plane_nodes * nplane(e);
-            const TY* r1 = a.r + 3 * cn + 3 * plane_nodes * nplane(e + 1);
+            const TR* r0 = a.r + 3 * cn + 3 * plane_nodes * nplane(e);
+            const TR* r1 = a.r + 3 * cn + 3 * plane_nodes * nplane(e + 1);
             #pragma unroll
-            for (int k = 0; k < 3; ++k) { pl.r0[k] = Storage<TY>::raw(r0 + k); pl.r1[k] = Storage<TY>::raw(r1 + k); }
+            for (int k = 0; k < 3; ++k) { pl.r0[k] = Storage<TR>::raw(r0 + k); pl.r1[k] = Storage<TR>::raw(r1 + k); }
             if constexpr (EPI == EPI_JACOBI) {
-                const TY* d0 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e);
-                const TY* d1 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e + 1);
+                const TR* d0 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e);
+                const TR* d1 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e + 1);
                 #pragma unroll
-                for (int k = 0; k < 3; ++k) { pl.d0[k] = Storage<TY>::raw(d0 + k); pl.d1[k] = Storage<TY>::raw(d1 + k); }
+                for (int k = 0; k < 3; ++k) { pl.d0[k] = Storage<TR>::raw(d0 + k); pl.d1[k] = Storage<TR>::raw(d1 + k); }
             }
         }
     };
@@ -723,9 +434,9 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
         if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
             #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                rr0[k] = TC(Storage<TY>::cvt(cur.r0[k]));
-                rr1[k] = TC(Storage<TY>::cvt(cur.r1[k]));
-                if constexpr (EPI == EPI_JACOBI) { dd0[k] = TC(Storage<TY>::cvt(cur.d0[k])); dd1[k] = TC(Storage<TY>::cvt(cur.d1[k])); }
+                rr0[k] = TC(Storage<TR>::cvt(cur.r0[k]));
+                rr1[k] = TC(Storage<TR>::cvt(cur.r1[k]));
+                if constexpr (EPI == EPI_JACOBI) { dd0[k] = TC(Storage<TR>::cvt(cur.d0[k])); dd1[k] = TC(Storage<TR>::cvt(cur.d1[k])); }
             }
         }
         if (e + 2 <= x1 - 1) load_step(e + 2, cur);          // refill: next step's planes
@@ -881,9 +592,9 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY> args) {
 #undef HSP
 }
 
-// CTA tiling of the streaming operators: parity_stream2 (author layout, node or no mask) tiles
-// (y, z) node columns as (NW-2) x 62; parity_stream (natural-layout / SIMP / DOF-mask product) as
-// 14 x 30.  x-chunk: the longest chunk (least halo recomputation) with >= 4 CTAs per SM.
+// CTA tiling of the streaming operators: parity_stream_xp (author layout, node or no mask) tiles
+// (y, z) node columns as (NW-2) x 30 with NW = 16 (FP32) or 8 (FP64) warps; parity_stream
+// (natural-layout / SIMP / DOF-mask product) as 14 x 30.  x-chunk: the longest chunk (least halo recomputation) with >= 4 CTAs per SM.
 struct Tiling { int tz, ty; };
 inline Tiling tiling(int prec, bool v2) {
     if (!v2) return {TZ, TYR};
@@ -908,16 +619,17 @@ int64_t stream_ctas(const Grid& g, int prec) {
     return int64_t(d.x) * d.y * d.z;
 }
 
-template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP>
-int launch_stream(const OpArgs<TC, TU, TE, TY>& a_in, cudaStream_t s, const char* what) {
+template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP, typename TR = TY>
+int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const char* what) {
     constexpr bool v2 = !REV && !SIMP && MASK != MASK_DOF;
-    OpArgs<TC, TU, TE, TY> a = a_in;
+    static_assert(v2 || std::is_same<TR, TY>::value, "parity_stream takes r and invd of the output type");
+    OpArgs<TC, TU, TE, TY, TR> a = a_in;
     const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
     a.cx = stream_cx(a.g, t);
     size_t smem, threads;
     const void* kern;
     if constexpr (v2) {
-        kern = (const void*)parity_stream_xp<TC, TU, TE, TY, EPI, MASK>;
+        kern = (const void*)parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK>;
         threads = XpCfg<TC>::NW * 32;
         smem = size_t(2) * XpCfg<TC>::NW * 6 * 32 * sizeof(V2<TC>);
     } else {
@@ -938,13 +650,13 @@ int launch_stream(const OpArgs<TC, TU, TE, TY>& a_in, cudaStream_t s, const char
         configured = true;
     }
     if constexpr (v2) {
-        OpArgs2<TC, TU, TE, TY> a2;
+        OpArgs2<TC, TU, TE, TY, TR> a2;
         a2.a = a;
         for (int i = 0; i < 72; ++i) {
             if constexpr (std::is_same<TC, float>::value) a2.C2.c[i] = make_float2(a.C.c[i], a.C.c[i]);
             else a2.C2.c[i] = a.C.c[i];
         }
-        parity_stream_xp<TC, TU, TE, TY, EPI, MASK><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+        parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
     } else {
         parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a);
     }
@@ -1079,28 +791,19 @@ extern "C" int vx_matvec(int prec, int nx, int ny, int nz, const double* blocks,
     int st = check_grid(nx, ny, nz);
     if (st) return st;
     VX_CHECK_ARG(blocks && E && u && y, VX_ERR_NULL_POINTER, "vx_matvec: NULL pointer");
-    Grid g{nx, ny, nz};
-    if (prec == VX_F64) {
-        OpArgs<double, double, double, double> a{};
-        a.g = g; a.u = (const double*)u; a.E = (const double*)E; a.y = (double*)y; a.node_mask = node_mask;
-        a.C = convert_blocks<double>(blocks);
-        return node_mask ? launch_stream<double, double, double, double, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
-                         : launch_stream<double, double, double, double, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
-    } else if (prec == VX_F32) {
-        OpArgs<float, float, float, float> a{};
-        a.g = g; a.u = (const float*)u; a.E = (const float*)E; a.y = (float*)y; a.node_mask = node_mask;
-        a.C = convert_blocks<float>(blocks);
-        return node_mask ? launch_stream<float, float, float, float, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
-                         : launch_stream<float, float, float, float, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
-    } else if (prec == VX_BF16_F32) {
-        OpArgs<float, __nv_bfloat16, __nv_bfloat16, float> a{};
-        a.g = g; a.u = (const __nv_bfloat16*)u; a.E = (const __nv_bfloat16*)E; a.y = (float*)y; a.node_mask = node_mask;
-        a.C = convert_blocks<float>(blocks);
-        return node_mask ? launch_stream<float, __nv_bfloat16, __nv_bfloat16, float, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
-                         : launch_stream<float, __nv_bfloat16, __nv_bfloat16, float, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
-    }
-    set_error("vx_matvec: unknown precision %d", prec);
-    return VX_ERR_INVALID_ARGUMENT;
+    int rc = VX_OK;
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using X = typename decltype(t)::X;                 // operand u: an iterate
+        using M = typename decltype(t)::M;
+        using TC = arith_t<X>;                              // y in the arithmetic type
+        OpArgs<TC, X, M, TC> a{};
+        a.g = Grid{nx, ny, nz}; a.u = (const X*)u; a.E = (const M*)E; a.y = (TC*)y; a.node_mask = node_mask;
+        a.C = convert_blocks<TC>(blocks);
+        rc = node_mask ? launch_stream<TC, X, M, TC, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
+                       : launch_stream<TC, X, M, TC, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_matvec: unknown precision %d", prec);
+    return rc;
 }
 
 extern "C" int vx_modal8(const double* blocks, const double* E, const double* u, double* y,
@@ -1229,19 +932,9 @@ extern "C" int vx_product(int nx, int ny, int nz, const double* rho, const doubl
 
 // Fused smoother / residual / outer-CG operator forms (author layout, node mask optional).
 namespace {
-template <int EPI, typename T>
-int fused_op(const char* what, int nx, int ny, int nz, const double* blocks, const void* E,
-             const uint8_t* node_mask, const void* x, const void* r, const void* invd, double omega,
-             void* out, double* partials, cudaStream_t stream) {
-    OpArgs<T, T, T, T> a{};
-    a.g = Grid{nx, ny, nz};
-    a.u = (const T*)x; a.E = (const T*)E; a.y = (T*)out; a.node_mask = node_mask;
-    a.r = (const T*)r; a.invd = (const T*)invd; a.omega = T(omega); a.partials = partials;
-    a.C = convert_blocks<T>(blocks);
-    return node_mask ? launch_stream<T, T, T, T, EPI, MASK_NODE, false, false>(a, stream, what)
-                     : launch_stream<T, T, T, T, EPI, MASK_NONE, false, false>(a, stream, what);
-}
-
+// The fused smoother / residual / reducing forms.  Operand x and the Jacobi output are iterates;
+// the right-hand side, the inverse diagonal and the residual output are auxiliary vectors; the
+// reducing forms (apply_dot, true_residual) exist for VX_F64 and VX_F32.
 template <int EPI>
 int fused_dispatch(const char* what, int prec, int nx, int ny, int nz, const double* blocks, const void* E,
                    const uint8_t* node_mask, const void* x, const void* r, const void* invd, double omega,
@@ -1250,12 +943,32 @@ int fused_dispatch(const char* what, int prec, int nx, int ny, int nz, const dou
     if (st) return st;
     VX_CHECK_ARG(blocks && E && x && out, VX_ERR_NULL_POINTER, "%s: NULL pointer", what);
     VX_CHECK_ARG(x != out, VX_ERR_INVALID_ARGUMENT, "%s: output may not alias the operand", what);
-    if (prec == VX_F64)
-        return fused_op<EPI, double>(what, nx, ny, nz, blocks, E, node_mask, x, r, invd, omega, out, partials, stream);
-    if (prec == VX_F32)
-        return fused_op<EPI, float>(what, nx, ny, nz, blocks, E, node_mask, x, r, invd, omega, out, partials, stream);
-    set_error("%s: unsupported precision %d", what, prec);
-    return VX_ERR_INVALID_ARGUMENT;
+    constexpr bool reducing = EPI == EPI_TRUE_RES || EPI == EPI_APPLY_DOT;
+    VX_CHECK_ARG(!reducing || prec == VX_F64 || prec == VX_F32, VX_ERR_INVALID_ARGUMENT,
+                 "%s: unsupported precision %d", what, prec);
+    int rc = VX_OK;
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using X = typename decltype(t)::X;
+        using R = typename decltype(t)::R;
+        using M = typename decltype(t)::M;
+        using TC = arith_t<X>;
+        using TY = std::conditional_t<EPI == EPI_RESIDUAL, R, X>;
+        if constexpr (reducing && !std::is_same<X, R>::value) {
+            rc = VX_ERR_INVALID_ARGUMENT;                   // excluded above
+        } else if constexpr (reducing && std::is_same<X, __nv_bfloat16>::value) {
+            rc = VX_ERR_INVALID_ARGUMENT;
+        } else {
+            OpArgs<TC, X, M, TY, R> a{};
+            a.g = Grid{nx, ny, nz};
+            a.u = (const X*)x; a.E = (const M*)E; a.y = (TY*)out; a.node_mask = node_mask;
+            a.r = (const R*)r; a.invd = (const R*)invd; a.omega = TC(omega); a.partials = partials;
+            a.C = convert_blocks<TC>(blocks);
+            rc = node_mask ? launch_stream<TC, X, M, TY, EPI, MASK_NODE, false, false, R>(a, stream, what)
+                           : launch_stream<TC, X, M, TY, EPI, MASK_NONE, false, false, R>(a, stream, what);
+        }
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "%s: unsupported precision %d", what, prec);
+    return rc;
 }
 }  // namespace
 

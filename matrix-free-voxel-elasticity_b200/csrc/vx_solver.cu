@@ -110,7 +110,7 @@ __global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, con
                                     T* __restrict__ z_old) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const T zi = T(z[i]);
+    const T zi = T(Storage<TZ>::load(z + i));
     p[i] = zi + T(S[S_BETA]) * p[i];
     if (z_old) z_old[i] = zi;
 }
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restr
     const int64_t G = gridDim.x;
     double a = 0.0, b = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
-        const double ri = double(r[i]), zi = double(zn[i]);
+        const double ri = double(r[i]), zi = double(Storage<TZ>::load(zn + i));
         a = fma(ri, zi, a);
         if (zo) b = fma(ri, zi - double(zo[i]), b);
     }
@@ -150,22 +150,26 @@ __global__ void __launch_bounds__(FT) jacobi_precond_dot_kernel(int64_t n, const
 }
 
 // V-cycle entry: r_mg = (TM) r64 (skipped when r_mg is NULL), x = omega * invd * r_mg
-template <typename TM>
-__global__ void vcycle_entry_kernel(int64_t n, const double* __restrict__ r64, TM* __restrict__ rmg,
-                                    const TM* __restrict__ invd, double omega, TM* __restrict__ x) {
+// V-cycle entry: r_mg = r64 in auxiliary storage, x = omega * invd * r_mg (the first pre-sweep from x = 0)
+template <typename TX, typename TR>
+__global__ void vcycle_entry_kernel(int64_t n, const double* __restrict__ r64, TR* __restrict__ rmg,
+                                    const TR* __restrict__ invd, double omega, TX* __restrict__ x) {
+    using A = arith_t<TX>;
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const TM r = TM(r64[i]);
-    if (rmg) rmg[i] = r;
-    x[i] = TM(omega) * invd[i] * r;
+    const A r = A(Storage<TR>::round(arith_t<TR>(r64[i])));   // the level residual as stored
+    if (rmg) Storage<TR>::store(rmg + i, r);
+    Storage<TX>::store(x + i, A(omega) * A(Storage<TR>::load(invd + i)) * r);
 }
 
-template <typename T>
-__global__ void scaled_product_kernel(int64_t n, double omega, const T* __restrict__ a, const T* __restrict__ b,
-                                      T* __restrict__ out) {
+// out = omega * a * b: a, b auxiliary, out an iterate
+template <typename TX, typename TR>
+__global__ void scaled_product_kernel(int64_t n, double omega, const TR* __restrict__ a, const TR* __restrict__ b,
+                                      TX* __restrict__ out) {
+    using A = arith_t<TX>;
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[i] = T(omega) * a[i] * b[i];
+    Storage<TX>::store(out + i, A(omega) * A(Storage<TR>::load(a + i)) * A(Storage<TR>::load(b + i)));
 }
 
 __global__ void set_scalars_kernel(double* S, int first, int count, double value) {
@@ -234,6 +238,9 @@ extern "C" int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, 
         cg_direction_kernel<double, double><<<nb(n, 256), 256, 0, stream>>>(n, S, (const double*)z, (double*)p, (double*)z_old);
     else if (prec == VX_F64 && zprec == VX_F32)
         cg_direction_kernel<double, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (double*)p, (double*)z_old);
+    else if (prec == VX_F64 && zprec == VX_BF16_F32)
+        cg_direction_kernel<double, __nv_bfloat16><<<nb(n, 256), 256, 0, stream>>>(n, S, (const __nv_bfloat16*)z, (double*)p,
+                                                                                   (double*)z_old);
     else if (prec == VX_F32 && zprec == VX_F32)
         cg_direction_kernel<float, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p, (float*)z_old);
     else { set_error("vx_cg_direction: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
@@ -250,6 +257,9 @@ extern "C" int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const v
         dots_pr_kernel<double, double><<<G, FT, 0, stream>>>(n, (const double*)r, (const double*)zn, (const double*)zo, partials);
     else if (prec == VX_F64 && zprec == VX_F32)
         dots_pr_kernel<double, float><<<G, FT, 0, stream>>>(n, (const double*)r, (const float*)zn, (const double*)zo, partials);
+    else if (prec == VX_F64 && zprec == VX_BF16_F32)
+        dots_pr_kernel<double, __nv_bfloat16><<<G, FT, 0, stream>>>(n, (const double*)r, (const __nv_bfloat16*)zn,
+                                                                    (const double*)zo, partials);
     else if (prec == VX_F32 && zprec == VX_F32)
         dots_pr_kernel<float, float><<<G, FT, 0, stream>>>(n, (const float*)r, (const float*)zn, (const float*)zo, partials);
     else { set_error("vx_dots_pr: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
@@ -275,11 +285,12 @@ extern "C" int vx_vcycle_entry(int prec, int64_t n, const double* r64, void* r_m
                                void* x, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry: n must be positive");
     VX_CHECK_ARG(r64 && inv_diag && x, VX_ERR_NULL_POINTER, "vx_vcycle_entry: NULL pointer");
-    if (prec == VX_F64)
-        vcycle_entry_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, r64, (double*)r_mg, (const double*)inv_diag, omega, (double*)x);
-    else if (prec == VX_F32)
-        vcycle_entry_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, r64, (float*)r_mg, (const float*)inv_diag, omega, (float*)x);
-    else { set_error("vx_vcycle_entry: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using X = typename decltype(t)::X;
+        using R = typename decltype(t)::R;
+        vcycle_entry_kernel<X, R><<<nb(n, 256), 256, 0, stream>>>(n, r64, (R*)r_mg, (const R*)inv_diag, omega, (X*)x);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_vcycle_entry");
     return VX_OK;
 }
@@ -288,11 +299,12 @@ extern "C" int vx_scaled_product(int prec, int64_t n, double omega, const void* 
                                  cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_scaled_product: n must be positive");
     VX_CHECK_ARG(a && b && out, VX_ERR_NULL_POINTER, "vx_scaled_product: NULL pointer");
-    if (prec == VX_F64)
-        scaled_product_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, omega, (const double*)a, (const double*)b, (double*)out);
-    else if (prec == VX_F32)
-        scaled_product_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, omega, (const float*)a, (const float*)b, (float*)out);
-    else { set_error("vx_scaled_product: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using X = typename decltype(t)::X;
+        using R = typename decltype(t)::R;
+        scaled_product_kernel<X, R><<<nb(n, 256), 256, 0, stream>>>(n, omega, (const R*)a, (const R*)b, (X*)out);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_scaled_product: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_scaled_product");
     return VX_OK;
 }

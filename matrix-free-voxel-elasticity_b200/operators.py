@@ -20,6 +20,9 @@ from .element import Modal
 from .layout import n_elems, n_nodes
 
 PREC = {torch.float64: _lib.VX_F64, torch.float32: _lib.VX_F32, torch.bfloat16: _lib.VX_BF16_F32}
+# (iterate dtype, auxiliary dtype) -> storage selector; the modulus is stored like the auxiliary vectors
+STORAGE = {(torch.float64, torch.float64): _lib.VX_F64, (torch.float32, torch.float32): _lib.VX_F32,
+           (torch.bfloat16, torch.bfloat16): _lib.VX_BF16_F32, (torch.float32, torch.bfloat16): _lib.VX_F32_BF16AUX}
 
 
 def stream_ptr(device=None) -> int:
@@ -60,18 +63,21 @@ def dofs_from_node_mask(node_mask: torch.Tensor, dtype=torch.float64) -> torch.T
 
 class VoxelOperator:
     """K(E) on a (nx, ny, nz) voxel grid in `dtype` storage (float64, float32, or bfloat16 with
-    FP32 arithmetic for the raw product)."""
+    FP32 arithmetic).  `aux_dtype` (default `dtype`) is the storage of the modulus and of the
+    auxiliary vectors (right-hand side, inverse diagonal, residual output); float32 iterates with
+    bfloat16 auxiliaries is the VX_F32_BF16AUX mode."""
 
-    def __init__(self, shape, ke, dtype=torch.float64):
+    def __init__(self, shape, ke, dtype=torch.float64, aux_dtype=None):
         self.shape = tuple(int(s) for s in shape)
         if len(self.shape) != 3 or min(self.shape) < 1:
             raise ValueError(f"invalid grid {shape}")
         self.ke = np.ascontiguousarray(np.asarray(ke, dtype=np.float64).reshape(24, 24))
         self.blocks = np.ascontiguousarray(Modal(self.ke).blocks.reshape(72))
-        if dtype not in PREC:
-            raise ValueError(f"unsupported dtype {dtype}")
-        self.dtype = dtype
-        self.prec = PREC[dtype]
+        aux_dtype = dtype if aux_dtype is None else aux_dtype
+        if (dtype, aux_dtype) not in STORAGE:
+            raise ValueError(f"unsupported storage: iterate {dtype}, auxiliary {aux_dtype}")
+        self.dtype, self.aux_dtype = dtype, aux_dtype
+        self.prec = STORAGE[(dtype, aux_dtype)]
         self.nodes = n_nodes(self.shape)
         self.ndof = 3 * self.nodes
         self.n_elem = n_elems(self.shape)
@@ -88,7 +94,7 @@ class VoxelOperator:
         return _ptr(t, what, dtype or self.dtype, self.ndof)
 
     def _E(self, E, dtype=None):
-        return _ptr(E, "E", dtype or self.dtype, self.n_elem)
+        return _ptr(E, "E", dtype or self.aux_dtype, self.n_elem)
 
     def _mask(self, m):
         return _ptr(m, "node_mask", torch.uint8, self.nodes, allow_none=True)
@@ -126,18 +132,20 @@ class VoxelOperator:
         return d
 
     def jacobi(self, x, r, inv_diag, E, node_mask, omega, out=None):
-        """out = x + omega * inv_diag * (r - A x), A the Dirichlet operator."""
-        o = self._out(out)
+        """out = x + omega * inv_diag * (r - A x), A the Dirichlet operator (bfloat16: every
+        vector in bf16, FP32 arithmetic)."""
+        o = self._out(out, self.dtype)
         _lib.call("vx_jacobi_sweep", self.prec, *self.shape, self._bp, self._E(E), self._mask(node_mask),
-                  self._vec(x, "x"), self._vec(r, "r"), self._vec(inv_diag, "inv_diag"), float(omega),
-                  self._vec(o, "out"), stream_ptr())
+                  self._vec(x, "x"), self._vec(r, "r", self.aux_dtype), self._vec(inv_diag, "inv_diag", self.aux_dtype),
+                  float(omega), self._vec(o, "out"), stream_ptr())
         return o
 
     def residual(self, x, r, E, node_mask, out=None):
         """out = (r - A x) * M."""
-        o = self._out(out)
+        o = self._out(out, self.aux_dtype)
         _lib.call("vx_residual", self.prec, *self.shape, self._bp, self._E(E), self._mask(node_mask),
-                  self._vec(x, "x"), self._vec(r, "r"), self._vec(o, "out"), stream_ptr())
+                  self._vec(x, "x"), self._vec(r, "r", self.aux_dtype), self._vec(o, "out", self.aux_dtype),
+                  stream_ptr())
         return o
 
     def apply_dot(self, p, E, node_mask, q, partials):

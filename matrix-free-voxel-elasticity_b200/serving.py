@@ -55,13 +55,14 @@ def footprint_estimate(shape, precision="mixed", levels=None, max_coarse_x=16) -
     shapes = hierarchy_shapes(shape, max_coarse_x)
     if levels is not None:
         shapes = shapes[:levels]
-    es = 8 if precision == "fp64" else 4
+    ex, ea = {"fp64": (8, 8), "bf16": (4, 2), "bf16-all": (2, 2)}.get(precision, (4, 4))   # iterate, auxiliary
     total = 0
     for i, (nx, ny, nz) in enumerate(shapes):
         nodes, elems = (nx + 1) * (ny + 1) * (nz + 1), nx * ny * nz
         if i == 0:
             total += 6 * 24 * nodes + 2 * 8 * elems        # b x r p q z_old; E and its owned copy
-        total += 4 * 3 * es * nodes + elems * (8 + es) + nodes
+        res = 0 if ex == ea else 3 * ea * nodes            # separate residual buffer
+        total += 3 * nodes * (2 * ex + 2 * ea) + res + elems * (8 + ea) + nodes
     nx, ny, nz = shapes[-1]
     nc = 3 * (nx + 1) * (ny + 1) * (nz + 1)
     return int(total + 3 * 8 * nc * nc + (64 << 20))   # A, its factor, its inverse; workspace margin

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .operators import PREC, VoxelOperator, _ptr, stream_ptr
+from .operators import PREC, STORAGE, VoxelOperator, _ptr, stream_ptr
 
 # scalar slots of S (csrc/vx_solver.cu)
 (S_RZ, S_PQ, S_ALPHA, S_RR, S_REL, S_NB, S_BETA, S_RZN, S_RZD, S_TOL, S_DONE, S_IT, S_MAXIT, S_MV,
@@ -46,21 +46,28 @@ def all_free_mask(shape, device="cuda"):
 
 
 class _Level:
-    __slots__ = ("shape", "op", "op64", "E64", "E", "mask", "invd", "omega", "r", "x", "xt", "n")
+    __slots__ = ("shape", "op", "op64", "E64", "E", "mask", "invd", "omega", "r", "x", "xt", "res", "n")
 
 
 class MGHierarchy:
     """Rediscretised geometric multigrid (src/voxel_mg.py:1-21,74-178): level l has element matrix
     ke * 2^l, modulus the 2x2x2 mean of level l-1, mask injected from level l-1; damped Jacobi
     V(pre, post) in `dtype` (float64 or float32); the coarsest level is solved in FP64 with the
-    inverse of its dense constrained matrix (from an FP64 Cholesky factorisation)."""
+    inverse of its dense constrained matrix (from an FP64 Cholesky factorisation).
+
+    BF16 storage (no reference counterpart), FP32 arithmetic in both: aux_dtype=bfloat16 stores the
+    level moduli and the auxiliary vectors (right-hand sides, residuals, inverse diagonals) in bf16
+    and keeps the iterates in `dtype` float32; dtype=bfloat16 stores the iterates in bf16 too.  The
+    coarsest solve accumulates in FP64 either way."""
 
     def __init__(self, shape, ke, E, node_mask=None, dtype=torch.float32, pre=2, post=2, omegas=None,
-                 max_coarse_x=16, shapes=None):
-        if dtype not in (torch.float64, torch.float32):
-            raise ValueError("the V-cycle runs in float64 or float32")
+                 max_coarse_x=16, shapes=None, aux_dtype=None):
+        aux_dtype = dtype if aux_dtype is None else aux_dtype
+        if (dtype, aux_dtype) not in STORAGE:
+            raise ValueError(f"unsupported V-cycle storage: iterate {dtype}, auxiliary {aux_dtype}")
         self.shapes = [tuple(s) for s in (shapes or hierarchy_shapes(shape, max_coarse_x))]
-        self.dtype, self.prec, self.pre, self.post = dtype, PREC[dtype], int(pre), int(post)
+        self.dtype, self.aux_dtype = dtype, aux_dtype
+        self.prec, self.pre, self.post = STORAGE[(dtype, aux_dtype)], int(pre), int(post)
         self.ke = np.asarray(ke, dtype=np.float64).reshape(24, 24)
         E64 = E.to(torch.float64).contiguous()
         mask = node_mask if node_mask is not None else all_free_mask(self.shapes[0])
@@ -75,16 +82,18 @@ class MGHierarchy:
                 E64, mask = Ec, mc
             L = _Level()
             L.shape = s
-            L.op = VoxelOperator(s, self.ke * 2 ** i, dtype)
+            L.op = VoxelOperator(s, self.ke * 2 ** i, dtype, aux_dtype)
             L.op64 = L.op if dtype == torch.float64 else VoxelOperator(s, self.ke * 2 ** i, torch.float64)
             L.E64, L.mask = E64, mask
-            L.E = E64 if dtype == torch.float64 else E64.to(dtype)
+            L.E = E64 if aux_dtype == torch.float64 else E64.to(aux_dtype)
             inv64 = L.op64.diagonal(E64, mask, inverse=True)
-            L.invd = inv64 if dtype == torch.float64 else inv64.to(dtype)
+            L.invd = inv64 if aux_dtype == torch.float64 else inv64.to(aux_dtype)
             L.n = L.op.ndof
-            L.r = torch.zeros(L.n, dtype=dtype, device="cuda")
+            L.r = torch.zeros(L.n, dtype=aux_dtype, device="cuda")
             L.x = torch.zeros(L.n, dtype=dtype, device="cuda")
             L.xt = torch.zeros(L.n, dtype=dtype, device="cuda")
+            # the residual goes to the free iterate buffer when both have one storage type
+            L.res = None if aux_dtype == dtype else torch.zeros(L.n, dtype=aux_dtype, device="cuda")
             self.levels.append(L)
         c = self.levels[-1]
         A = torch.empty(c.n, c.n, dtype=torch.float64, device="cuda")
@@ -146,8 +155,9 @@ class MGHierarchy:
     def footprint_bytes(self) -> int:
         b = 0
         for L in self.levels:
-            es = torch.finfo(self.dtype).bits // 8
-            b += L.n * es * 4 + L.E.numel() * es + L.E64.numel() * 8 + L.mask.numel()
+            for t in (L.x, L.xt, L.r, L.invd, L.res, L.E):
+                b += 0 if t is None else t.numel() * t.element_size()
+            b += L.E64.numel() * 8 + L.mask.numel()
         return b + self.A_inv.numel() * 8 * 3
 
     def spectral_omegas(self, iterations=30, seed=20260923):
@@ -176,8 +186,8 @@ class MGHierarchy:
         L0 = self.levels[0]
         if len(self.levels) == 1:
             src = r64
-            if self.dtype != torch.float64:
-                _lib.call("vx_cast", L0.n, _lib.VX_F64, _ptr(r64, "r"), self.prec, L0.r.data_ptr(), 1.0, _s())
+            if self.aux_dtype != torch.float64:
+                _lib.call("vx_cast", L0.n, _lib.VX_F64, _ptr(r64, "r"), PREC[self.aux_dtype], L0.r.data_ptr(), 1.0, _s())
                 src = L0.r
             _lib.call("vx_coarse_apply", self.prec, L0.n, self.A_inv.data_ptr(), src.data_ptr(), L0.mask.data_ptr(),
                       L0.x.data_ptr(), _s())
@@ -199,9 +209,10 @@ class MGHierarchy:
         for _ in range(self.pre - 1):
             L.op.jacobi(bufs[ci], r, L.invd, L.E, L.mask, L.omega, out=bufs[1 - ci])
             ci ^= 1
-        L.op.residual(bufs[ci], r, L.E, L.mask, out=bufs[1 - ci])
+        res = bufs[1 - ci] if L.res is None else L.res
+        L.op.residual(bufs[ci], r, L.E, L.mask, out=res)
         nxt = self.levels[l + 1]
-        _lib.call("vx_restrict", self.prec, *L.shape, bufs[1 - ci].data_ptr(), nxt.mask.data_ptr(), nxt.r.data_ptr(), _s())
+        _lib.call("vx_restrict", self.prec, *L.shape, res.data_ptr(), nxt.mask.data_ptr(), nxt.r.data_ptr(), _s())
         if l + 1 < len(self.levels) - 1:
             _lib.call("vx_scaled_product", self.prec, nxt.n, nxt.omega, nxt.invd.data_ptr(), nxt.r.data_ptr(),
                       nxt.x.data_ptr(), _s())
