@@ -47,6 +47,10 @@ WORKLOADS = {
                 "256 solve requests, Poisson arrivals (seeded, offered load 1.2x the serial FP64 capacity), "
                 "grids uniform from 48x24x24/96x48x48/160x80x80/256x128x128, seeded GRF densities l=8, "
                 "tol uniform from {1e-6, 1e-8}, mixed GMG-PCG V(2,2) omega=0.6, HBM budget 150 GB"),
+    "simp_192x96x96": ((192, 96, 96), ("simp", 0.12, 0), 5,
+                       "SIMP topology optimisation, 100 iterations: cantilever 192x96x96 (5.45M DOF), volume fraction "
+                       "0.12, p=3, start 0.12+U(-0.01,0.01) seed 0, hat filter rmin 1.5, OC move 0.2 bisection to 1e-6, "
+                       "mixed GMG-PCG V(2,2) spectral omega, solves warm-started to 1e-6, 5 levels"),
     "jacobi_32x16x16": ((32, 16, 16), ("uniform", 0), None,
                         "cantilever 32x16x16 (28,611 DOF), uniform(0.01,1) seed 0, Jacobi-PCG, tol 1e-8"),
 }
@@ -62,6 +66,9 @@ def parse():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="gmg_128x64x64")
     ap.add_argument("--no-large", action="store_true", help="skip the 144.6M-DOF section")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler: no CPU baseline, no large")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="launch the CG loop body from the host instead of the WHILE graph (the same kernels; "
+                         "a profiler then lists every launch)")
     ap.add_argument("--kernels", action="store_true",
                     help="only launch the hot kernels on the workload's data (for an ncu capture); prints their times")
     return ap.parse_args()
@@ -180,6 +187,21 @@ def stream_bytes(nodes, elems, vec_bytes, e_bytes, n_vec_in, n_vec_out, mask=Tru
     return nodes * 3 * vec_bytes * (n_vec_in + n_vec_out) + elems * e_bytes + (nodes if mask else 0)
 
 
+def vec_bytes(nodes, elems, vector_sizes, e_bytes, mask=True):
+    """Algorithmic bytes of a launch reading/writing vectors of the given element sizes once each."""
+    return nodes * 3 * sum(vector_sizes) + elems * e_bytes + (nodes if mask else 0)
+
+
+def mg_mode(M):
+    """Short name of a hierarchy's storage mode: f64, f32, bf16 (bf16 auxiliaries) or bf16all."""
+    import torch
+    if M.dtype == torch.bfloat16:
+        return "bf16all"
+    if M.aux_dtype == torch.bfloat16:
+        return "bf16"
+    return "f32" if M.dtype == torch.float32 else "f64"
+
+
 def kernel_table(solver, vx, torch, flush, reps=10):
     """Per-kernel device time and algorithmic bytes of the hot kernels on the solver's own data."""
     fcg, M = solver.fcg, solver.M
@@ -193,12 +215,13 @@ def kernel_table(solver, vx, torch, flush, reps=10):
     rows["true_residual_f64"] = (t, stream_bytes(N, Ne, 8, 8, 2, 1))
     if hasattr(M, "levels") and len(M.levels) > 1:
         L = M.levels[0]
-        es = 4 if M.dtype == torch.float32 else 8
-        name = "f32" if es == 4 else "f64"
+        xb, rb = L.x.element_size(), L.r.element_size()
+        name = mg_mode(M)
         t = kernel_time(lambda: L.op.jacobi(L.x, L.r, L.invd, L.E, L.mask, L.omega, out=L.xt), reps, flush)
-        rows[f"jacobi_sweep_{name}"] = (t, stream_bytes(N, Ne, es, es, 3, 1))
-        t = kernel_time(lambda: L.op.residual(L.x, L.r, L.E, L.mask, out=L.xt), reps, flush)
-        rows[f"residual_{name}"] = (t, stream_bytes(N, Ne, es, es, 2, 1))
+        rows[f"jacobi_sweep_{name}"] = (t, vec_bytes(N, Ne, (xb, rb, rb, xb), rb))
+        res = L.xt if L.res is None else L.res
+        t = kernel_time(lambda: L.op.residual(L.x, L.r, L.E, L.mask, out=res), reps, flush)
+        rows[f"residual_{name}"] = (t, vec_bytes(N, Ne, (xb, rb, rb), rb))
     return rows
 
 
@@ -219,7 +242,8 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MB > L2
     shape, levels, rho, E, mask, force = build_inputs(args.workload)
     precision = "jacobi" if levels is None else "mixed"
-    kw = dict(tol=1e-8, maxiter=5000 if levels is None else 200, check_every=50 if levels is None else CHECK_EVERY)
+    kw = dict(tol=1e-8, maxiter=5000 if levels is None else 200, check_every=50 if levels is None else CHECK_EVERY,
+              graph=not args.host_loop)
     if levels is not None:
         kw.update(pre=2, post=2, omega=0.6, levels=levels)
     solver = ElasticitySolver(shape, E, mask, precision=precision, **kw)
@@ -257,6 +281,12 @@ def run_b200(args, rank, world, local_rank):
                        "compliance": float(force @ r64.x), "rel_residual": r64.rel}
         out["speedup_mixed_vs_fp64"] = float(np.mean(times64)) / t_local
         del s64
+        sb = ElasticitySolver(shape, E, mask, precision="bf16", **kw)     # bf16 moduli and auxiliaries
+        times_b, rb = time_solves(sb, force, args.steps, args.warmup, flush, rank_sync)
+        out["bf16"] = {"value": float(np.mean(times_b)), "iterations": rb.iterations,
+                       "compliance": float(force @ rb.x), "rel_residual": rb.rel,
+                       "speedup_vs_fp64": float(np.mean(times64)) / float(np.mean(times_b))}
+        del sb
 
     # roofline of the dominant kernel (largest share of one solve) on the solver's own data
     table = kernel_table(solver, vx, torch, flush)
@@ -279,6 +309,7 @@ def run_b200(args, rank, world, local_rank):
     e2e = []
     api_kw = dict(kw)
     api_kw.pop("levels", None)
+    api_kw.pop("graph", None)
     for i in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -294,6 +325,7 @@ def run_b200(args, rank, world, local_rank):
         del solver
         torch.cuda.empty_cache()
         out["large"] = large_section(args, flush, rank_sync)
+        out["matvec_sweep"] = matvec_sweep(flush)
     if rank == 0 and world == 1 and not args.profile and args.workload != "gmg_576x288x288":
         out["cpu_baseline"] = cpu_baseline(args.workload)
     return out
@@ -307,13 +339,14 @@ def per_solve_counts(solver, res, levels):
     checks = it // k + (0 if it % k == 0 else 1)
     M = solver.M
     n_sweeps = (M.pre - 1) + M.post
-    name = "f32" if M.dtype.itemsize == 4 else "f64"
+    name = mg_mode(M)
     return {"apply_dot_f64": it, "true_residual_f64": checks, f"jacobi_sweep_{name}": (it + 1) * n_sweeps,
             f"residual_{name}": it + 1}
 
 
 def large_section(args, flush, rank_sync):
-    """144.6M-DOF grid: mixed vs FP64 time-to-1e-8, and the FP64/FP32 matvec bandwidth."""
+    """144.6M-DOF grid: time-to-1e-8 of FP64 and the three mixed-precision preconditioners (FP32,
+    bf16 auxiliaries, all-bf16), with the hot kernels of each."""
     import torch
     import voxel_b200 as vx
     from voxel_b200.api import ElasticitySolver
@@ -324,31 +357,50 @@ def large_section(args, flush, rank_sync):
     hbm, _ = peaks()
     out = {"workload": name, "description": WORKLOADS[name][3]}
     steps, warm = max(2, min(args.steps, 3)), 1
-    for prec in ("mixed", "fp64"):
+    for prec in ("mixed", "bf16", "bf16-all", "fp64"):
         s = ElasticitySolver(shape, E, mask, precision=prec, **kw)
         times, res = time_solves(s, force, steps, warm, flush, rank_sync)
         out[prec] = {"s": float(np.mean(times)), "iterations": res.iterations, "rel": res.rel,
                      "compliance": float(force @ res.x)}
-        if prec == "mixed":
-            table = kernel_table(s, vx, torch, flush, reps=5)
-            out["kernels"] = {k: {"launch_ms": v[0] * 1e3, "GB/s": v[1] / v[0] / 1e9, "frac_hbm": v[1] / v[0] / 1e9 / hbm}
-                              for k, v in table.items()}
-            N = s.op64.nodes
-            out["matvec_f64_GDOF/s"] = 3 * N / table["apply_dot_f64"][0] / 1e9
+        table = kernel_table(s, vx, torch, flush, reps=5)
+        out[prec]["kernels"] = {k: {"launch_ms": v[0] * 1e3, "GB/s": v[1] / v[0] / 1e9,
+                                    "frac_hbm": v[1] / v[0] / 1e9 / hbm} for k, v in table.items()}
         del s
         torch.cuda.empty_cache()
-    out["speedup_mixed_vs_fp64"] = out["fp64"]["s"] / out["mixed"]["s"]
-    # raw FP32 and BF16-storage matvecs
-    op32 = vx.VoxelOperator(shape, vx.quadrature([1, 1, 1], 0.3), torch.float32)
-    u32 = torch.randn(op32.ndof, device="cuda", dtype=torch.float32)
-    E32 = E.float()
-    y32 = torch.empty_like(u32)
-    t = kernel_time(lambda: op32.matvec(u32, E32, out=y32), 5, flush)
-    out["matvec_f32"] = {"ms": t * 1e3, "GDOF/s": op32.ndof / t / 1e9,
-                         "GB/s": stream_bytes(op32.nodes, op32.n_elem, 4, 4, 1, 1, mask=False) / t / 1e9}
-    del op32, u32, E32, y32
-    torch.cuda.empty_cache()
+    for prec in ("mixed", "bf16", "bf16-all"):
+        out[f"speedup_{prec}_vs_fp64"] = out["fp64"]["s"] / out[prec]["s"]
     return out
+
+
+SWEEP_GRIDS = ((32, 16, 16), (128, 64, 64), (192, 96, 96), (256, 128, 128), (576, 288, 288))
+
+
+def matvec_sweep(flush, reps=5):
+    """Dirichlet product y = M K M u + (I - M) u alone (one launch, inputs resident, L2 flushed), on
+    the grids of every workload, in FP64, FP32 and bf16 storage (u and E in bf16, y in FP32)."""
+    import torch
+    import voxel_b200 as vx
+    hbm, _ = peaks()
+    ke = vx.quadrature([1, 1, 1], 0.3)
+    rows = []
+    for shape in SWEEP_GRIDS:
+        mask, _ = vx.problems.cantilever_equal_split(shape)
+        nm = vx.node_mask_from_dofs(mask)
+        del mask
+        g = torch.Generator(device="cuda").manual_seed(1)
+        for dt, ydt, label in ((torch.float64, torch.float64, "f64"), (torch.float32, torch.float32, "f32"),
+                               (torch.bfloat16, torch.float32, "bf16")):
+            op = vx.VoxelOperator(shape, ke, dt)
+            u = torch.randn(op.ndof, device="cuda", dtype=torch.float32, generator=g).to(dt)
+            E = torch.rand(op.n_elem, device="cuda", dtype=torch.float32, generator=g).to(dt)
+            y = torch.empty(op.ndof, device="cuda", dtype=ydt)
+            t = kernel_time(lambda: op.matvec(u, E, nm, out=y), reps, flush)
+            b = vec_bytes(op.nodes, op.n_elem, (u.element_size(), y.element_size()), E.element_size())
+            rows.append({"grid": "x".join(map(str, shape)), "dofs": op.ndof, "storage": label, "us": t * 1e6,
+                         "GDOF/s": op.ndof / t / 1e9, "GB/s": b / t / 1e9, "frac_hbm": b / t / 1e9 / hbm})
+            del op, u, E, y
+        torch.cuda.empty_cache()
+    return rows
 
 
 def cpu_baseline(workload, timed=True):
@@ -390,6 +442,9 @@ def cpu_baseline(workload, timed=True):
 def run_reference(args, rank):
     if rank != 0:
         return None
+    if args.workload in ("serving", "simp_192x96x96"):
+        return {"impl": "reference", "unavailable": f"no CPU arm for {args.workload}: the CPU port of one solve of its "
+                "largest grid alone takes minutes; the CPU baseline is timed on the gmg and jacobi workloads"}
     times = []
     for i in range(args.warmup + args.steps):
         if i < args.warmup:
@@ -420,6 +475,70 @@ def run_kernels(args):
     # residual f32 x4 (one warm-up + 3 timed each)
     table = kernel_table(s, vx, torch, flush, reps=3)
     print(json.dumps({k: {"us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9} for k, v in table.items()}))
+
+
+def run_simp_bench(args):
+    """Config-4 SIMP run: 100 density-filtered SIMP iterations on the device, with the autograd
+    sensitivity checked by central differences (64 seeded elements, step 1e-6) at the start design."""
+    import torch
+    import voxel_b200 as vx
+    from voxel_b200 import simp
+    from voxel_b200.api import ElasticitySolver
+    shape, _, levels, desc = WORKLOADS["simp_192x96x96"]
+    n = int(np.prod(shape))
+    steps = 100
+    # ---- finite-difference check of d compliance / d rho at the start design (FP64 solves to 1e-12)
+    rho0 = torch.as_tensor(0.12 + np.random.default_rng(0).uniform(-0.01, 0.01, n), device="cuda")
+    mask, force = vx.problems.cantilever_equal_split(shape)
+    s64 = ElasticitySolver(shape, vx.problems.simp_modulus(rho0, 1e-9), mask, precision="fp64", omega="spectral",
+                           levels=levels, tol=1e-12, maxiter=500, check_every=1)
+    st = simp.SimpState(s64, force)
+    r = rho0.clone().requires_grad_(True)
+    simp.compliance(r, st).backward()
+    grad = r.grad.cpu().numpy()
+    idx = np.random.default_rng(6).choice(n, 64, replace=False)
+    h = 1e-6
+    u0 = st.u.clone()
+    fd = []
+    t_fd = time.perf_counter()
+    for e in idx:
+        vals = []
+        for sgn in (1.0, -1.0):
+            rr = rho0.clone()
+            rr[int(e)] += sgn * h
+            st.u = u0.clone()
+            vals.append(float(simp.compliance(rr, st)))
+        fd.append((vals[0] - vals[1]) / (2 * h))
+    t_fd = time.perf_counter() - t_fd
+    fd = np.array(fd)
+    relerr = np.abs(fd - grad[idx]) / np.abs(grad[idx])
+    del s64, st
+    torch.cuda.empty_cache()
+    # ---- the optimisation (every step: solve, backward, filter transpose, OC bisection, filter)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    x, rho, hist = simp.run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=steps, penal=3.0,
+                                 precision="mixed", solve_tol=1e-6, noise=0.01, seed=0, levels=levels)
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    per_step = [h_["seconds"] for h_ in hist]
+    return {"metric": "SIMP iteration time (solve + autograd sensitivity + filter + OC bisection), 192x96x96",
+            "value": float(np.mean(per_step[1:])), "unit": "s", "n_gpus": 1, "steps": steps, "warmup": 1,
+            "ms_per_step": 1e3 * float(np.mean(per_step[1:])), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner", "data": "synthetic",
+            "config": {"workload": "simp_192x96x96", "description": desc,
+                       "timing": "per-step wall time with a device synchronize per step; step 0 (graph capture) excluded"},
+            "simp": {"total_s_incl_setup": wall, "device_s": ev0.elapsed_time(ev1) / 1e3,
+                     "median_step_s": float(np.median(per_step[1:])),
+                     "compliance_first_last": [hist[0]["compliance"], hist[-1]["compliance"]],
+                     "volume_last": hist[-1]["volume"], "change_last": hist[-1]["change"],
+                     "solve_iterations_mean": float(np.mean([h_["iterations"] for h_ in hist])),
+                     "oc_probes_mean": float(np.mean([h_["oc_probes"] for h_ in hist]))},
+            "fd_check": {"elements": 64, "step": h, "solve_tol": 1e-12, "max_rel_err": float(relerr.max()),
+                         "median_rel_err": float(np.median(relerr)), "seconds": t_fd}}
 
 
 def run_serving(args):
@@ -476,6 +595,9 @@ def main():
         return
     if args.workload == "serving" and args.impl == "b200":
         print(json.dumps(run_serving(args)))
+        return
+    if args.workload == "simp_192x96x96" and args.impl == "b200":
+        print(json.dumps(run_simp_bench(args)))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -49,6 +49,7 @@ struct OpArgs {
     double* partials;         // TRUE_RES (|res|^2) / APPLY_DOT (p.q): one double per CTA
     double emin, de, penal;   // SIMP modulus E = emin + de * rho^penal
     int cx;                   // owned node planes per CTA (x chunk)
+    bool cubic;               // host side: the blocks have the cube pattern (CubeK)
     BlocksT<TC> C;
 };
 
@@ -302,11 +303,64 @@ parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
 // ============================================================================= packed coefficients
 template <typename TC> struct Blocks2 { typename Coef<TC>::type c[72]; };
 
+// Cube elements (equal edge lengths): the parity blocks have the pattern
+//   g0 [a b b; b a b; b b a]      g1/g2/g4 [c d; d c] on their two non-translation components
+//   g3/g5/g6 [e e; e e] (+ f on the third component)      g7 [h k k; k h k; k k h]
+// so a block product needs 33 operations instead of 45, with 16 constants.
+template <typename TC> struct CubeK {
+    typename Coef<TC>::type amb0, b0, c1, d1, c2, d2, c4, d4, e3, f3, e5, f5, e6, f6, hmk7, k7;
+};
+
 template <typename TC, typename TU, typename TE, typename TY, typename TR = TY>
 struct OpArgs2 {
     OpArgs<TC, TU, TE, TY, TR> a;
     Blocks2<TC> C2;
+    CubeK<TC> K;
 };
+
+// true if the 72 parity coefficients have the cube pattern above (to 1e-14 of the largest); the
+// constants are then taken from fixed positions
+inline bool cube_pattern(const double* c) {
+    double m = 0;
+    for (int i = 0; i < 72; ++i) m = std::max(m, std::fabs(c[i]));
+    const double tol = 1e-14 * m;
+    auto B = [&](int g, int r, int col) { return c[9 * g + 3 * r + col]; };
+    auto eq = [&](double x, double y) { return std::fabs(x - y) <= tol; };
+    for (int g = 0; g < 8; ++g)
+        for (int r = 0; r < 3; ++r)
+            for (int col = 0; col < 3; ++col)
+                if (!eq(B(g, r, col), B(g, col, r))) return false;
+    const bool g0 = eq(B(0, 0, 0), B(0, 1, 1)) && eq(B(0, 0, 0), B(0, 2, 2)) && eq(B(0, 0, 1), B(0, 0, 2)) &&
+                    eq(B(0, 0, 1), B(0, 1, 2));
+    const bool g1 = eq(B(1, 1, 1), B(1, 2, 2));
+    const bool g2 = eq(B(2, 0, 0), B(2, 2, 2));
+    const bool g4 = eq(B(4, 0, 0), B(4, 1, 1));
+    const bool g3 = eq(B(3, 0, 0), B(3, 0, 1)) && eq(B(3, 0, 0), B(3, 1, 1));
+    const bool g5 = eq(B(5, 0, 0), B(5, 0, 2)) && eq(B(5, 0, 0), B(5, 2, 2));
+    const bool g6 = eq(B(6, 1, 1), B(6, 1, 2)) && eq(B(6, 1, 1), B(6, 2, 2));
+    const bool g7 = eq(B(7, 0, 0), B(7, 1, 1)) && eq(B(7, 0, 0), B(7, 2, 2)) && eq(B(7, 0, 1), B(7, 0, 2)) &&
+                    eq(B(7, 0, 1), B(7, 1, 2));
+    return g0 && g1 && g2 && g4 && g3 && g5 && g6 && g7;
+}
+
+template <typename TC>
+CubeK<TC> cube_constants(const BlocksT<TC>& C) {
+    auto B = [&](int g, int r, int col) { return C.c[9 * g + 3 * r + col]; };
+    auto k = [](TC v) {
+        if constexpr (std::is_same<TC, float>::value) return make_float2(v, v);
+        else return v;
+    };
+    CubeK<TC> K;
+    K.amb0 = k(B(0, 0, 0) - B(0, 0, 1)); K.b0 = k(B(0, 0, 1));
+    K.c1 = k(B(1, 1, 1)); K.d1 = k(B(1, 1, 2));
+    K.c2 = k(B(2, 0, 0)); K.d2 = k(B(2, 0, 2));
+    K.c4 = k(B(4, 0, 0)); K.d4 = k(B(4, 0, 1));
+    K.e3 = k(B(3, 0, 0)); K.f3 = k(B(3, 2, 2));
+    K.e5 = k(B(5, 0, 0)); K.f5 = k(B(5, 1, 1));
+    K.e6 = k(B(6, 1, 1)); K.f6 = k(B(6, 0, 0));
+    K.hmk7 = k(B(7, 0, 0) - B(7, 0, 1)); K.k7 = k(B(7, 0, 1));
+    return K;
+}
 
 // ============================================================================= parity_stream_xp
 // Third-generation streaming operator: one z node column per thread, TWO consecutive element
@@ -314,8 +368,9 @@ struct OpArgs2 {
 // the same (y, z) position, the y exchange (shared memory) and the z exchange (shuffles) move whole
 // pairs with no repacking, and there are two block barriers per two element planes.  Each step
 // consumes the loads issued one step (two planes) earlier and refills the same registers after use;
-// validity, masking and packing happen at consumption.  Ownership, halo recomputation and
-// determinism as in parity_stream.
+// masking and packing happen at consumption.  Loads use clamped addresses and need no validity
+// test (elements outside the grid have modulus 0).  Cube elements take the 33-operation block
+// product (CubeK).  Ownership, halo recomputation and determinism as in parity_stream.
 template <typename TC> struct XpCfg;
 template <> struct XpCfg<float> { static constexpr int NW = 16; };
 template <> struct XpCfg<double> { static constexpr int NW = 8; };
@@ -328,7 +383,7 @@ struct XpPlane {
     typename Storage<TR>::raw_t r0[3], r1[3], d0[3], d1[3];   // epilogue operands, node planes e, e+1
 };
 
-template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK>
+template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC>
 __global__ void __launch_bounds__(XpCfg<TC>::NW * 32, 1)
 parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
     constexpr int NWS = XpCfg<TC>::NW;
@@ -356,21 +411,23 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
 #define XSP(r, k) xs[((r) * 6 + (k)) * 32 + lane]
 #define HSP(r, k) hs[((r) * 6 + (k)) * 32 + lane]
 
-    // clamped (always in-bounds) addresses; values are validated when consumed
-    const int64_t plane_nodes = int64_t(g.ny + 1) * (g.nz + 1);
-    const int64_t plane_elems = int64_t(g.ny) * g.nz;
+    // Clamped (always in-bounds) addresses.  A node outside the grid only touches elements outside
+    // the grid, whose modulus is 0, so the finite value read at the clamped address contributes
+    // nothing and needs no validity test.  Offsets fit in 32 bits (fewer than 2^31 DOFs).
+    const int plane_nodes = (g.ny + 1) * (g.nz + 1);
+    const int plane_elems = g.ny * g.nz;
     const int iyc = min(max(iy, 0), g.ny), izc = min(max(iz, 0), g.nz);
     const int iye = min(max(iy, 0), g.ny - 1), ize = min(max(iz, 0), g.nz - 1);
-    const int64_t cn = int64_t(iyc) * (g.nz + 1) + izc;
+    const int cn = iyc * (g.nz + 1) + izc;
     const TU* ub = a.u + 3 * cn;
-    const TE* eb = a.E + int64_t(iye) * g.nz + ize;
+    const TE* eb = a.E + (iye * g.nz + ize);
     const uint8_t* mb = a.node_mask + cn;
-    const int64_t col = int64_t(iy) * (g.nz + 1) + iz;      // unclamped: owners only
+    const int col = iy * (g.nz + 1) + iz;                    // unclamped: owners only
 
-    auto nplane = [&](int ix) { return int64_t(min(max(ix, 0), g.nx)); };
-    auto eplane = [&](int ex) { return int64_t(min(max(ex, 0), g.nx - 1)); };
+    auto nplane = [&](int ix) { return min(max(ix, 0), g.nx); };
+    auto eplane = [&](int ex) { return min(max(ex, 0), g.nx - 1); };
     auto load_step = [&](int e, Plane& pl) {
-        const int64_t n1 = 3 * plane_nodes * nplane(e + 1), n2 = 3 * plane_nodes * nplane(e + 2);
+        const int n1 = 3 * plane_nodes * nplane(e + 1), n2 = 3 * plane_nodes * nplane(e + 2);
         #pragma unroll
         for (int k = 0; k < 3; ++k) { pl.u1[k] = Storage<TU>::raw(ub + n1 + k); pl.u2[k] = Storage<TU>::raw(ub + n2 + k); }
         pl.e0 = Storage<TE>::raw(eb + plane_elems * eplane(e));
@@ -380,13 +437,13 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
             pl.m2 = mb[plane_nodes * nplane(e + 2)];
         }
         if constexpr (EPI == EPI_JACOBI || EPI == EPI_RESIDUAL || EPI == EPI_TRUE_RES) {
-            const TR* r0 = a.r + 3 * cn + 3 * plane_nodes * nplane(e);
-            const TR* r1 = a.r + 3 * cn + 3 * plane_nodes * nplane(e + 1);
+            const TR* r0 = a.r + (3 * cn + 3 * plane_nodes * nplane(e));
+            const TR* r1 = a.r + (3 * cn + 3 * plane_nodes * nplane(e + 1));
             #pragma unroll
             for (int k = 0; k < 3; ++k) { pl.r0[k] = Storage<TR>::raw(r0 + k); pl.r1[k] = Storage<TR>::raw(r1 + k); }
             if constexpr (EPI == EPI_JACOBI) {
-                const TR* d0 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e);
-                const TR* d1 = a.invd + 3 * cn + 3 * plane_nodes * nplane(e + 1);
+                const TR* d0 = a.invd + (3 * cn + 3 * plane_nodes * nplane(e));
+                const TR* d1 = a.invd + (3 * cn + 3 * plane_nodes * nplane(e + 1));
                 #pragma unroll
                 for (int k = 0; k < 3; ++k) { pl.d0[k] = Storage<TR>::raw(d0 + k); pl.d1[k] = Storage<TR>::raw(d1 + k); }
             }
@@ -398,13 +455,12 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
     unsigned bits_up;
     {
         const int e = x0 - 1;
-        const bool v = in_node && e >= 0 && e <= g.nx;
-        const int64_t n = 3 * plane_nodes * nplane(e);
+        const int n = 3 * plane_nodes * nplane(e);
         unsigned b = 7u;
-        if constexpr (MASK == MASK_NODE) b = v ? unsigned(mb[plane_nodes * nplane(e)]) : 7u;
+        if constexpr (MASK == MASK_NODE) b = unsigned(mb[plane_nodes * nplane(e)]);
         #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            upraw[k] = v ? TC(Storage<TU>::load(ub + n + k)) : TC(0);
+            upraw[k] = TC(Storage<TU>::load(ub + n + k));
             up[k] = ((b >> k) & 1u) ? upraw[k] : TC(0);
         }
         bits_up = b;
@@ -416,15 +472,13 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
 
     for (int e = x0 - 1; e <= x1 - 1; e += 2) {               // element planes e, e + 1
         // ---- consume the loads of this step
-        const bool v1 = in_node && e + 1 >= 0 && e + 1 <= g.nx;
-        const bool v2 = in_node && e + 2 >= 0 && e + 2 <= g.nx;
         unsigned b1 = 7u, b2 = 7u;
-        if constexpr (MASK == MASK_NODE) { b1 = v1 ? unsigned(cur.m1) : 7u; b2 = v2 ? unsigned(cur.m2) : 7u; }
+        if constexpr (MASK == MASK_NODE) { b1 = unsigned(cur.m1); b2 = unsigned(cur.m2); }
         TC u1r[3], u1m[3], u2m[3], u2r[3];
         #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            u1r[k] = v1 ? TC(Storage<TU>::cvt(cur.u1[k])) : TC(0);
-            u2r[k] = v2 ? TC(Storage<TU>::cvt(cur.u2[k])) : TC(0);
+            u1r[k] = TC(Storage<TU>::cvt(cur.u1[k]));
+            u2r[k] = TC(Storage<TU>::cvt(cur.u2[k]));
             u1m[k] = ((b1 >> k) & 1u) ? u1r[k] : TC(0);
             u2m[k] = ((b2 >> k) & 1u) ? u2r[k] : TC(0);
         }
@@ -480,23 +534,69 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
                 }
                 v[k][0] = mk2(TC(0), TC(0));
             }
-            #pragma unroll
-            for (int gi = 0; gi < 8; ++gi) {
-                const int pa[3] = {gi ^ 1, gi ^ 2, gi ^ 4};
-                const P in[3] = {v[0][pa[0]], v[1][pa[1]], v[2][pa[2]]};
+            if constexpr (CUBIC) {
+                const auto& K = args.K;
+                {   // g0: x@1 y@2 z@4, (a - b) I + b 1 1^T
+                    const P bs = cmul2(K.b0, add2(add2(v[0][1], v[1][2]), v[2][4]));
+                    v[0][1] = cfma2(K.amb0, v[0][1], bs);
+                    v[1][2] = cfma2(K.amb0, v[1][2], bs);
+                    v[2][4] = cfma2(K.amb0, v[2][4], bs);
+                }
+                {   // g1: y@3 z@5
+                    const P a1 = v[1][3], a2 = v[2][5];
+                    v[1][3] = cfma2(K.d1, a2, cmul2(K.c1, a1));
+                    v[2][5] = cfma2(K.d1, a1, cmul2(K.c1, a2));
+                }
+                {   // g2: x@3 z@6
+                    const P a0 = v[0][3], a2 = v[2][6];
+                    v[0][3] = cfma2(K.d2, a2, cmul2(K.c2, a0));
+                    v[2][6] = cfma2(K.d2, a0, cmul2(K.c2, a2));
+                }
+                {   // g4: x@5 y@6
+                    const P a0 = v[0][5], a1 = v[1][6];
+                    v[0][5] = cfma2(K.d4, a1, cmul2(K.c4, a0));
+                    v[1][6] = cfma2(K.d4, a0, cmul2(K.c4, a1));
+                }
+                {   // g3: x@2 y@1 (e e; e e), z@7 (f)
+                    const P t = cmul2(K.e3, add2(v[0][2], v[1][1]));
+                    v[0][2] = t; v[1][1] = t;
+                    v[2][7] = cmul2(K.f3, v[2][7]);
+                }
+                {   // g5: x@4 z@1 (e e; e e), y@7 (f)
+                    const P t = cmul2(K.e5, add2(v[0][4], v[2][1]));
+                    v[0][4] = t; v[2][1] = t;
+                    v[1][7] = cmul2(K.f5, v[1][7]);
+                }
+                {   // g6: y@4 z@2 (e e; e e), x@7 (f)
+                    const P t = cmul2(K.e6, add2(v[1][4], v[2][2]));
+                    v[1][4] = t; v[2][2] = t;
+                    v[0][7] = cmul2(K.f6, v[0][7]);
+                }
+                {   // g7: x@6 y@5 z@3, (h - k) I + k 1 1^T
+                    const P ks = cmul2(K.k7, add2(add2(v[0][6], v[1][5]), v[2][3]));
+                    v[0][6] = cfma2(K.hmk7, v[0][6], ks);
+                    v[1][5] = cfma2(K.hmk7, v[1][5], ks);
+                    v[2][3] = cfma2(K.hmk7, v[2][3], ks);
+                }
+            } else {
                 #pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    if (pa[r] == 0) continue;
-                    P sacc = mk2(TC(0), TC(0));
-                    bool first = true;
+                for (int gi = 0; gi < 8; ++gi) {
+                    const int pa[3] = {gi ^ 1, gi ^ 2, gi ^ 4};
+                    const P in[3] = {v[0][pa[0]], v[1][pa[1]], v[2][pa[2]]};
                     #pragma unroll
-                    for (int cc = 0; cc < 3; ++cc) {
-                        if (!parity_nonzero(gi, r, cc)) continue;
-                        const auto coef = args.C2.c[9 * gi + 3 * r + cc];
-                        sacc = first ? cmul2(coef, in[cc]) : cfma2(coef, in[cc], sacc);
-                        first = false;
+                    for (int r = 0; r < 3; ++r) {
+                        if (pa[r] == 0) continue;
+                        P sacc = mk2(TC(0), TC(0));
+                        bool first = true;
+                        #pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) {
+                            if (!parity_nonzero(gi, r, cc)) continue;
+                            const auto coef = args.C2.c[9 * gi + 3 * r + cc];
+                            sacc = first ? cmul2(coef, in[cc]) : cfma2(coef, in[cc], sacc);
+                            first = false;
+                        }
+                        v[r][pa[r]] = sacc;
                     }
-                    v[r][pa[r]] = sacc;
                 }
             }
             // ---- inverse Z: face iz gets G0 (own) + G1 of lane - 1
@@ -536,9 +636,9 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
             TC y0[3], y1[3];
             #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const P zero = mk2(TC(0), TC(0));
-                const P fx0 = add2(H0[k][0], row > 0 ? HSP(rowp, k) : zero);
-                const P fx1 = add2(H0[k][1], row > 0 ? HSP(rowp, 3 + k) : zero);
+                // row 0 (halo, never an owner) reads its own entry: its sums are not stored
+                const P fx0 = add2(H0[k][0], HSP(rowp, k));
+                const P fx1 = add2(H0[k][1], HSP(rowp, 3 + k));
                 const P sm = add2(fx0, fx1), df = sub2(fx0, fx1);
                 y0[k] = carry[k] + sm.lo();
                 y1[k] = df.lo() + sm.hi();
@@ -550,7 +650,7 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
                     const int ixo = e + h;                       // node plane written by this half
                     if (ixo < x0 || ixo >= x1) continue;
                     const unsigned bb = h == 0 ? bits_up : b1;
-                    TY* yo = a.y + 3 * (int64_t(ixo) * plane_nodes + col);
+                    TY* yo = a.y + 3 * (ixo * plane_nodes + col);
                     #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const TC yv = h == 0 ? y0[k] : y1[k];
@@ -624,12 +724,14 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
     constexpr bool v2 = !REV && !SIMP && MASK != MASK_DOF;
     static_assert(v2 || std::is_same<TR, TY>::value, "parity_stream takes r and invd of the output type");
     OpArgs<TC, TU, TE, TY, TR> a = a_in;
+    const bool cubic = a.cubic;
     const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
     a.cx = stream_cx(a.g, t);
     size_t smem, threads;
     const void* kern;
     if constexpr (v2) {
-        kern = (const void*)parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK>;
+        kern = cubic ? (const void*)parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true>
+                     : (const void*)parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false>;
         threads = XpCfg<TC>::NW * 32;
         smem = size_t(2) * XpCfg<TC>::NW * 6 * 32 * sizeof(V2<TC>);
     } else {
@@ -640,14 +742,14 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
     // dynamic + static shared memory exceeds the 48 KB default: opt in once per instantiation.  The
     // solvers run every loop body once un-captured before capturing it, so this call never happens
     // inside a stream capture.
-    static bool configured = false;
-    if (!configured) {
+    static bool configured[2] = {false, false};
+    if (!configured[cubic]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) {
             set_error("%s: cudaFuncSetAttribute: %s", what, cudaGetErrorString(e));
             return VX_ERR_CUDA;
         }
-        configured = true;
+        configured[cubic] = true;
     }
     if constexpr (v2) {
         OpArgs2<TC, TU, TE, TY, TR> a2;
@@ -656,7 +758,12 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
             if constexpr (std::is_same<TC, float>::value) a2.C2.c[i] = make_float2(a.C.c[i], a.C.c[i]);
             else a2.C2.c[i] = a.C.c[i];
         }
-        parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+        if (cubic) {
+            a2.K = cube_constants<TC>(a.C);
+            parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+        } else {
+            parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+        }
     } else {
         parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a);
     }
@@ -799,6 +906,7 @@ extern "C" int vx_matvec(int prec, int nx, int ny, int nz, const double* blocks,
         OpArgs<TC, X, M, TC> a{};
         a.g = Grid{nx, ny, nz}; a.u = (const X*)u; a.E = (const M*)E; a.y = (TC*)y; a.node_mask = node_mask;
         a.C = convert_blocks<TC>(blocks);
+        a.cubic = cube_pattern(blocks);
         rc = node_mask ? launch_stream<TC, X, M, TC, EPI_RAW, MASK_NODE, false, false>(a, stream, "vx_matvec")
                        : launch_stream<TC, X, M, TC, EPI_RAW, MASK_NONE, false, false>(a, stream, "vx_matvec");
     });
@@ -963,6 +1071,8 @@ int fused_dispatch(const char* what, int prec, int nx, int ny, int nz, const dou
             a.u = (const X*)x; a.E = (const M*)E; a.y = (TY*)out; a.node_mask = node_mask;
             a.r = (const R*)r; a.invd = (const R*)invd; a.omega = TC(omega); a.partials = partials;
             a.C = convert_blocks<TC>(blocks);
+            a.cubic = cube_pattern(blocks);
+        a.cubic = cube_pattern(blocks);
             rc = node_mask ? launch_stream<TC, X, M, TY, EPI, MASK_NODE, false, false, R>(a, stream, what)
                            : launch_stream<TC, X, M, TY, EPI, MASK_NONE, false, false, R>(a, stream, what);
         }

@@ -228,7 +228,7 @@ def run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=100, em
         change = float((x_new - x).abs().max())
         x = x_new
         torch.cuda.synchronize()
-        history.append({"step": k, "compliance": float(c), "iterations": state.last.iterations,
+        history.append({"step": k, "compliance": float(c.detach()), "iterations": state.last.iterations,
                         "rel": state.last.rel, "change": change, "volume": float(rho.mean()),
                         "oc_probes": oc.probes, "seconds": time.perf_counter() - t0})
         if callback:

@@ -61,6 +61,32 @@ def test_brick_element_and_fixture_ke():
         assert maxrel(y, vo.product_raw(shape, ke, u, E)) < 1e-13
 
 
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-13), (torch.float32, 1e-5)])
+def test_brick_element_fused_forms(dtype, tol):
+    """A brick element has no cube symmetry: the kernels take the general 45-coefficient product
+    (a cube takes the 33-operation form); both must match the oracle in every fused form."""
+    shape = (17, 10, 21)
+    ke = vo.quadrature([1.0, 0.5, 2.0], 0.25)
+    E, u = case(shape, 8)
+    r = np.random.default_rng(9).standard_normal(u.size)
+    mask, _ = vo.cantilever_equal_split(shape)
+    nm = vx.node_mask_from_dofs(cu(mask))
+    op = vx.VoxelOperator(shape, ke, dtype)
+    rd = lambda a: a.astype(np.float32).astype(np.float64) if dtype == torch.float32 else a
+    Eh, uh, rh = rd(E), rd(u), rd(r)
+    Au = vo.apply_dirichlet(shape, ke, Eh, mask, uh)
+    invd = rd(1 / np.where(mask != 0, vo.product_diagonal(shape, ke, Eh), 1.0))
+    x = op.jacobi(cu(uh, dtype), cu(rh, dtype), cu(invd, dtype), cu(Eh, dtype), nm, 0.6)
+    assert maxrel(x.double().cpu().numpy(), uh + 0.6 * invd * (rh - Au)) < tol
+    res = op.residual(cu(uh, dtype), cu(rh, dtype), cu(Eh, dtype), nm)
+    assert maxrel(res.double().cpu().numpy(), (rh - Au) * mask) < tol
+    q = torch.empty(u.size, dtype=dtype, device="cuda")
+    part = torch.empty(op.partials_size, dtype=torch.float64, device="cuda")
+    op.apply_dot(cu(uh, dtype), cu(Eh, dtype), nm, q, part)
+    assert maxrel(q.double().cpu().numpy(), Au) < tol
+    assert abs(float(part.sum()) - float(uh @ Au)) <= tol * abs(float(uh @ Au)) * 10
+
+
 def test_modal8_entry_point_matches_reference_emulation():
     g = golden("element.npz")
     shape = tuple(int(s) for s in g["emu_shape"])
