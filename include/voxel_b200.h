@@ -262,6 +262,10 @@ int64_t vx_solver_partials(int64_t n);
 int vx_solver_finalize(int op, int64_t G, const double* partials, double* S, cudaStream_t stream);
 int vx_cg_update(int prec, int64_t n, const double* S, void* x, const void* p, void* r, const void* q,
                  int update_r, cudaStream_t stream);
+/* p = z + beta p, and z_old = z when z_old is not NULL.  p (and r of vx_dots_pr) are of `prec`;
+ * z, z_old (and zn, zo) are iterates of the preconditioner's selector `zprec`, so a mixed-precision
+ * loop keeps z_old in FP32 (an exact copy of the FP32 z).  vx_dots_pr writes the partials of r.zn
+ * and, with zo, of r.(zn - zo) (Polak-Ribiere, src/voxel_mg.py:205-208). */
 int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, const void* z, void* p, void* z_old,
                     cudaStream_t stream);
 int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const void* zn, const void* zo,
@@ -272,6 +276,11 @@ int vx_jacobi_precond_dot(int prec, int64_t n, const void* d, const void* r, voi
  * the first damped-Jacobi step of src/voxel_mg.py:165 fused with the cast of :178. */
 int vx_vcycle_entry(int prec, int64_t n, const double* r64, void* r_mg, const void* inv_diag, double omega,
                     void* x, cudaStream_t stream);
+/* vx_vcycle_entry preceded by the CG update r64 -= S[alpha] q (skipped once S says done or
+ * breakdown), so the residual is read once for both: the r update of src/voxel_mg.py:200 fused
+ * into the preconditioner's first step. */
+int vx_vcycle_entry_update(int prec, int64_t n, const double* S, double* r64, const double* q, void* r_mg,
+                           const void* inv_diag, double omega, void* x, cudaStream_t stream);
 int vx_scaled_product(int prec, int64_t n, double omega, const void* a, const void* b, void* out,
                       cudaStream_t stream);
 int vx_set_scalars(double* S, int first, int count, double value, cudaStream_t stream);

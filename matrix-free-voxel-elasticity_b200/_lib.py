@@ -61,6 +61,7 @@ SIGNATURES = {
     "vx_dots_pr": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P]),
     "vx_jacobi_precond_dot": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P]),
     "vx_vcycle_entry": (c_int, [c_int, c_int64, _P, _P, _P, c_double, _P, _P]),
+    "vx_vcycle_entry_update": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P, c_double, _P, _P]),
     "vx_scaled_product": (c_int, [c_int, c_int64, c_double, _P, _P, _P, _P]),
     "vx_set_scalars": (c_int, [_P, c_int, c_int, c_double, _P]),
     "vx_graph_while_begin": (c_int, [_P, ctypes.POINTER(c_void_p)]),

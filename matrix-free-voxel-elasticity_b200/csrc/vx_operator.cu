@@ -371,9 +371,11 @@ CubeK<TC> cube_constants(const BlocksT<TC>& C) {
 // masking and packing happen at consumption.  Loads use clamped addresses and need no validity
 // test (elements outside the grid have modulus 0).  Cube elements take the 33-operation block
 // product (CubeK).  Ownership, halo recomputation and determinism as in parity_stream.
+// Warps per CTA and CTAs per SM: FP32 runs two 8-warp CTAs per SM (at most 128 registers), so one
+// CTA computes while the other waits at a barrier; FP64 needs ~200 registers and runs one.
 template <typename TC> struct XpCfg;
-template <> struct XpCfg<float> { static constexpr int NW = 16; };
-template <> struct XpCfg<double> { static constexpr int NW = 8; };
+template <> struct XpCfg<float> { static constexpr int NW = 8, MINB = 2; };
+template <> struct XpCfg<double> { static constexpr int NW = 8, MINB = 1; };
 
 template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK>
 struct XpPlane {
@@ -384,7 +386,7 @@ struct XpPlane {
 };
 
 template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC>
-__global__ void __launch_bounds__(XpCfg<TC>::NW * 32, 1)
+__global__ void __launch_bounds__(XpCfg<TC>::NW * 32, XpCfg<TC>::MINB)
 parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
     constexpr int NWS = XpCfg<TC>::NW;
     constexpr int TYS = NWS - 2;
@@ -693,7 +695,7 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
 }
 
 // CTA tiling of the streaming operators: parity_stream_xp (author layout, node or no mask) tiles
-// (y, z) node columns as (NW-2) x 30 with NW = 16 (FP32) or 8 (FP64) warps; parity_stream
+// (y, z) node columns as (NW-2) x 30 with NW = 8 warps; parity_stream
 // (natural-layout / SIMP / DOF-mask product) as 14 x 30.  x-chunk: the longest chunk (least halo recomputation) with >= 4 CTAs per SM.
 struct Tiling { int tz, ty; };
 inline Tiling tiling(int prec, bool v2) {

@@ -104,27 +104,28 @@ __global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __r
     if (update_r) r[i] = r[i] - a * q[i];
 }
 
-// p = z + beta p (z in the preconditioner's storage TZ), and z_old = z when z_old is given
+// p = z + beta p and, when z_old is given, z_old = z; z and z_old in the preconditioner's storage TZ
+// (a copy in z's own type is exact and moves half the bytes of an FP64 copy of an FP32 z)
 template <typename T, typename TZ>
 __global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, const TZ* __restrict__ z, T* __restrict__ p,
-                                    T* __restrict__ z_old) {
+                                    TZ* __restrict__ z_old) {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const T zi = T(Storage<TZ>::load(z + i));
-    p[i] = zi + T(S[S_BETA]) * p[i];
-    if (z_old) z_old[i] = zi;
+    const TZ zr = z[i];
+    p[i] = T(Storage<TZ>::cvt(zr)) + T(S[S_BETA]) * p[i];
+    if (z_old) z_old[i] = zr;
 }
 
 // partials for r . zn and r . (zn - zo), fixed grid G (a function of n), fixed order
 template <typename T, typename TZ>
 __global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const TZ* __restrict__ zn,
-                                                     const T* __restrict__ zo, double* __restrict__ partials) {
+                                                     const TZ* __restrict__ zo, double* __restrict__ partials) {
     const int64_t G = gridDim.x;
     double a = 0.0, b = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
         const double ri = double(r[i]), zi = double(Storage<TZ>::load(zn + i));
         a = fma(ri, zi, a);
-        if (zo) b = fma(ri, zi - double(zo[i]), b);
+        if (zo) b = fma(ri, zi - double(Storage<TZ>::load(zo + i)), b);
     }
     a = block_sum_ft(a);
     if (threadIdx.x == 0) partials[blockIdx.x] = a;
@@ -158,6 +159,25 @@ __global__ void vcycle_entry_kernel(int64_t n, const double* __restrict__ r64, T
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const A r = A(Storage<TR>::round(arith_t<TR>(r64[i])));   // the level residual as stored
+    if (rmg) Storage<TR>::store(rmg + i, r);
+    Storage<TX>::store(x + i, A(omega) * A(Storage<TR>::load(invd + i)) * r);
+}
+
+// The same entry preceded by the CG residual update r64 -= alpha q (alpha = S[S_ALPHA]), which is
+// skipped, like vx_cg_update's, once the loop has converged or broken down.
+template <typename TX, typename TR>
+__global__ void vcycle_entry_update_kernel(int64_t n, const double* __restrict__ S, double* __restrict__ r64,
+                                           const double* __restrict__ q, TR* __restrict__ rmg,
+                                           const TR* __restrict__ invd, double omega, TX* __restrict__ x) {
+    using A = arith_t<TX>;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double rv = r64[i];
+    if (S[S_DONE] == 0.0 && S[S_BREAK] == 0.0) {
+        rv = rv - S[S_ALPHA] * q[i];
+        r64[i] = rv;
+    }
+    const A r = A(Storage<TR>::round(arith_t<TR>(rv)));
     if (rmg) Storage<TR>::store(rmg + i, r);
     Storage<TX>::store(x + i, A(omega) * A(Storage<TR>::load(invd + i)) * r);
 }
@@ -237,10 +257,10 @@ extern "C" int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, 
     if (prec == VX_F64 && zprec == VX_F64)
         cg_direction_kernel<double, double><<<nb(n, 256), 256, 0, stream>>>(n, S, (const double*)z, (double*)p, (double*)z_old);
     else if (prec == VX_F64 && zprec == VX_F32)
-        cg_direction_kernel<double, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (double*)p, (double*)z_old);
+        cg_direction_kernel<double, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (double*)p, (float*)z_old);
     else if (prec == VX_F64 && zprec == VX_BF16_F32)
         cg_direction_kernel<double, __nv_bfloat16><<<nb(n, 256), 256, 0, stream>>>(n, S, (const __nv_bfloat16*)z, (double*)p,
-                                                                                   (double*)z_old);
+                                                                                   (__nv_bfloat16*)z_old);
     else if (prec == VX_F32 && zprec == VX_F32)
         cg_direction_kernel<float, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p, (float*)z_old);
     else { set_error("vx_cg_direction: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
@@ -256,10 +276,10 @@ extern "C" int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const v
     if (prec == VX_F64 && zprec == VX_F64)
         dots_pr_kernel<double, double><<<G, FT, 0, stream>>>(n, (const double*)r, (const double*)zn, (const double*)zo, partials);
     else if (prec == VX_F64 && zprec == VX_F32)
-        dots_pr_kernel<double, float><<<G, FT, 0, stream>>>(n, (const double*)r, (const float*)zn, (const double*)zo, partials);
+        dots_pr_kernel<double, float><<<G, FT, 0, stream>>>(n, (const double*)r, (const float*)zn, (const float*)zo, partials);
     else if (prec == VX_F64 && zprec == VX_BF16_F32)
         dots_pr_kernel<double, __nv_bfloat16><<<G, FT, 0, stream>>>(n, (const double*)r, (const __nv_bfloat16*)zn,
-                                                                    (const double*)zo, partials);
+                                                                    (const __nv_bfloat16*)zo, partials);
     else if (prec == VX_F32 && zprec == VX_F32)
         dots_pr_kernel<float, float><<<G, FT, 0, stream>>>(n, (const float*)r, (const float*)zn, (const float*)zo, partials);
     else { set_error("vx_dots_pr: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
@@ -292,6 +312,21 @@ extern "C" int vx_vcycle_entry(int prec, int64_t n, const double* r64, void* r_m
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_vcycle_entry");
+    return VX_OK;
+}
+
+extern "C" int vx_vcycle_entry_update(int prec, int64_t n, const double* S, double* r64, const double* q, void* r_mg,
+                                      const void* inv_diag, double omega, void* x, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry_update: n must be positive");
+    VX_CHECK_ARG(S && r64 && q && inv_diag && x, VX_ERR_NULL_POINTER, "vx_vcycle_entry_update: NULL pointer");
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using X = typename decltype(t)::X;
+        using R = typename decltype(t)::R;
+        vcycle_entry_update_kernel<X, R><<<nb(n, 256), 256, 0, stream>>>(n, S, r64, q, (R*)r_mg, (const R*)inv_diag,
+                                                                         omega, (X*)x);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry_update: unsupported precision %d", prec);
+    VX_CHECK_LAUNCH("vx_vcycle_entry_update");
     return VX_OK;
 }
 

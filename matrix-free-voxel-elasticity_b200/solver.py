@@ -180,9 +180,16 @@ class MGHierarchy:
         return omegas, lambdas
 
     # ------------------------------------------------------------------ kernel emission
-    def emit(self, r64: torch.Tensor) -> torch.Tensor:
+    @property
+    def fuses_residual_update(self) -> bool:
+        """emit(r64, update=...) can apply the CG update r64 -= alpha q in its first kernel."""
+        return len(self.levels) > 1
+
+    def emit(self, r64: torch.Tensor, update=None) -> torch.Tensor:
         """Launch one V-cycle on the current stream: z = M(r64); returns the buffer holding z (in
-        the hierarchy's dtype).  r64 is the FP64 finest residual; it is read, never written."""
+        the hierarchy's dtype).  r64 is the FP64 finest residual; it is read, and written only when
+        `update` = (q, S) asks the entry kernel to apply r64 -= S[alpha] q first (multi-level
+        hierarchies, see fuses_residual_update)."""
         L0 = self.levels[0]
         if len(self.levels) == 1:
             src = r64
@@ -193,9 +200,14 @@ class MGHierarchy:
                       L0.x.data_ptr(), _s())
             return L0.x
         r0 = r64 if self.dtype == torch.float64 else L0.r
-        _lib.call("vx_vcycle_entry", self.prec, L0.n, _ptr(r64, "r"),
-                  None if self.dtype == torch.float64 else L0.r.data_ptr(), L0.invd.data_ptr(), L0.omega,
-                  L0.x.data_ptr(), _s())
+        r_mg = None if self.dtype == torch.float64 else L0.r.data_ptr()
+        if update is None:
+            _lib.call("vx_vcycle_entry", self.prec, L0.n, _ptr(r64, "r"), r_mg, L0.invd.data_ptr(), L0.omega,
+                      L0.x.data_ptr(), _s())
+        else:
+            q, S = update
+            _lib.call("vx_vcycle_entry_update", self.prec, L0.n, _ptr(S, "S", torch.float64), _ptr(r64, "r"),
+                      _ptr(q, "q", torch.float64, L0.n), r_mg, L0.invd.data_ptr(), L0.omega, L0.x.data_ptr(), _s())
         return self._level(0, r0)
 
     def _level(self, l, r):
@@ -349,7 +361,7 @@ class FCGSolver:
         self.r = torch.zeros(n, **f64)
         self.p = torch.zeros(n, **f64)
         self.q = torch.zeros(n, **f64)
-        self.z_old = torch.zeros(n, **f64)
+        self.z_old = torch.zeros(n, dtype=precond.dtype, device="cuda")     # z's own storage: an exact copy
         self.S = torch.zeros(16, **f64)
         self.S_host = torch.zeros(16, dtype=torch.float64, pin_memory=True)
         self.G_op = op64.partials_size
@@ -372,14 +384,17 @@ class FCGSolver:
 
     def _iteration(self, check: bool):
         op, S, pp = self.op, self.S.data_ptr(), self.partials.data_ptr()
+        # r -= alpha q is applied by the preconditioner's first kernel when it can (one read of r
+        # saved), else here; at a check iteration r is replaced by b - A x instead
+        fuse = not check and getattr(self.M, "fuses_residual_update", False)
         op.apply_dot(self.p, self.E, self.mask, self.q, self.partials)          # q = A p, p.q
         self._fin(FIN_PQ, self.G_op)
         _lib.call("vx_cg_update", _lib.VX_F64, self.n, S, self.x.data_ptr(), self.p.data_ptr(), self.r.data_ptr(),
-                  self.q.data_ptr(), 0 if check else 1, _s())
+                  self.q.data_ptr(), 0 if (check or fuse) else 1, _s())
         if check:                                                                # r = b - A x (replacement)
             op.true_residual(self.x, self.b, self.E, self.mask, self.r, self.partials)
             self._fin(FIN_TRUE, self.G_op)
-        z = self.M.emit(self.r)
+        z = self.M.emit(self.r, update=(self.q, self.S)) if fuse else self.M.emit(self.r)
         _lib.call("vx_dots_pr", _lib.VX_F64, self.zprec, self.n, self.r.data_ptr(), z.data_ptr(),
                   self.z_old.data_ptr(), pp, _s())
         self._fin(FIN_BETA_PR, self.G_vec)
