@@ -132,6 +132,13 @@ def build_inputs(name, device="cuda"):
     return shape, levels, rho, E, mask, force
 
 
+# DRAM bytes per grid node of one launch, from ncu captures of the same kernels on the 256x128x128
+# grid (4,276,737 nodes; profiles/parity_stream_xp_*_256x128x128_ncu.md): dram__bytes_read.sum +
+# dram__bytes_write.sum / nodes.  Scaled by the node count of the measured launch.
+NCU_TRAFFIC_PER_NODE = {"jacobi_sweep_f32": (175.528960e6 + 36.767744e6) / 4276737,
+                        "apply_dot_f64": (140.506880e6 + 71.061504e6) / 4276737}
+
+
 def peaks():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -141,6 +148,21 @@ def peaks():
 
 
 # ----------------------------------------------------------------------------------- timing
+def max_over_ranks(t_local, world, device):
+    """The slowest rank's time (every rank gets it); the timed region ends when the last replica does."""
+    if world <= 1:
+        return float(t_local)
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([float(t_local)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt)
+
+
+def whole_job_time_per_solve(t_max, world):
+    """N replicas each finish one solve per step within t_max: whole-job time per solve."""
+    return t_max / world
+
 def time_solves(solver, force, steps, warmup, flush, rank_sync):
     import torch
     for _ in range(warmup):
@@ -255,15 +277,11 @@ def run_b200(args, rank, world, local_rank):
         launches = (_lib.launches - launches0)
     launches_per_solve = launches // (args.steps + args.warmup)
     t_local = float(np.mean(times))
-    t_max = t_local
-    if world > 1:
-        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt)
+    t_max = max_over_ranks(t_local, world, "cuda")
     compliance = float(force @ res.x)
     out = {"metric": "time-to-1e-8 solve, mixed-precision GMG-PCG (FP32 V-cycle in FP64 flexible CG)"
                      if levels is not None else "time-to-1e-8 solve, FP64 Jacobi-PCG",
-           "value": t_max / world, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "value": whole_job_time_per_solve(t_max, world), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": t_max * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64 outer / f32 preconditioner" if levels is not None else "f64", "data": "synthetic",
            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][3],
@@ -294,8 +312,11 @@ def run_b200(args, rank, world, local_rank):
     share = {k: table[k][0] * counts.get(k, 0) for k in table}
     dom = max(share, key=share.get)
     t_dom, b_dom = table[dom]
+    tpn = NCU_TRAFFIC_PER_NODE.get(dom)
     out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": b_dom / t_dom / 1e9, "peak": hbm, "unit": "GB/s",
-                       "frac": b_dom / t_dom / 1e9 / hbm, "traffic": None, "peak_kind": peak_kind,
+                       "frac": b_dom / t_dom / 1e9 / hbm, "traffic": None if tpn is None else tpn * solver.op64.nodes,
+                       "traffic_source": "ncu dram bytes of the same kernel on 256x128x128, scaled by nodes",
+                       "peak_kind": peak_kind,
                        "bytes_per_launch": b_dom, "launch_s": t_dom,
                        "kernels": {k: {"launch_us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9,
                                        "per_solve": counts.get(k, 0)} for k, v in table.items()}}
