@@ -65,7 +65,7 @@ def footprint_estimate(shape, precision="mixed", levels=None, max_coarse_x=16) -
         total += 3 * nodes * (2 * ex + 2 * ea) + res + elems * (8 + ea) + nodes
     nx, ny, nz = shapes[-1]
     nc = 3 * (nx + 1) * (ny + 1) * (nz + 1)
-    return int(total + 3 * 8 * nc * nc + (64 << 20))   # A, its factor, its inverse; workspace margin
+    return int(total + 5 * 8 * nc * nc + (64 << 20))   # A, factor, inverse, identity, L^-1; workspace
 
 
 def percentile(values, q):
@@ -83,8 +83,10 @@ def summarize(completions, makespan):
 
 class Scheduler:
     """FIFO admission by slots and memory budget; completion by polling.  `backend` provides
-    footprint(req), start(req) -> handle, done(handle) -> bool, finish(handle, req) -> dict,
-    release(handle) and reclaim(bytes_needed) -> bytes freed from idle pooled state."""
+    footprint(req) (bytes a start would add), start(req) -> handle, done(handle) -> bool,
+    finish(handle, req) -> dict, release(handle) -> bytes freed (None: the job's footprint) and
+    reclaim(bytes_needed) -> bytes freed from idle pooled state; optionally resident_bytes(), the
+    bytes already held when a run starts (a pre-built pool)."""
 
     def __init__(self, backend, budget_bytes=150e9, max_slots=16, clock=time.perf_counter, poll_s=50e-6):
         self.backend, self.budget, self.max_slots = backend, float(budget_bytes), int(max_slots)
@@ -96,7 +98,7 @@ class Scheduler:
         pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
         active = []            # (req, handle, bytes, admitted)
         done = []
-        used = 0.0
+        used = float(self.backend.resident_bytes()) if hasattr(self.backend, "resident_bytes") else 0.0
         t0 = self.clock()
         while pending or active:
             now = self.clock() - t0
@@ -122,8 +124,8 @@ class Scheduler:
                 if self.backend.done(handle):
                     info = self.backend.finish(handle, req)
                     fin = self.clock() - t0
-                    self.backend.release(handle)
-                    used -= need
+                    freed = self.backend.release(handle)
+                    used -= need if freed is None else freed
                     done.append(Completion(req.rid, tuple(req.shape), req.tol, req.arrival, adm, fin, **info))
                     progressed = True
                 else:
@@ -181,7 +183,7 @@ class CudaBackend:
                                  post=self.post, omega=self.omega, max_coarse_x=self.max_coarse_x, tol=req.tol,
                                  maxiter=self.maxiter, check_every=self.check_every)
         s.fcg.tol = float(req.tol)
-        s.fcg.launch(force)
+        s.fcg.launch(force, dot_with=force)                    # the compliance comes back with the scalars
         return s
 
     def done(self, s):
@@ -189,14 +191,39 @@ class CudaBackend:
 
     def finish(self, s, req):
         res = s.fcg.finish()
-        _, force = self._force(tuple(req.shape))
-        x = res.x.clone() if self.keep else None
+        x = res.x.clone() if self.keep else None       # finish() ordered the caller's stream after the solve
         return {"iterations": res.iterations, "converged": res.converged, "rel": res.rel,
-                "compliance": float(force @ res.x), "x": x}
+                "compliance": s.fcg.last_dot, "x": x}
+
+    def prewarm(self, shapes, per_shape, budget_bytes=None):
+        """Build `per_shape` idle solvers for each grid shape (hierarchy, buffers and the captured
+        loop graph), so that serving never allocates device memory (cudaMalloc synchronises the
+        device and would stall every job in flight).  Stops early at `budget_bytes` of footprint."""
+        from .api import ElasticitySolver
+        torch = self.torch
+        used = self.resident_bytes()
+        for shape in shapes:
+            shape = tuple(shape)
+            mask, force = self._force(shape)
+            fp = footprint_estimate(shape, self.precision, max_coarse_x=self.max_coarse_x)
+            for _ in range(per_shape - len(self.free.get(shape, []))):
+                if budget_bytes is not None and used + fp > budget_bytes:
+                    break
+                E = torch.ones(shape[0] * shape[1] * shape[2], dtype=torch.float64, device="cuda")
+                s = ElasticitySolver(shape, E, mask, precision=self.precision, pre=self.pre, post=self.post,
+                                     omega=self.omega, max_coarse_x=self.max_coarse_x, tol=1e-6,
+                                     maxiter=self.maxiter, check_every=self.check_every)
+                s.fcg.launch(force)                            # captures the loop graph
+                s.fcg.finish()
+                self.release(s)
+                used += fp
+        torch.cuda.synchronize()
 
     def release(self, s):
+        """The solver goes back to the pool and stays resident: nothing is freed."""
         self.free.setdefault(s.shape, []).append(s)
         self.free_bytes[id(s)] = footprint_estimate(s.shape, self.precision, max_coarse_x=self.max_coarse_x)
+        return 0.0
 
     def reclaim(self, need):
         """Drop idle pooled solvers (largest first) until `need` bytes are freed; returns bytes freed."""
@@ -217,10 +244,15 @@ class CudaBackend:
         return sum(self.free_bytes.values())
 
 
-def serve(requests, precision="mixed", budget_bytes=150e9, max_slots=16, keep_solution=False, **kw):
+def serve(requests, precision="mixed", budget_bytes=150e9, max_slots=16, keep_solution=False, prewarm=False, **kw):
     """Run a request stream through the continuous-batching server; returns (completions, summary).
-    Pooled idle solvers are charged to the budget (they stay resident for reuse)."""
+    Pooled idle solvers are charged to the budget (they stay resident for reuse).  With `prewarm`,
+    max_slots idle solvers per requested grid shape are built first (within the budget), so the
+    stream itself never allocates device memory."""
     backend = CudaBackend(precision=precision, keep_solution=keep_solution, **kw)
+    if prewarm:
+        shapes = sorted({tuple(r.shape) for r in requests})
+        backend.prewarm(shapes, max_slots, budget_bytes)
     sched = Scheduler(_PoolCharge(backend), budget_bytes=budget_bytes, max_slots=max_slots)
     done, makespan = sched.run(requests)
     out = summarize(done, makespan)
@@ -249,7 +281,10 @@ class _PoolCharge:
         return self.b.finish(h, req)
 
     def release(self, h):
-        self.b.release(h)
+        return self.b.release(h)
+
+    def resident_bytes(self):
+        return self.b.resident_bytes()
 
     def reclaim(self, need):
         return self.b.reclaim(need)

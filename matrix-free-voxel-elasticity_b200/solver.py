@@ -100,12 +100,13 @@ class MGHierarchy:
         _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
                   _ptr(c.E64, "E"), _ptr(c.mask, "mask"), A.data_ptr(), _s())
         self.A_coarse = A
-        # the same factorisation call as update_modulus, so a refreshed pooled hierarchy and a fresh
-        # one are bitwise identical; checked once here (the check synchronises)
-        self.coarse_factor, info = torch.linalg.cholesky_ex(A)
+        self._eye = torch.eye(c.n, dtype=torch.float64, device="cuda")
+        self.A_inv = torch.empty_like(A)
+        # the same calls as update_modulus, so a refreshed pooled hierarchy and a fresh one are
+        # bitwise identical; the factorisation is checked once here (the check synchronises)
+        info = self._coarse_inverse()
         if int(info) != 0:
             raise ValueError(f"coarsest-level matrix is not positive definite (cholesky info {int(info)})")
-        self.A_inv = torch.cholesky_inverse(self.coarse_factor).contiguous()
         n_smooth = len(self.levels) - 1
         if omegas is None:
             self.omegas = [0.6] * n_smooth                      # the reference default (voxel_mg.py:148)
@@ -149,8 +150,16 @@ class MGHierarchy:
                   c.E64.data_ptr(), c.mask.data_ptr(), self.A_coarse.data_ptr(), _s())
         # no error check here (it would synchronise the stream); a non-SPD coarse matrix shows up as a
         # non-finite residual and a non-converged solve
-        self.coarse_factor = torch.linalg.cholesky_ex(self.A_coarse)[0]
-        self.A_inv.copy_(torch.cholesky_inverse(self.coarse_factor))
+        self._coarse_inverse()
+
+    def _coarse_inverse(self):
+        """A_inv = L^-T L^-1 from the FP64 Cholesky factor A = L L^T: a triangular solve against the
+        identity and one product, all queued on the current stream without a host synchronisation.
+        Returns the factorisation's device-side info tensor (0 when A is positive definite)."""
+        self.coarse_factor, info = torch.linalg.cholesky_ex(self.A_coarse)
+        linv = torch.linalg.solve_triangular(self.coarse_factor, self._eye, upper=False)
+        torch.matmul(linv.mT, linv, out=self.A_inv)
+        return info
 
     def footprint_bytes(self) -> int:
         b = 0
@@ -158,7 +167,7 @@ class MGHierarchy:
             for t in (L.x, L.xt, L.r, L.invd, L.res, L.E):
                 b += 0 if t is None else t.numel() * t.element_size()
             b += L.E64.numel() * 8 + L.mask.numel()
-        return b + self.A_inv.numel() * 8 * 3
+        return b + self.A_inv.numel() * 8 * 5         # A, factor, inverse, identity, transient L^-1
 
     def spectral_omegas(self, iterations=30, seed=20260923):
         """omega_l = 4 / (3 lambda_l), lambda_l from a seeded FP64 power iteration on D^-1 A over the
@@ -364,6 +373,12 @@ class FCGSolver:
         self.z_old = torch.zeros(n, dtype=precond.dtype, device="cuda")     # z's own storage: an exact copy
         self.S = torch.zeros(16, **f64)
         self.S_host = torch.zeros(16, dtype=torch.float64, pin_memory=True)
+        # f . x after a launched solve (launch(..., dot_with=f)): device value and its pinned copy
+        self.dot_partials = torch.zeros(int(_lib.load().vx_partials_size(n)), **f64)
+        self.dot_dev = torch.zeros(1, **f64)
+        self.dot_host = torch.zeros(1, dtype=torch.float64, pin_memory=True)
+        self._dot_with = None
+        self.last_dot = None
         self.G_op = op64.partials_size
         self.G_vec = int(_lib.load().vx_solver_partials(n))
         self.partials = torch.zeros(max(self.G_op, 2 * self.G_vec), **f64)
@@ -433,10 +448,13 @@ class FCGSolver:
         torch.cuda.current_stream().synchronize()
         return self.S_host.numpy().copy()
 
-    def launch(self, b: torch.Tensor, x0: torch.Tensor | None = None, stream: torch.cuda.Stream | None = None):
+    def launch(self, b: torch.Tensor, x0: torch.Tensor | None = None, stream: torch.cuda.Stream | None = None,
+               dot_with: torch.Tensor | None = None):
         """Enqueue a solve of A x = b on `stream` (default: the solver's own) without waiting: the
         initialisation, the whole-loop graph and an asynchronous read-back of the scalars.  Call
-        finish() for the result; done() polls without blocking."""
+        finish() for the result; done() polls without blocking.  With `dot_with` = f, the dot
+        product f . x (e.g. the compliance) is computed on the same stream after the loop and read
+        back with the scalars: finish() leaves it in `last_dot` without another synchronisation."""
         if b.numel() != self.n:
             raise ValueError(f"b has {b.numel()} entries, expected {self.n}")
         st = stream or self.stream
@@ -461,9 +479,21 @@ class FCGSolver:
             if full > 0 and self.use_graph:
                 self._graph.launch(st)
             self.S_host.copy_(self.S, non_blocking=True)
+            self._dot_with = dot_with
+            if dot_with is not None:
+                if st != caller:
+                    dot_with.record_stream(st)
+                self._emit_dot()
+                self.dot_host.copy_(self.dot_dev, non_blocking=True)
             self._event = torch.cuda.Event()
             self._event.record(st)
         self._pending = (st, k, checking, limit, full, x0 is not None)
+
+    def _emit_dot(self):
+        f = self._dot_with
+        A = (ctypes.c_void_p * 3)(_ptr(f, "dot_with", torch.float64, self.n), None, None)
+        B = (ctypes.c_void_p * 3)(self.x.data_ptr(), None, None)
+        _lib.call("vx_dots", _lib.VX_F64, self.n, 1, A, B, self.dot_partials.data_ptr(), self.dot_dev.data_ptr(), _s())
 
     def done(self) -> bool:
         return self._pending is None or self._event.query()
@@ -476,6 +506,7 @@ class FCGSolver:
         self._event.synchronize()
         with torch.cuda.stream(st):
             s = self.S_host.numpy().copy()
+            s_launch = s.copy()
             if full > 0 and self.use_graph:
                 self._graph.account(max(1, -(-int(s[S_IT]) // k)))
             if not self.use_graph and not (warm and s[S_DONE]):
@@ -493,6 +524,13 @@ class FCGSolver:
                 self.op.true_residual(self.x, self.b, self.E, self.mask, self.q, self.partials)
                 self._fin(FIN_TRUE, self.G_op)
                 s = self._read()
+            if self._dot_with is not None:
+                if int(s[S_IT]) != int(s_launch[S_IT]):                      # x moved after the dot: redo it
+                    self._emit_dot()
+                    self.dot_host.copy_(self.dot_dev, non_blocking=True)
+                    torch.cuda.current_stream().synchronize()
+                self.last_dot = float(self.dot_host[0])
+                self._dot_with = None
         torch.cuda.current_stream().wait_stream(st)
         rel = float(s[S_REL])
         return SolveResult(self.x, int(s[S_IT]), bool(rel <= self.tol), rel, int(s[S_MV]))

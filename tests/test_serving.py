@@ -97,3 +97,60 @@ def test_footprint_grows_with_the_grid():
     a = footprint_estimate((48, 24, 24))
     b = footprint_estimate((256, 128, 128))
     assert 0 < a < b and b < 4e9
+
+
+class PoolingBackend(FakeBackend):
+    """Finished jobs stay resident in a pool (release frees nothing); a new job on a pooled shape
+    needs no memory; reclaim frees idle pooled jobs."""
+
+    def __init__(self, clock, duration, size, pooled=()):
+        super().__init__(clock, duration, size)
+        self.pool = list(pooled)
+        self.reclaimed = 0.0
+
+    def resident_bytes(self):
+        return sum(self.size[s] for s in self.pool)
+
+    def footprint(self, req):
+        return 0.0 if req.shape in self.pool else self.size[req.shape]
+
+    def start(self, req):
+        if req.shape in self.pool:
+            self.pool.remove(req.shape)
+        self.running[req.rid] = (self.clock() + self.duration[req.shape], req.shape)
+        return req.rid
+
+    def done(self, h):
+        self.clock.t += 1e-4
+        return self.clock() >= self.running[h][0]
+
+    def release(self, h):
+        self.pool.append(self.running.pop(h)[1])
+        return 0.0
+
+    def reclaim(self, need):
+        freed = 0.0
+        while self.pool and freed < need:
+            freed += self.size[self.pool.pop(0)]
+        self.reclaimed += freed
+        return freed
+
+
+def test_pooled_solvers_stay_charged_until_reclaimed():
+    big, small = (8, 4, 4), (4, 2, 2)
+    clock = FakeClock()
+    be = PoolingBackend(clock, {big: 1.0, small: 0.5}, {big: 6.0, small: 1.0}, pooled=[small, small])
+    sched = Scheduler(be, budget_bytes=10.0, max_slots=8, clock=clock, poll_s=0.0)
+    reqs = [Request(0, small, None, 1e-8, 0.0), Request(1, big, None, 1e-8, 0.0), Request(2, big, None, 1e-8, 0.0)]
+    import voxel_b200.serving as srv
+    real_sleep = srv.time.sleep
+    srv.time.sleep = lambda s: setattr(clock, "t", clock.t + max(s, 1e-4))
+    try:
+        done, makespan = sched.run(reqs)
+    finally:
+        srv.time.sleep = real_sleep
+    assert len(done) == 3
+    assert sched.peak_bytes <= 10.0                 # pool (2) + one big (6); the second big must wait
+    byid = {c.rid: c for c in done}
+    assert byid[2].admitted >= byid[1].finished - 1e-3
+    assert be.reclaimed > 0                         # idle pooled memory was given back for the second big job
