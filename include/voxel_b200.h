@@ -173,6 +173,16 @@ int vx_assemble_dense(int nx, int ny, int nz, const double* ke, const double* E,
 int vx_coarse_apply(int prec, int n, const double* Ainv, const void* r, const uint8_t* node_mask,
                     void* z, cudaStream_t stream);
 
+/* The coarse solve from the inverse Cholesky factor instead of the inverse: with A = L L^T and
+ * Linv = L^-1, vx_coarse_pack writes M = tril(Linv) + triu(Linv^T, 1) (n x n row-major; m may not
+ * alias linv), and vx_coarse_apply_factor computes z = (Linv^T (Linv r)) * M in two passes over the
+ * two triangles of M (y: n doubles of caller scratch).  Same bytes per apply as vx_coarse_apply,
+ * but the set-up needs no n^3 product.  Replaces the two triangular solves of
+ * src/voxel_mg.py:152-159 coarse_solve.  r auxiliary, z an iterate of `prec`. */
+int vx_coarse_pack(int n, const double* linv, double* m, cudaStream_t stream);
+int vx_coarse_apply_factor(int prec, int n, const double* m, const void* r, const uint8_t* node_mask,
+                           double* y, void* z, cudaStream_t stream);
+
 /* Node masks <-> the reference's 0/1 DOF masks (double, 3 per node, author layout). */
 int vx_mask_from_dofs(int64_t nodes, const double* dof_mask, uint8_t* node_mask, cudaStream_t stream);
 

@@ -61,6 +61,8 @@ SIGNATURES = {
     "vx_dots_pr": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P]),
     "vx_jacobi_precond_dot": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P]),
     "vx_vcycle_entry": (c_int, [c_int, c_int64, _P, _P, _P, c_double, _P, _P]),
+    "vx_coarse_pack": (c_int, [c_int, _P, _P, _P]),
+    "vx_coarse_apply_factor": (c_int, [c_int, c_int, _P, _P, _P, _P, _P, _P]),
     "vx_vcycle_entry_update": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P, c_double, _P, _P]),
     "vx_scaled_product": (c_int, [c_int, c_int64, c_double, _P, _P, _P, _P]),
     "vx_set_scalars": (c_int, [_P, c_int, c_int, c_double, _P]),
@@ -118,7 +120,7 @@ CAPTURE_STREAM = None
 
 # Kernel launches issued by each entry point (entry points not listed launch none or one:
 # host-only entry points are in HOST_ONLY).  Used to count this library's launches.
-KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2}
+KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2, "vx_coarse_apply_factor": 2}
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",

@@ -156,6 +156,68 @@ __global__ void coarse_apply_kernel(int n, const double* __restrict__ Ainv, cons
     }
 }
 
+// Packed inverse factor: M = tril(Linv) + triu(Linv^T, 1), Linv = L^-1 of A = L L^T, so
+// A^-1 r = Linv^T (Linv r) reads row i of M left of the diagonal (pass 1) and right of it (pass 2).
+// 32x32 tiles through shared memory keep the transposed reads coalesced.
+__global__ void coarse_pack_kernel(int n, const double* __restrict__ linv, double* __restrict__ m) {
+    __shared__ double tile[32][33];
+    const int bi = blockIdx.y * 32, bj = blockIdx.x * 32;      // output tile rows bi.., cols bj..
+    const int tx = threadIdx.x, ty = threadIdx.y;              // 32 x 8 threads
+    if (bj > bi) {                                             // strictly-upper tile: read Linv^T
+        for (int k = ty; k < 32; k += 8) {
+            const int r = bj + k, c = bi + tx;                 // source element Linv[r][c]
+            tile[k][tx] = (r < n && c < n) ? linv[int64_t(r) * n + c] : 0.0;
+        }
+        __syncthreads();
+        for (int k = ty; k < 32; k += 8) {
+            const int i = bi + k, j = bj + tx;
+            if (i < n && j < n) m[int64_t(i) * n + j] = tile[tx][k];
+        }
+    } else {                                                   // lower or diagonal tile
+        for (int k = ty; k < 32; k += 8) {
+            const int i = bi + k, j = bj + tx;
+            if (i < n && j < n) {
+                if (j <= i) m[int64_t(i) * n + j] = linv[int64_t(i) * n + j];
+                else m[int64_t(i) * n + j] = linv[int64_t(j) * n + i];    // diagonal tile, upper part
+            }
+        }
+    }
+}
+
+// pass 1: y = Linv r (row i, columns 0..i of M), one warp per row, FP64 accumulation
+template <typename TR>
+__global__ void coarse_lower_kernel(int n, const double* __restrict__ m, const TR* __restrict__ r,
+                                    double* __restrict__ y) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double* mr = m + int64_t(row) * n;
+    double s = 0.0;
+    for (int j = lane; j <= row; j += 32) s = fma(mr[j], double(Storage<TR>::load(r + j)), s);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) y[row] = s;
+}
+
+// pass 2: z = Linv^T y (row i: the diagonal Linv[i][i] and columns i+1.. of M), masked
+template <typename T>
+__global__ void coarse_upper_kernel(int n, const double* __restrict__ m, const double* __restrict__ y,
+                                    const uint8_t* __restrict__ mask, T* __restrict__ z) {
+    using A = arith_t<T>;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double* mr = m + int64_t(row) * n;
+    double s = 0.0;
+    for (int j = row + lane; j < n; j += 32) s = fma(mr[j], y[j], s);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const bool fr = mask ? ((mask[row / 3] >> (row % 3)) & 1u) : true;
+        Storage<T>::store(z + row, fr ? A(s) : A(0));
+    }
+}
+
 __global__ void mask_from_dofs_kernel(int64_t nodes, const double* __restrict__ m, uint8_t* __restrict__ out) {
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= nodes) return;
@@ -273,5 +335,31 @@ extern "C" int vx_mask_from_dofs(int64_t nodes, const double* dof_mask, uint8_t*
     VX_CHECK_ARG(dof_mask && node_mask, VX_ERR_NULL_POINTER, "vx_mask_from_dofs: NULL pointer");
     mask_from_dofs_kernel<<<blocks_for(nodes, 256), 256, 0, stream>>>(nodes, dof_mask, node_mask);
     VX_CHECK_LAUNCH("vx_mask_from_dofs");
+    return VX_OK;
+}
+
+extern "C" int vx_coarse_pack(int n, const double* linv, double* m, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_pack: n must be positive");
+    VX_CHECK_ARG(linv && m, VX_ERR_NULL_POINTER, "vx_coarse_pack: NULL pointer");
+    VX_CHECK_ARG(linv != m, VX_ERR_INVALID_ARGUMENT, "vx_coarse_pack: m may not alias linv");
+    const unsigned t = unsigned((n + 31) / 32);
+    coarse_pack_kernel<<<dim3(t, t), dim3(32, 8), 0, stream>>>(n, linv, m);
+    VX_CHECK_LAUNCH("vx_coarse_pack");
+    return VX_OK;
+}
+
+extern "C" int vx_coarse_apply_factor(int prec, int n, const double* m, const void* r, const uint8_t* node_mask,
+                                      double* y, void* z, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply_factor: n must be positive");
+    VX_CHECK_ARG(m && r && y && z, VX_ERR_NULL_POINTER, "vx_coarse_apply_factor: NULL pointer");
+    const unsigned gb = blocks_for(int64_t(n) * 32, 256);
+    const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
+        using R = typename decltype(t)::R;
+        using X = typename decltype(t)::X;
+        coarse_lower_kernel<R><<<gb, 256, 0, stream>>>(n, m, (const R*)r, y);
+        coarse_upper_kernel<X><<<gb, 256, 0, stream>>>(n, m, y, node_mask, (X*)z);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply_factor: unsupported precision %d", prec);
+    VX_CHECK_LAUNCH("vx_coarse_apply_factor");
     return VX_OK;
 }

@@ -49,11 +49,30 @@ class _Level:
     __slots__ = ("shape", "op", "op64", "E64", "E", "mask", "invd", "omega", "r", "x", "xt", "res", "n")
 
 
+def _lower_inverse(L: torch.Tensor, leaf: int = 256) -> torch.Tensor:
+    """L^-1 of a lower-triangular FP64 matrix by recursive halving:
+    [[A, 0], [B, C]]^-1 = [[A^-1, 0], [-C^-1 B A^-1, C^-1]]; blocks of at most `leaf` rows are
+    inverted by a triangular solve.  About n^3/3 multiply-adds, nearly all in matrix products."""
+    n = L.shape[0]
+    if n <= leaf:
+        eye = torch.eye(n, dtype=L.dtype, device=L.device)
+        return torch.linalg.solve_triangular(L, eye, upper=False).contiguous()
+    h = n // 2
+    out = torch.zeros((n, n), dtype=L.dtype, device=L.device)       # row-major, whatever L's layout
+    ai = _lower_inverse(L[:h, :h], leaf)
+    ci = _lower_inverse(L[h:, h:], leaf)
+    out[:h, :h] = ai
+    out[h:, h:] = ci
+    out[h:, :h] = -(ci @ (L[h:, :h] @ ai))
+    return out
+
+
 class MGHierarchy:
     """Rediscretised geometric multigrid (src/voxel_mg.py:1-21,74-178): level l has element matrix
     ke * 2^l, modulus the 2x2x2 mean of level l-1, mask injected from level l-1; damped Jacobi
     V(pre, post) in `dtype` (float64 or float32); the coarsest level is solved in FP64 with the
-    inverse of its dense constrained matrix (from an FP64 Cholesky factorisation).
+    inverse Cholesky factor of its dense constrained matrix (two triangular passes per cycle, the
+    reference's two triangular solves).
 
     BF16 storage (no reference counterpart), FP32 arithmetic in both: aux_dtype=bfloat16 stores the
     level moduli and the auxiliary vectors (right-hand sides, residuals, inverse diagonals) in bf16
@@ -100,8 +119,8 @@ class MGHierarchy:
         _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
                   _ptr(c.E64, "E"), _ptr(c.mask, "mask"), A.data_ptr(), _s())
         self.A_coarse = A
-        self._eye = torch.eye(c.n, dtype=torch.float64, device="cuda")
-        self.A_inv = torch.empty_like(A)
+        self.coarse_packed = torch.empty_like(A)              # tril(L^-1) + triu(L^-T, 1)
+        self._coarse_y = torch.zeros(c.n, dtype=torch.float64, device="cuda")
         # the same calls as update_modulus, so a refreshed pooled hierarchy and a fresh one are
         # bitwise identical; the factorisation is checked once here (the check synchronises)
         info = self._coarse_inverse()
@@ -133,7 +152,7 @@ class MGHierarchy:
 
     def update_modulus(self, E):
         """New finest modulus (FP64, same grid): refresh every level's moduli, inverse diagonal and
-        the coarsest inverse IN PLACE, so captured graphs that use this hierarchy stay valid."""
+        the coarsest inverse factor IN PLACE, so captured graphs that use this hierarchy stay valid."""
         L0 = self.levels[0]
         if E.data_ptr() != L0.E64.data_ptr():
             L0.E64.copy_(E)
@@ -153,12 +172,13 @@ class MGHierarchy:
         self._coarse_inverse()
 
     def _coarse_inverse(self):
-        """A_inv = L^-T L^-1 from the FP64 Cholesky factor A = L L^T: a triangular solve against the
-        identity and one product, all queued on the current stream without a host synchronisation.
+        """Factor the coarsest matrix A = L L^T (FP64 Cholesky) and pack L^-1 with its transpose for
+        vx_coarse_apply_factor; L^-1 comes from a recursive block inversion whose work is matrix
+        products.  Everything is queued on the current stream without a host synchronisation.
         Returns the factorisation's device-side info tensor (0 when A is positive definite)."""
         self.coarse_factor, info = torch.linalg.cholesky_ex(self.A_coarse)
-        linv = torch.linalg.solve_triangular(self.coarse_factor, self._eye, upper=False)
-        torch.matmul(linv.mT, linv, out=self.A_inv)
+        linv = _lower_inverse(self.coarse_factor).contiguous()     # the kernel reads it row-major
+        _lib.call("vx_coarse_pack", linv.shape[0], linv.data_ptr(), self.coarse_packed.data_ptr(), _s())
         return info
 
     def footprint_bytes(self) -> int:
@@ -167,7 +187,7 @@ class MGHierarchy:
             for t in (L.x, L.xt, L.r, L.invd, L.res, L.E):
                 b += 0 if t is None else t.numel() * t.element_size()
             b += L.E64.numel() * 8 + L.mask.numel()
-        return b + self.A_inv.numel() * 8 * 5         # A, factor, inverse, identity, transient L^-1
+        return b + self.coarse_packed.numel() * 8 * 4    # A, factor, packed inverse factor, transient L^-1
 
     def spectral_omegas(self, iterations=30, seed=20260923):
         """omega_l = 4 / (3 lambda_l), lambda_l from a seeded FP64 power iteration on D^-1 A over the
@@ -205,7 +225,8 @@ class MGHierarchy:
             if self.aux_dtype != torch.float64:
                 _lib.call("vx_cast", L0.n, _lib.VX_F64, _ptr(r64, "r"), PREC[self.aux_dtype], L0.r.data_ptr(), 1.0, _s())
                 src = L0.r
-            _lib.call("vx_coarse_apply", self.prec, L0.n, self.A_inv.data_ptr(), src.data_ptr(), L0.mask.data_ptr(),
+            _lib.call("vx_coarse_apply_factor", self.prec, L0.n, self.coarse_packed.data_ptr(), src.data_ptr(),
+                      L0.mask.data_ptr(), self._coarse_y.data_ptr(),
                       L0.x.data_ptr(), _s())
             return L0.x
         r0 = r64 if self.dtype == torch.float64 else L0.r
@@ -222,7 +243,8 @@ class MGHierarchy:
     def _level(self, l, r):
         L = self.levels[l]
         if l == len(self.levels) - 1:
-            _lib.call("vx_coarse_apply", self.prec, L.n, self.A_inv.data_ptr(), r.data_ptr(), L.mask.data_ptr(),
+            _lib.call("vx_coarse_apply_factor", self.prec, L.n, self.coarse_packed.data_ptr(), r.data_ptr(),
+                      L.mask.data_ptr(), self._coarse_y.data_ptr(),
                       L.x.data_ptr(), _s())
             return L.x
         bufs = [L.x, L.xt]

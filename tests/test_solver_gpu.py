@@ -198,3 +198,34 @@ def test_reference_published_kat_q96x3_full_scale(precision):
     assert ok and it == obs[0]["iterations"] == 20
     ref_c = np.array([o["compliance"] for o in obs])
     assert np.min(np.abs(comp - ref_c)) <= 1e-9 * ref_c.mean()
+
+
+@pytest.mark.parametrize("n", [1, 31, 100, 517])
+def test_coarse_solve_from_the_packed_inverse_factor(n):
+    """vx_coarse_pack + vx_coarse_apply_factor give A^-1 r (masked) for an SPD A, to FP64 rounding
+    (1e-12 relative to |A^-1 r|, condition number about 1e2), for sizes that are not tile multiples."""
+    rng = np.random.default_rng(n)
+    B = rng.standard_normal((n, n))
+    A = B @ B.T + n * np.eye(n)
+    Ad = cu(A)
+    L = torch.linalg.cholesky(Ad).mT.contiguous().mT                 # column-major, as cuSOLVER may return it
+    linv = vs._lower_inverse(L, leaf=16)
+    assert linv.is_contiguous()
+    assert rel(linv @ L, np.eye(n)) < 1e-12
+    packed = torch.empty_like(Ad)
+    st = torch.cuda.current_stream().cuda_stream
+    vx._lib.call("vx_coarse_pack", n, linv.data_ptr(), packed.data_ptr(), st)
+    lh = linv.cpu().numpy()
+    ph = packed.cpu().numpy()
+    assert np.array_equal(np.tril(ph), np.tril(lh)) and np.array_equal(np.triu(ph, 1), np.triu(lh.T, 1))
+    nodes = (n + 2) // 3
+    mask = rng.integers(0, 8, nodes).astype(np.uint8)
+    bits = ((mask[:, None] >> np.arange(3)) & 1).reshape(-1)[:n]
+    r = rng.standard_normal(n)
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    z = torch.empty(n, dtype=torch.float64, device="cuda")
+    rd, md = cu(r), cu(mask, torch.uint8)          # held: their memory must outlive the launch
+    vx._lib.call("vx_coarse_apply_factor", vx._lib.VX_F64, n, packed.data_ptr(), rd.data_ptr(), md.data_ptr(),
+                 y.data_ptr(), z.data_ptr(), st)
+    ref = np.linalg.solve(A, r) * bits
+    assert rel(z, ref) < 1e-12
