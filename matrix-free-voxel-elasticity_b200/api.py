@@ -6,6 +6,8 @@ or Jacobi) and the graph-captured flexible-CG loop; `solve(...)` is the host-buf
 """
 from __future__ import annotations
 
+from collections import OrderedDict
+
 import numpy as np
 import torch
 
@@ -60,6 +62,7 @@ class ElasticitySolver:
             self.M = MGHierarchy(self.shape, self.ke, self.E, self.node_mask, dt, pre, post,
                                  None if spectral else omega, shapes=shapes, aux_dtype=aux)
             self.spectral_seed = spectral_seed
+            self._spectral = spectral
             if spectral:
                 # lambda_l from the FP64 level operators, as the reference estimates it once on the
                 # FP64 hierarchy shared by all arms (experiments/session_i/run_gpu.py:287-288)
@@ -94,16 +97,52 @@ class ElasticitySolver:
             self.E.copy_(E)
         self.M.update_modulus(self.E)
 
+    def update(self, E, mask=None):
+        """A new problem on the same grid: moduli and (optionally) the 0/1 DOF or uint8 node mask,
+        refreshed in place -- every level's moduli, masks and diagonals and the coarsest factor are
+        recomputed from the new inputs; buffers and captured graphs are reused."""
+        if mask is not None:
+            m = mask.to("cuda", non_blocking=True) if isinstance(mask, torch.Tensor) else _dev(mask)
+            nm = m.contiguous() if m.dtype == torch.uint8 else node_mask_from_dofs(m.to(torch.float64))
+            self.node_mask.copy_(nm)
+            if hasattr(self.M, "update_mask"):
+                self.M.update_mask()
+        self.update_modulus(E)
+        if getattr(self, "_spectral", False):
+            self.refresh_omegas()
+
     def compliance(self, f, x):
         return float(_dev(f) @ x)
+
+
+_SOLVERS = OrderedDict()      # set-up key -> ElasticitySolver, least recently used first
+_SOLVER_CACHE_SIZE = 4
 
 
 def solve(shape, E, force, mask, *, ke=None, precision="mixed", tol=1e-8, maxiter=200, check_every=1, pre=2,
           post=2, omega=0.6, max_coarse_x=16, levels=None):
     """Host-buffer entry point: E (Ne), force and 0/1 DOF mask (3N), numpy, author layout.
-    Returns (u as numpy, dict(iterations, converged, rel, matvecs, compliance))."""
-    s = ElasticitySolver(shape, E, mask, ke=ke, precision=precision, pre=pre, post=post, omega=omega,
-                         max_coarse_x=max_coarse_x, levels=levels, tol=tol, maxiter=maxiter, check_every=check_every)
+    Returns (u as numpy, dict(iterations, converged, rel, matvecs, compliance)).
+
+    Solvers are kept for the last few set-ups (grid, element, precision, cycle, damping, levels):
+    a call with a known set-up copies its inputs into that solver and recomputes every level's
+    moduli, masks, diagonals and the coarsest factor from them, reusing the device buffers and
+    the captured solve graph."""
+    shape = tuple(int(v) for v in shape)
+    ke_key = None if ke is None else np.asarray(ke, dtype=np.float64).tobytes()
+    om_key = tuple(omega) if isinstance(omega, (list, tuple)) else omega
+    key = (shape, ke_key, precision, int(check_every), int(pre), int(post), om_key, int(max_coarse_x), levels)
+    s = _SOLVERS.pop(key, None)
+    if s is None:
+        s = ElasticitySolver(shape, E, mask, ke=ke, precision=precision, pre=pre, post=post, omega=omega,
+                             max_coarse_x=max_coarse_x, levels=levels, tol=tol, maxiter=maxiter,
+                             check_every=check_every)
+    else:
+        s.update(E, mask)
+    _SOLVERS[key] = s
+    while len(_SOLVERS) > _SOLVER_CACHE_SIZE:
+        _SOLVERS.popitem(last=False)
+    s.fcg.tol, s.fcg.maxiter = float(tol), int(maxiter)
     f = _dev(force)
     res = s.solve(f)
     u = res.x.cpu().numpy()

@@ -137,22 +137,36 @@ __global__ void assemble_dense_kernel(Grid g, const __grid_constant__ Ke576 ke, 
     A[row * (nn * 3) + col] = out;
 }
 
-// z = (Ainv r) * mask, one warp per row, FP64 accumulation
-template <typename TR, typename T>
-__global__ void coarse_apply_kernel(int n, const double* __restrict__ Ainv, const TR* __restrict__ r,
-                                    const uint8_t* __restrict__ mask, T* __restrict__ z) {
-    using A = arith_t<T>;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const double* row = Ainv + int64_t(warp) * n;
+// sum over j in [j0, j1) of row[j] * v(j) by one CTA of CT threads (stride CT), reduced in a fixed
+// order.  A CTA per row keeps each thread's dependent chain short: with a warp per row, every warp
+// is resident at once and the launch lasts as long as one warp's walk along a full row.
+constexpr int CT = 256;
+template <typename V>
+__device__ __forceinline__ double block_row_dot(const double* __restrict__ row, int j0, int j1, V v) {
+    __shared__ double red[CT / 32];
     double s = 0.0;
-    for (int j = lane; j < n; j += 32) s = fma(row[j], double(Storage<TR>::load(r + j)), s);
+    for (int j = j0 + int(threadIdx.x); j < j1; j += CT) s = fma(row[j], v(j), s);
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-        const bool fr = mask ? ((mask[warp / 3] >> (warp % 3)) & 1u) : true;
-        Storage<T>::store(z + warp, fr ? A(s) : A(0));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < CT / 32; ++k) t += red[k];
+    return t;                                                   // valid in thread 0
+}
+
+// z = (Ainv r) * mask, one CTA per row, FP64 accumulation
+template <typename TR, typename T>
+__global__ void __launch_bounds__(CT) coarse_apply_kernel(int n, const double* __restrict__ Ainv,
+                                                          const TR* __restrict__ r, const uint8_t* __restrict__ mask,
+                                                          T* __restrict__ z) {
+    using A = arith_t<T>;
+    const int row = blockIdx.x;
+    const double s = block_row_dot(Ainv + int64_t(row) * n, 0, n, [&](int j) { return double(Storage<TR>::load(r + j)); });
+    if (threadIdx.x == 0) {
+        const bool fr = mask ? ((mask[row / 3] >> (row % 3)) & 1u) : true;
+        Storage<T>::store(z + row, fr ? A(s) : A(0));
     }
 }
 
@@ -184,35 +198,24 @@ __global__ void coarse_pack_kernel(int n, const double* __restrict__ linv, doubl
     }
 }
 
-// pass 1: y = Linv r (row i, columns 0..i of M), one warp per row, FP64 accumulation
+// pass 1: y = Linv r (row i, columns 0..i of M), one CTA per row, FP64 accumulation
 template <typename TR>
-__global__ void coarse_lower_kernel(int n, const double* __restrict__ m, const TR* __restrict__ r,
-                                    double* __restrict__ y) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const double* mr = m + int64_t(row) * n;
-    double s = 0.0;
-    for (int j = lane; j <= row; j += 32) s = fma(mr[j], double(Storage<TR>::load(r + j)), s);
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) y[row] = s;
+__global__ void __launch_bounds__(CT) coarse_lower_kernel(int n, const double* __restrict__ m,
+                                                          const TR* __restrict__ r, double* __restrict__ y) {
+    const int row = blockIdx.x;
+    const double s = block_row_dot(m + int64_t(row) * n, 0, row + 1, [&](int j) { return double(Storage<TR>::load(r + j)); });
+    if (threadIdx.x == 0) y[row] = s;
 }
 
 // pass 2: z = Linv^T y (row i: the diagonal Linv[i][i] and columns i+1.. of M), masked
 template <typename T>
-__global__ void coarse_upper_kernel(int n, const double* __restrict__ m, const double* __restrict__ y,
-                                    const uint8_t* __restrict__ mask, T* __restrict__ z) {
+__global__ void __launch_bounds__(CT) coarse_upper_kernel(int n, const double* __restrict__ m,
+                                                          const double* __restrict__ y,
+                                                          const uint8_t* __restrict__ mask, T* __restrict__ z) {
     using A = arith_t<T>;
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const double* mr = m + int64_t(row) * n;
-    double s = 0.0;
-    for (int j = row + lane; j < n; j += 32) s = fma(mr[j], y[j], s);
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) {
+    const int row = blockIdx.x;
+    const double s = block_row_dot(m + int64_t(row) * n, row, n, [&](int j) { return y[j]; });
+    if (threadIdx.x == 0) {
         const bool fr = mask ? ((mask[row / 3] >> (row % 3)) & 1u) : true;
         Storage<T>::store(z + row, fr ? A(s) : A(0));
     }
@@ -319,11 +322,10 @@ extern "C" int vx_coarse_apply(int prec, int n, const double* Ainv, const void* 
                                void* z, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply: n must be positive");
     VX_CHECK_ARG(Ainv && r && z, VX_ERR_NULL_POINTER, "vx_coarse_apply: NULL pointer");
-    const unsigned gb = blocks_for(int64_t(n) * 32, 256);
     const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
         using R = typename decltype(t)::R;
         using X = typename decltype(t)::X;
-        coarse_apply_kernel<R, X><<<gb, 256, 0, stream>>>(n, Ainv, (const R*)r, node_mask, (X*)z);
+        coarse_apply_kernel<R, X><<<unsigned(n), CT, 0, stream>>>(n, Ainv, (const R*)r, node_mask, (X*)z);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarse_apply");
@@ -352,12 +354,11 @@ extern "C" int vx_coarse_apply_factor(int prec, int n, const double* m, const vo
                                       double* y, void* z, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply_factor: n must be positive");
     VX_CHECK_ARG(m && r && y && z, VX_ERR_NULL_POINTER, "vx_coarse_apply_factor: NULL pointer");
-    const unsigned gb = blocks_for(int64_t(n) * 32, 256);
     const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
         using R = typename decltype(t)::R;
         using X = typename decltype(t)::X;
-        coarse_lower_kernel<R><<<gb, 256, 0, stream>>>(n, m, (const R*)r, y);
-        coarse_upper_kernel<X><<<gb, 256, 0, stream>>>(n, m, y, node_mask, (X*)z);
+        coarse_lower_kernel<R><<<unsigned(n), CT, 0, stream>>>(n, m, (const R*)r, y);
+        coarse_upper_kernel<X><<<unsigned(n), CT, 0, stream>>>(n, m, y, node_mask, (X*)z);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply_factor: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarse_apply_factor");

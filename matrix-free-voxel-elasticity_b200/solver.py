@@ -49,7 +49,7 @@ class _Level:
     __slots__ = ("shape", "op", "op64", "E64", "E", "mask", "invd", "omega", "r", "x", "xt", "res", "n")
 
 
-def _lower_inverse(L: torch.Tensor, leaf: int = 256) -> torch.Tensor:
+def _lower_inverse(L: torch.Tensor, leaf: int = 2048) -> torch.Tensor:
     """L^-1 of a lower-triangular FP64 matrix by recursive halving:
     [[A, 0], [B, C]]^-1 = [[A^-1, 0], [-C^-1 B A^-1, C^-1]]; blocks of at most `leaf` rows are
     inverted by a triangular solve.  About n^3/3 multiply-adds, nearly all in matrix products."""
@@ -149,6 +149,14 @@ class MGHierarchy:
     @property
     def finest(self):
         return self.levels[0]
+
+    def update_mask(self):
+        """Re-inject the coarse levels' node masks from the finest one (after the finest mask tensor
+        was rewritten in place); update_modulus must follow, as the diagonals and the coarsest
+        matrix depend on the masks."""
+        for i in range(1, len(self.levels)):
+            prev, L = self.levels[i - 1], self.levels[i]
+            _lib.call("vx_coarsen_mask", *prev.shape, prev.mask.data_ptr(), L.mask.data_ptr(), _s())
 
     def update_modulus(self, E):
         """New finest modulus (FP64, same grid): refresh every level's moduli, inverse diagonal and

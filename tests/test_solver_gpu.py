@@ -229,3 +229,27 @@ def test_coarse_solve_from_the_packed_inverse_factor(n):
                  y.data_ptr(), z.data_ptr(), st)
     ref = np.linalg.solve(A, r) * bits
     assert rel(z, ref) < 1e-12
+
+
+def test_host_api_reuses_its_setup_for_new_inputs():
+    """vx.solve keeps the solver of a known set-up; a second call with other moduli AND another
+    mask must give what a fresh solver gives on those inputs (same kernels: iterations equal,
+    displacements to 1e-12)."""
+    shape = (24, 12, 12)
+    mask1, force = vo.cantilever_equal_split(shape)
+    mask2 = mask1.copy()
+    nodes = vo.n_nodes(shape)
+    ix = np.arange(nodes) // ((shape[1] + 1) * (shape[2] + 1))
+    mask2[3 * np.nonzero(ix == 1)[0]] = 0.0                       # x-rollers on the plane ix = 1
+    # smooth densities: with omega = 0.6, i.i.d. random moduli make damped Jacobi diverge
+    E1 = vx.problems.simp_modulus(vx.problems.gaussian_random_field(shape, 4.0, 1), 1e-9).cpu().numpy()
+    E2 = vx.problems.simp_modulus(vx.problems.gaussian_random_field(shape, 4.0, 2), 1e-9).cpu().numpy()
+    kw = dict(precision="mixed", tol=1e-10, maxiter=200, check_every=1)
+    u1, i1 = vx.solve(shape, E1, force, mask1, **kw)
+    u2, i2 = vx.solve(shape, E2, force, mask2, **kw)               # reuses the first call's solver
+    fresh = ElasticitySolver(shape, cu(E2), cu(mask2), tol=1e-10, maxiter=200, check_every=1).solve(cu(force))
+    assert i2["converged"] and i2["iterations"] == fresh.iterations and fresh.converged
+    assert rel(u2, fresh.x.cpu().numpy()) < 1e-12
+    assert np.all(u2[mask2 == 0] == 0)
+    u1b, _ = vx.solve(shape, E1, force, mask1, **kw)               # and back
+    assert rel(u1b, u1) < 1e-12
