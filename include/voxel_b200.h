@@ -280,6 +280,11 @@ int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, const void*
                     cudaStream_t stream);
 int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const void* zn, const void* zo,
                double* partials, cudaStream_t stream);
+/* FP64 x += S[alpha] p (skipped once S says done or breakdown) followed by vx_cg_direction, with p
+ * read once: the x update of src/voxel_mg.py:199 deferred into the direction update of :209 on the
+ * iterations that do not test the true residual.  z, z_old iterates of `zprec`. */
+int vx_cg_direction_update(int zprec, int64_t n, const double* S, const void* z, double* p, void* z_old,
+                           double* x, cudaStream_t stream);
 int vx_jacobi_precond_dot(int prec, int64_t n, const void* d, const void* r, void* z, double* partials,
                           cudaStream_t stream);
 /* V-cycle entry: r_mg = (prec) r64 (skipped if r_mg is NULL) and x = omega * inv_diag * r_mg;

@@ -62,6 +62,7 @@ SIGNATURES = {
     "vx_jacobi_precond_dot": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P]),
     "vx_vcycle_entry": (c_int, [c_int, c_int64, _P, _P, _P, c_double, _P, _P]),
     "vx_coarse_pack": (c_int, [c_int, _P, _P, _P]),
+    "vx_cg_direction_update": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P, _P]),
     "vx_coarse_apply_factor": (c_int, [c_int, c_int, _P, _P, _P, _P, _P, _P]),
     "vx_vcycle_entry_update": (c_int, [c_int, c_int64, _P, _P, _P, _P, _P, c_double, _P, _P]),
     "vx_scaled_product": (c_int, [c_int, c_int64, c_double, _P, _P, _P, _P]),

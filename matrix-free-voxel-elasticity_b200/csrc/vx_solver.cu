@@ -116,6 +116,20 @@ __global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, con
     if (z_old) z_old[i] = zr;
 }
 
+// The same direction update preceded by the deferred x += alpha p of this iteration (p still the old
+// direction), skipped once the loop has converged or broken down: one read of p serves both.
+template <typename T, typename TZ>
+__global__ void cg_direction_update_kernel(int64_t n, const double* __restrict__ S, const TZ* __restrict__ z,
+                                           T* __restrict__ p, TZ* __restrict__ z_old, T* __restrict__ x) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T pi = p[i];
+    if (S[S_DONE] == 0.0 && S[S_BREAK] == 0.0) x[i] = x[i] + T(S[S_ALPHA]) * pi;
+    const TZ zr = z[i];
+    p[i] = T(Storage<TZ>::cvt(zr)) + T(S[S_BETA]) * pi;
+    if (z_old) z_old[i] = zr;
+}
+
 // partials for r . zn and r . (zn - zo), fixed grid G (a function of n), fixed order
 template <typename T, typename TZ>
 __global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const TZ* __restrict__ zn,
@@ -265,6 +279,19 @@ extern "C" int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, 
         cg_direction_kernel<float, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p, (float*)z_old);
     else { set_error("vx_cg_direction: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cg_direction");
+    return VX_OK;
+}
+
+extern "C" int vx_cg_direction_update(int zprec, int64_t n, const double* S, const void* z, double* p, void* z_old,
+                                      double* x, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction_update: n must be positive");
+    VX_CHECK_ARG(S && z && p && x, VX_ERR_NULL_POINTER, "vx_cg_direction_update: NULL pointer");
+    const bool ok = dispatch_prec(zprec, [&](auto t) {
+        using X = typename decltype(t)::X;
+        cg_direction_update_kernel<double, X><<<nb(n, 256), 256, 0, stream>>>(n, S, (const X*)z, p, (X*)z_old, x);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction_update: unsupported precision %d", zprec);
+    VX_CHECK_LAUNCH("vx_cg_direction_update");
     return VX_OK;
 }
 

@@ -429,13 +429,15 @@ class FCGSolver:
 
     def _iteration(self, check: bool):
         op, S, pp = self.op, self.S.data_ptr(), self.partials.data_ptr()
-        # r -= alpha q is applied by the preconditioner's first kernel when it can (one read of r
-        # saved), else here; at a check iteration r is replaced by b - A x instead
+        # Off the check iterations the updates ride on kernels that stream the same vectors anyway:
+        # r -= alpha q in the preconditioner's first kernel, x += alpha p in the direction update.
+        # At a check iteration x is updated here and r is replaced by b - A x.
         fuse = not check and getattr(self.M, "fuses_residual_update", False)
         op.apply_dot(self.p, self.E, self.mask, self.q, self.partials)          # q = A p, p.q
         self._fin(FIN_PQ, self.G_op)
-        _lib.call("vx_cg_update", _lib.VX_F64, self.n, S, self.x.data_ptr(), self.p.data_ptr(), self.r.data_ptr(),
-                  self.q.data_ptr(), 0 if (check or fuse) else 1, _s())
+        if not fuse:
+            _lib.call("vx_cg_update", _lib.VX_F64, self.n, S, self.x.data_ptr(), self.p.data_ptr(),
+                      self.r.data_ptr(), self.q.data_ptr(), 0 if check else 1, _s())
         if check:                                                                # r = b - A x (replacement)
             op.true_residual(self.x, self.b, self.E, self.mask, self.r, self.partials)
             self._fin(FIN_TRUE, self.G_op)
@@ -443,8 +445,12 @@ class FCGSolver:
         _lib.call("vx_dots_pr", _lib.VX_F64, self.zprec, self.n, self.r.data_ptr(), z.data_ptr(),
                   self.z_old.data_ptr(), pp, _s())
         self._fin(FIN_BETA_PR, self.G_vec)
-        _lib.call("vx_cg_direction", _lib.VX_F64, self.zprec, self.n, S, z.data_ptr(), self.p.data_ptr(),
-                  self.z_old.data_ptr(), _s())
+        if fuse:
+            _lib.call("vx_cg_direction_update", self.zprec, self.n, S, z.data_ptr(), self.p.data_ptr(),
+                      self.z_old.data_ptr(), self.x.data_ptr(), _s())
+        else:
+            _lib.call("vx_cg_direction", _lib.VX_F64, self.zprec, self.n, S, z.data_ptr(), self.p.data_ptr(),
+                      self.z_old.data_ptr(), _s())
 
     def _body(self, k, checking):
         for j in range(k):
