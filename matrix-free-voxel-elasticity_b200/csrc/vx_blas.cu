@@ -39,6 +39,7 @@ __device__ __forceinline__ double block_sum(double v) {
 // partials[k * G + blockIdx.x] = sum over this CTA's strided elements of a_k * b_k
 template <typename S>
 __global__ void __launch_bounds__(RT) dots_stage1(int64_t n, int count, Vec3<S> a, Vec3<S> b, double* partials) {
+    vx::pdl_begin();
     const int64_t G = gridDim.x;
     for (int k = 0; k < count; ++k) {
         double s = 0.0;
@@ -51,6 +52,7 @@ __global__ void __launch_bounds__(RT) dots_stage1(int64_t n, int count, Vec3<S> 
 
 // out[k] = sum_j partials[k * G + j] in a fixed order (one CTA)
 __global__ void __launch_bounds__(RT) reduce_stage2(int64_t G, int count, const double* partials, double* out) {
+    vx::pdl_begin();
     for (int k = 0; k < count; ++k) {
         double s = 0.0;
         for (int64_t j = threadIdx.x; j < G; j += RT) s += partials[k * G + j];
@@ -61,6 +63,7 @@ __global__ void __launch_bounds__(RT) reduce_stage2(int64_t G, int count, const 
 
 template <typename S>
 __global__ void axpby_kernel(int64_t n, double alpha, const S* __restrict__ x, double beta, S* __restrict__ y) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     using C = decltype(Storage<S>::load(x));
@@ -69,6 +72,7 @@ __global__ void axpby_kernel(int64_t n, double alpha, const S* __restrict__ x, d
 
 template <typename A, typename B>
 __global__ void cast_kernel(int64_t n, const A* __restrict__ src, B* __restrict__ dst, double scale) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double v = double(Storage<A>::load(src + i));
@@ -78,6 +82,7 @@ __global__ void cast_kernel(int64_t n, const A* __restrict__ src, B* __restrict_
 
 template <typename S>
 __global__ void simp_kernel(int64_t n, const double* __restrict__ rho, double emin, double de, double penal, S* E) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double r = rho[i];
@@ -91,9 +96,9 @@ inline unsigned nblocks(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 template <typename A>
 int cast_to(int64_t n, const A* src, int dst_prec, void* dst, double scale, cudaStream_t s) {
     const unsigned g = nblocks(n, 256);
-    if (dst_prec == VX_F64) cast_kernel<A, double><<<g, 256, 0, s>>>(n, src, (double*)dst, scale);
-    else if (dst_prec == VX_F32) cast_kernel<A, float><<<g, 256, 0, s>>>(n, src, (float*)dst, scale);
-    else if (dst_prec == VX_BF16_F32) cast_kernel<A, __nv_bfloat16><<<g, 256, 0, s>>>(n, src, (__nv_bfloat16*)dst, scale);
+    if (dst_prec == VX_F64) vx::launch(cast_kernel<A, double>, g, 256, 0, s, n, src, (double*)dst, scale);
+    else if (dst_prec == VX_F32) vx::launch(cast_kernel<A, float>, g, 256, 0, s, n, src, (float*)dst, scale);
+    else if (dst_prec == VX_BF16_F32) vx::launch(cast_kernel<A, __nv_bfloat16>, g, 256, 0, s, n, src, (__nv_bfloat16*)dst, scale);
     else { set_error("vx_cast: unknown destination precision %d", dst_prec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cast");
     return VX_OK;
@@ -113,17 +118,17 @@ extern "C" int vx_dots(int prec, int64_t n, int count, const void* const* a, con
     if (prec == VX_F64) {
         Vec3<double> va{}, vb{};
         for (int k = 0; k < count; ++k) { va.p[k] = (const double*)a[k]; vb.p[k] = (const double*)b[k]; }
-        dots_stage1<double><<<unsigned(G), RT, 0, stream>>>(n, count, va, vb, partials);
+        vx::launch(dots_stage1<double>, unsigned(G), RT, 0, stream, n, count, va, vb, partials);
     } else if (prec == VX_F32) {
         Vec3<float> va{}, vb{};
         for (int k = 0; k < count; ++k) { va.p[k] = (const float*)a[k]; vb.p[k] = (const float*)b[k]; }
-        dots_stage1<float><<<unsigned(G), RT, 0, stream>>>(n, count, va, vb, partials);
+        vx::launch(dots_stage1<float>, unsigned(G), RT, 0, stream, n, count, va, vb, partials);
     } else {
         set_error("vx_dots: unsupported precision %d", prec);
         return VX_ERR_INVALID_ARGUMENT;
     }
     VX_CHECK_LAUNCH("vx_dots(stage 1)");
-    reduce_stage2<<<1, RT, 0, stream>>>(G, count, partials, out);
+    vx::launch(reduce_stage2, 1, RT, 0, stream, G, count, partials, out);
     VX_CHECK_LAUNCH("vx_dots(stage 2)");
     return VX_OK;
 }
@@ -131,7 +136,7 @@ extern "C" int vx_dots(int prec, int64_t n, int count, const void* const* a, con
 extern "C" int vx_reduce_partials(int64_t G, int count, const double* partials, double* out, cudaStream_t stream) {
     VX_CHECK_ARG(G > 0 && count >= 1, VX_ERR_INVALID_ARGUMENT, "vx_reduce_partials: bad sizes");
     VX_CHECK_ARG(partials && out, VX_ERR_NULL_POINTER, "vx_reduce_partials: NULL pointer");
-    reduce_stage2<<<1, RT, 0, stream>>>(G, count, partials, out);
+    vx::launch(reduce_stage2, 1, RT, 0, stream, G, count, partials, out);
     VX_CHECK_LAUNCH("vx_reduce_partials");
     return VX_OK;
 }
@@ -139,8 +144,8 @@ extern "C" int vx_reduce_partials(int64_t G, int count, const double* partials, 
 extern "C" int vx_axpby(int prec, int64_t n, double alpha, const void* x, double beta, void* y, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_axpby: n must be positive");
     VX_CHECK_ARG(x && y, VX_ERR_NULL_POINTER, "vx_axpby: NULL pointer");
-    if (prec == VX_F64) axpby_kernel<double><<<nblocks(n, 256), 256, 0, stream>>>(n, alpha, (const double*)x, beta, (double*)y);
-    else if (prec == VX_F32) axpby_kernel<float><<<nblocks(n, 256), 256, 0, stream>>>(n, alpha, (const float*)x, beta, (float*)y);
+    if (prec == VX_F64) vx::launch(axpby_kernel<double>, nblocks(n, 256), 256, 0, stream, n, alpha, (const double*)x, beta, (double*)y);
+    else if (prec == VX_F32) vx::launch(axpby_kernel<float>, nblocks(n, 256), 256, 0, stream, n, alpha, (const float*)x, beta, (float*)y);
     else { set_error("vx_axpby: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_axpby");
     return VX_OK;
@@ -162,9 +167,9 @@ extern "C" int vx_simp_modulus(int prec, int64_t n, const double* rho, double em
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_simp_modulus: n must be positive");
     VX_CHECK_ARG(rho && E, VX_ERR_NULL_POINTER, "vx_simp_modulus: NULL pointer");
     const unsigned g = nblocks(n, 256);
-    if (prec == VX_F64) simp_kernel<double><<<g, 256, 0, stream>>>(n, rho, emin, emax - emin, penal, (double*)E);
-    else if (prec == VX_F32) simp_kernel<float><<<g, 256, 0, stream>>>(n, rho, emin, emax - emin, penal, (float*)E);
-    else if (prec == VX_BF16_F32) simp_kernel<__nv_bfloat16><<<g, 256, 0, stream>>>(n, rho, emin, emax - emin, penal, (__nv_bfloat16*)E);
+    if (prec == VX_F64) vx::launch(simp_kernel<double>, g, 256, 0, stream, n, rho, emin, emax - emin, penal, (double*)E);
+    else if (prec == VX_F32) vx::launch(simp_kernel<float>, g, 256, 0, stream, n, rho, emin, emax - emin, penal, (float*)E);
+    else if (prec == VX_BF16_F32) vx::launch(simp_kernel<__nv_bfloat16>, g, 256, 0, stream, n, rho, emin, emax - emin, penal, (__nv_bfloat16*)E);
     else { set_error("vx_simp_modulus: unknown precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_simp_modulus");
     return VX_OK;

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 
 #include "../../include/voxel_b200.h"
 
@@ -33,6 +34,34 @@ void set_error(const char* fmt, ...);
     } while (0)
 
 inline bool aligned(const void* p, size_t bytes) { return (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
+
+// ---------------------------------------------------------------------------- launches
+// Every kernel of the library is launched with programmatic stream serialization: the next kernel
+// in the stream may be scheduled while this one drains, which hides the launch gap between the
+// many short kernels of a solver iteration (also inside captured graphs).  Correctness does not
+// depend on it: every kernel begins with pdl_begin(), whose griddepcontrol.wait returns only once
+// the previous kernel has completed and its memory is visible (at once when there is none); its
+// trigger then lets the following kernel be scheduled.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                          Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Grid extents: element grid (nx, ny, nz); nodes (nx+1)(ny+1)(nz+1); author layout, z fastest.
 struct Grid {

@@ -13,18 +13,26 @@ __device__ __forceinline__ void node_coords(const Grid& g, int64_t n, int& ix, i
     ix = int(n / (int64_t(g.nz + 1) * (g.ny + 1)));
 }
 
+// Launch shape of the restriction: threads along z (TZ_T x TY_T per CTA), grid (z chunks, y rows /
+// TY_T, x planes), so no thread divides to find its node; offsets in 32 bits (fewer than 2^31 DOFs).
+constexpr int TZ_T = 64, TY_T = 2;
+inline dim3 transfer_grid(const Grid& g) {
+    return dim3(unsigned((g.nz + 1 + TZ_T - 1) / TZ_T), unsigned((g.ny + 1 + TY_T - 1) / TY_T), unsigned(g.nx + 1));
+}
+__device__ __forceinline__ int node32(const Grid& g, int ix, int iy, int iz) { return (ix * (g.ny + 1) + iy) * (g.nz + 1) + iz; }
+
 // coarse node (I,J,K) of fine grid f: rc = sum w(a) w(b) w(d) f(2I+a, 2J+b, 2K+d), w(0)=1, w(+-1)=1/2.
 // Arithmetic in arith_t<T> (bf16 storage: FP32).
 template <typename T>
-__global__ void restrict_kernel(Grid f, Grid c, const T* __restrict__ fine, const uint8_t* __restrict__ cmask,
-                                T* __restrict__ coarse) {
+__global__ void __launch_bounds__(TZ_T * TY_T) restrict_kernel(Grid f, Grid c, const T* __restrict__ fine,
+                                                              const uint8_t* __restrict__ cmask, T* __restrict__ coarse) {
+    vx::pdl_begin();
     using A = arith_t<T>;
-    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (n >= c.nodes()) return;
-    int I, J, K;
-    node_coords(c, n, I, J, K);
+    const int K = blockIdx.x * TZ_T + threadIdx.x, J = blockIdx.y * TY_T + threadIdx.y, I = blockIdx.z;
+    if (K > c.nz || J > c.ny) return;
+    const int n = node32(c, I, J, K);
     const unsigned bits = cmask ? unsigned(cmask[n]) : 7u;
-    auto ld = [&](int64_t i) { return Storage<T>::load(fine + i); };
+    auto ld = [&](int i) { return Storage<T>::load(fine + i); };
     for (int comp = 0; comp < 3; ++comp) {
         A ty[3][3];   // after the x pass, at fine (y = 2J + b - 1, z = 2K + d - 1)
         for (int b = 0; b < 3; ++b)
@@ -32,9 +40,9 @@ __global__ void restrict_kernel(Grid f, Grid c, const T* __restrict__ fine, cons
                 const int fy = 2 * J + b - 1, fz = 2 * K + d - 1;
                 A v = A(0);
                 if (fy >= 0 && fy <= f.ny && fz >= 0 && fz <= f.nz) {
-                    v = ld(3 * f.node(2 * I, fy, fz) + comp);
-                    if (2 * I + 1 <= f.nx) v = v + A(0.5) * ld(3 * f.node(2 * I + 1, fy, fz) + comp);
-                    if (I >= 1) v = v + A(0.5) * ld(3 * f.node(2 * I - 1, fy, fz) + comp);
+                    v = ld(3 * node32(f, 2 * I, fy, fz) + comp);
+                    if (2 * I + 1 <= f.nx) v = v + A(0.5) * ld(3 * node32(f, 2 * I + 1, fy, fz) + comp);
+                    if (I >= 1) v = v + A(0.5) * ld(3 * node32(f, 2 * I - 1, fy, fz) + comp);
                 }
                 ty[b][d] = v;
             }
@@ -52,10 +60,13 @@ __global__ void restrict_kernel(Grid f, Grid c, const T* __restrict__ fine, cons
     }
 }
 
-// x(i,j,k) += (P ec)(i,j,k) * mask; P is the separable trilinear interpolation
+// x(i,j,k) += (P ec)(i,j,k) * mask; P is the separable trilinear interpolation.  One thread per fine
+// node in a 1-D launch: consecutive threads read and write consecutive nodes of x (measured faster
+// than the 3-D launch of the restriction, whose threads gather from three fine planes).
 template <typename T>
 __global__ void prolong_add_kernel(Grid f, Grid c, const T* __restrict__ coarse, const uint8_t* __restrict__ fmask,
                                    T* __restrict__ x) {
+    vx::pdl_begin();
     using A = arith_t<T>;
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= f.nodes()) return;
@@ -82,6 +93,7 @@ __global__ void prolong_add_kernel(Grid f, Grid c, const T* __restrict__ coarse,
 
 template <typename S>
 __global__ void coarsen_modulus_kernel(Grid f, Grid c, const S* __restrict__ Ef, S* __restrict__ Ec) {
+    vx::pdl_begin();
     const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= c.elems()) return;
     const int ez = int(e % c.nz), ey = int((e / c.nz) % c.ny), ex = int(e / (int64_t(c.nz) * c.ny));
@@ -93,6 +105,7 @@ __global__ void coarsen_modulus_kernel(Grid f, Grid c, const S* __restrict__ Ef,
 }
 
 __global__ void coarsen_mask_kernel(Grid f, Grid c, const uint8_t* __restrict__ mf, uint8_t* __restrict__ mc) {
+    vx::pdl_begin();
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= c.nodes()) return;
     int I, J, K;
@@ -105,6 +118,7 @@ struct Ke576 { double k[576]; };
 // one thread per (row DOF, neighbour offset, column component); A is zeroed beforehand
 __global__ void assemble_dense_kernel(Grid g, const __grid_constant__ Ke576 ke, const double* __restrict__ E,
                                       const uint8_t* __restrict__ mask, double* __restrict__ A) {
+    vx::pdl_begin();
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t nn = g.nodes();
     if (t >= nn * 3 * 81) return;
@@ -161,6 +175,7 @@ template <typename TR, typename T>
 __global__ void __launch_bounds__(CT) coarse_apply_kernel(int n, const double* __restrict__ Ainv,
                                                           const TR* __restrict__ r, const uint8_t* __restrict__ mask,
                                                           T* __restrict__ z) {
+    vx::pdl_begin();
     using A = arith_t<T>;
     const int row = blockIdx.x;
     const double s = block_row_dot(Ainv + int64_t(row) * n, 0, n, [&](int j) { return double(Storage<TR>::load(r + j)); });
@@ -174,6 +189,7 @@ __global__ void __launch_bounds__(CT) coarse_apply_kernel(int n, const double* _
 // A^-1 r = Linv^T (Linv r) reads row i of M left of the diagonal (pass 1) and right of it (pass 2).
 // 32x32 tiles through shared memory keep the transposed reads coalesced.
 __global__ void coarse_pack_kernel(int n, const double* __restrict__ linv, double* __restrict__ m) {
+    vx::pdl_begin();
     __shared__ double tile[32][33];
     const int bi = blockIdx.y * 32, bj = blockIdx.x * 32;      // output tile rows bi.., cols bj..
     const int tx = threadIdx.x, ty = threadIdx.y;              // 32 x 8 threads
@@ -202,6 +218,7 @@ __global__ void coarse_pack_kernel(int n, const double* __restrict__ linv, doubl
 template <typename TR>
 __global__ void __launch_bounds__(CT) coarse_lower_kernel(int n, const double* __restrict__ m,
                                                           const TR* __restrict__ r, double* __restrict__ y) {
+    vx::pdl_begin();
     const int row = blockIdx.x;
     const double s = block_row_dot(m + int64_t(row) * n, 0, row + 1, [&](int j) { return double(Storage<TR>::load(r + j)); });
     if (threadIdx.x == 0) y[row] = s;
@@ -212,6 +229,7 @@ template <typename T>
 __global__ void __launch_bounds__(CT) coarse_upper_kernel(int n, const double* __restrict__ m,
                                                           const double* __restrict__ y,
                                                           const uint8_t* __restrict__ mask, T* __restrict__ z) {
+    vx::pdl_begin();
     using A = arith_t<T>;
     const int row = blockIdx.x;
     const double s = block_row_dot(m + int64_t(row) * n, row, n, [&](int j) { return y[j]; });
@@ -222,6 +240,7 @@ __global__ void __launch_bounds__(CT) coarse_upper_kernel(int n, const double* _
 }
 
 __global__ void mask_from_dofs_kernel(int64_t nodes, const double* __restrict__ m, uint8_t* __restrict__ out) {
+    vx::pdl_begin();
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= nodes) return;
     out[n] = uint8_t((m[3 * n] != 0.0) | ((m[3 * n + 1] != 0.0) << 1) | ((m[3 * n + 2] != 0.0) << 2));
@@ -232,6 +251,10 @@ inline unsigned blocks_for(int64_t n, int t) { return unsigned((n + t - 1) / t);
 int check_even(int nx, int ny, int nz, const char* what) {
     int st = check_grid(nx, ny, nz);
     if (st) return st;
+    if (nx + 1 > 65535 || (ny + 1 + TY_T - 1) / TY_T > 65535) {      // grid dimensions of the transfer launches
+        set_error("%s: fine grid (%d, %d, %d) is too long in x or y for one launch", what, nx, ny, nz);
+        return VX_ERR_INVALID_ARGUMENT;
+    }
     if ((nx | ny | nz) & 1) {
         set_error("%s: fine grid (%d, %d, %d) must have even extents", what, nx, ny, nz);
         return VX_ERR_INVALID_ARGUMENT;
@@ -251,7 +274,7 @@ extern "C" int vx_restrict(int prec, int nx, int ny, int nz, const void* fine, c
     Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
     const bool ok = dispatch_prec(prec, [&](auto t) {             // auxiliary vectors on both sides
         using R = typename decltype(t)::R;
-        restrict_kernel<R><<<blocks_for(c.nodes(), 128), 128, 0, stream>>>(f, c, (const R*)fine, coarse_mask, (R*)coarse);
+        vx::launch(restrict_kernel<R>, transfer_grid(c), dim3(TZ_T, TY_T), 0, stream, f, c, (const R*)fine, coarse_mask, (R*)coarse);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_restrict: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_restrict");
@@ -266,7 +289,7 @@ extern "C" int vx_prolong_add(int prec, int nx, int ny, int nz, const void* coar
     Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
     const bool ok = dispatch_prec(prec, [&](auto t) {             // iterates on both sides
         using X = typename decltype(t)::X;
-        prolong_add_kernel<X><<<blocks_for(f.nodes(), 256), 256, 0, stream>>>(f, c, (const X*)coarse, fine_mask, (X*)x);
+        vx::launch(prolong_add_kernel<X>, blocks_for(f.nodes(), 256), 256, 0, stream, f, c, (const X*)coarse, fine_mask, (X*)x);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_prolong_add: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_prolong_add");
@@ -282,7 +305,7 @@ extern "C" int vx_coarsen_modulus(int prec, int nx, int ny, int nz, const void* 
     const unsigned gb = blocks_for(c.elems(), 256);
     const bool ok = dispatch_prec(prec, [&](auto t) {
         using M = typename decltype(t)::M;
-        coarsen_modulus_kernel<M><<<gb, 256, 0, stream>>>(f, c, (const M*)E_fine, (M*)E_coarse);
+        vx::launch(coarsen_modulus_kernel<M>, gb, 256, 0, stream, f, c, (const M*)E_fine, (M*)E_coarse);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarsen_modulus: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarsen_modulus");
@@ -295,7 +318,7 @@ extern "C" int vx_coarsen_mask(int nx, int ny, int nz, const uint8_t* mask_fine,
     if (st) return st;
     VX_CHECK_ARG(mask_fine && mask_coarse, VX_ERR_NULL_POINTER, "vx_coarsen_mask: NULL pointer");
     Grid f{nx, ny, nz}, c{nx / 2, ny / 2, nz / 2};
-    coarsen_mask_kernel<<<blocks_for(c.nodes(), 256), 256, 0, stream>>>(f, c, mask_fine, mask_coarse);
+    vx::launch(coarsen_mask_kernel, blocks_for(c.nodes(), 256), 256, 0, stream, f, c, mask_fine, mask_coarse);
     VX_CHECK_LAUNCH("vx_coarsen_mask");
     return VX_OK;
 }
@@ -313,7 +336,7 @@ extern "C" int vx_assemble_dense(int nx, int ny, int nz, const double* ke, const
     for (int i = 0; i < 576; ++i) k.k[i] = ke[i];
     cudaError_t e = cudaMemsetAsync(A, 0, size_t(n) * size_t(n) * sizeof(double), stream);
     if (e != cudaSuccess) { set_error("vx_assemble_dense: memset: %s", cudaGetErrorString(e)); return VX_ERR_CUDA; }
-    assemble_dense_kernel<<<blocks_for(g.nodes() * 243, 256), 256, 0, stream>>>(g, k, E, node_mask, A);
+    vx::launch(assemble_dense_kernel, blocks_for(g.nodes() * 243, 256), 256, 0, stream, g, k, E, node_mask, A);
     VX_CHECK_LAUNCH("vx_assemble_dense");
     return VX_OK;
 }
@@ -325,7 +348,7 @@ extern "C" int vx_coarse_apply(int prec, int n, const double* Ainv, const void* 
     const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
         using R = typename decltype(t)::R;
         using X = typename decltype(t)::X;
-        coarse_apply_kernel<R, X><<<unsigned(n), CT, 0, stream>>>(n, Ainv, (const R*)r, node_mask, (X*)z);
+        vx::launch(coarse_apply_kernel<R, X>, unsigned(n), CT, 0, stream, n, Ainv, (const R*)r, node_mask, (X*)z);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarse_apply");
@@ -335,7 +358,7 @@ extern "C" int vx_coarse_apply(int prec, int n, const double* Ainv, const void* 
 extern "C" int vx_mask_from_dofs(int64_t nodes, const double* dof_mask, uint8_t* node_mask, cudaStream_t stream) {
     VX_CHECK_ARG(nodes > 0, VX_ERR_INVALID_ARGUMENT, "vx_mask_from_dofs: nodes must be positive");
     VX_CHECK_ARG(dof_mask && node_mask, VX_ERR_NULL_POINTER, "vx_mask_from_dofs: NULL pointer");
-    mask_from_dofs_kernel<<<blocks_for(nodes, 256), 256, 0, stream>>>(nodes, dof_mask, node_mask);
+    vx::launch(mask_from_dofs_kernel, blocks_for(nodes, 256), 256, 0, stream, nodes, dof_mask, node_mask);
     VX_CHECK_LAUNCH("vx_mask_from_dofs");
     return VX_OK;
 }
@@ -345,7 +368,7 @@ extern "C" int vx_coarse_pack(int n, const double* linv, double* m, cudaStream_t
     VX_CHECK_ARG(linv && m, VX_ERR_NULL_POINTER, "vx_coarse_pack: NULL pointer");
     VX_CHECK_ARG(linv != m, VX_ERR_INVALID_ARGUMENT, "vx_coarse_pack: m may not alias linv");
     const unsigned t = unsigned((n + 31) / 32);
-    coarse_pack_kernel<<<dim3(t, t), dim3(32, 8), 0, stream>>>(n, linv, m);
+    vx::launch(coarse_pack_kernel, dim3(t, t), dim3(32, 8), 0, stream, n, linv, m);
     VX_CHECK_LAUNCH("vx_coarse_pack");
     return VX_OK;
 }
@@ -357,8 +380,8 @@ extern "C" int vx_coarse_apply_factor(int prec, int n, const double* m, const vo
     const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
         using R = typename decltype(t)::R;
         using X = typename decltype(t)::X;
-        coarse_lower_kernel<R><<<unsigned(n), CT, 0, stream>>>(n, m, (const R*)r, y);
-        coarse_upper_kernel<X><<<unsigned(n), CT, 0, stream>>>(n, m, y, node_mask, (X*)z);
+        vx::launch(coarse_lower_kernel<R>, unsigned(n), CT, 0, stream, n, m, (const R*)r, y);
+        vx::launch(coarse_upper_kernel<X>, unsigned(n), CT, 0, stream, n, m, y, node_mask, (X*)z);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply_factor: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarse_apply_factor");

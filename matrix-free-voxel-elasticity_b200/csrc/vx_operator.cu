@@ -87,6 +87,7 @@ __device__ __forceinline__ void block_sum_store(double v, double* out) {
 template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP>
 __global__ void __launch_bounds__(NW * 32, 1)
 parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
+    vx::pdl_begin();
     const int lane = threadIdx.x & 31;
     const int row = threadIdx.x >> 5;
     const Grid g = a.g;
@@ -388,6 +389,7 @@ struct XpPlane {
 template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC>
 __global__ void __launch_bounds__(XpCfg<TC>::NW * 32, XpCfg<TC>::MINB)
 parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
+    vx::pdl_begin();
     constexpr int NWS = XpCfg<TC>::NW;
     constexpr int TYS = NWS - 2;
     using P = V2<TC>;
@@ -762,12 +764,12 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
         }
         if (cubic) {
             a2.K = cube_constants<TC>(a.C);
-            parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+            vx::launch(parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true>, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a2);
         } else {
-            parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a2);
+            vx::launch(parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false>, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a2);
         }
     } else {
-        parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP><<<stream_grid(a.g, t, a.cx), unsigned(threads), smem, s>>>(a);
+        vx::launch(parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a);
     }
     VX_CHECK_LAUNCH(what);
     return VX_OK;
@@ -784,6 +786,7 @@ BlocksT<TC> convert_blocks(const double* blocks) {
 template <typename T>
 __global__ void dense_gather(Grid g, const T* __restrict__ ke, const T* __restrict__ E,
                              const T* __restrict__ u, T* __restrict__ y) {
+    vx::pdl_begin();
     __shared__ T K[576];
     for (int i = threadIdx.x; i < 576; i += blockDim.x) K[i] = ke[i];
     __syncthreads();
@@ -819,6 +822,7 @@ template <typename T, bool REV, int MASK, bool SIMP>
 __global__ void diag_kernel(Grid g, BlocksT<T> kd /* c[0..23]: diagonal of ke */, const T* __restrict__ E,
                             const uint8_t* __restrict__ node_mask, const double* __restrict__ dof_mask,
                             double emin, double de, double penal, int mode, T* __restrict__ d) {
+    vx::pdl_begin();
     const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (n >= g.nodes()) return;
     const int iz = int(n % (g.nz + 1));
@@ -856,6 +860,7 @@ __global__ void energy_kernel(Grid g, const __grid_constant__ Ke ke, const doubl
                               const double* __restrict__ dof_mask, double* __restrict__ ce,
                               const double* __restrict__ rho, double emin, double de, double penal,
                               double* __restrict__ dc) {
+    vx::pdl_begin();
     const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= g.elems()) return;
     const int ez = int(e % g.nz);
@@ -931,10 +936,10 @@ extern "C" int vx_matvec_dense(int prec, int nx, int ny, int nz, const double* k
     const unsigned blocksz = 128;
     const unsigned grid = unsigned((n + blocksz - 1) / blocksz);
     if (prec == VX_F64) {
-        dense_gather<double><<<grid, blocksz, 0, stream>>>(g, ke, (const double*)E, (const double*)u, (double*)y);
+        vx::launch(dense_gather<double>, grid, blocksz, 0, stream, g, ke, (const double*)E, (const double*)u, (double*)y);
     } else if (prec == VX_F32) {
         // ke is device FP32 here
-        dense_gather<float><<<grid, blocksz, 0, stream>>>(g, (const float*)ke, (const float*)E, (const float*)u, (float*)y);
+        vx::launch(dense_gather<float>, grid, blocksz, 0, stream, g, (const float*)ke, (const float*)E, (const float*)u, (float*)y);
     } else {
         set_error("vx_matvec_dense: unsupported precision %d", prec);
         return VX_ERR_INVALID_ARGUMENT;
@@ -954,12 +959,12 @@ extern "C" int vx_diagonal(int prec, int nx, int ny, int nz, const double* ke, c
     if (prec == VX_F64) {
         BlocksT<double> kd{};
         for (int i = 0; i < 24; ++i) kd.c[i] = ke[25 * i];
-        diag_kernel<double, false, MASK_NODE, false><<<grid, 256, 0, stream>>>(
+        vx::launch(diag_kernel<double, false, MASK_NODE, false>, grid, 256, 0, stream, 
             g, kd, (const double*)E, node_mask, nullptr, 0, 0, 0, inverse ? 1 : 0, (double*)d);
     } else if (prec == VX_F32) {
         BlocksT<float> kd{};
         for (int i = 0; i < 24; ++i) kd.c[i] = float(ke[25 * i]);
-        diag_kernel<float, false, MASK_NODE, false><<<grid, 256, 0, stream>>>(
+        vx::launch(diag_kernel<float, false, MASK_NODE, false>, grid, 256, 0, stream, 
             g, kd, (const float*)E, node_mask, nullptr, 0, 0, 0, inverse ? 1 : 0, (float*)d);
     } else {
         set_error("vx_diagonal: unsupported precision %d", prec);
@@ -980,7 +985,7 @@ extern "C" int vx_element_energy(int nx, int ny, int nz, const double* ke, const
     Ke k;
     for (int i = 0; i < 576; ++i) k.k[i] = ke[i];
     const int64_t n = g.elems();
-    energy_kernel<false, MASK_NONE><<<unsigned((n + 127) / 128), 128, 0, stream>>>(
+    vx::launch(energy_kernel<false, MASK_NONE>, unsigned((n + 127) / 128), 128, 0, stream, 
         g, k, u, nullptr, ce, rho, emin, emax - emin, penal, dc);
     VX_CHECK_LAUNCH("vx_element_energy");
     return VX_OK;
@@ -1026,14 +1031,14 @@ extern "C" int vx_product(int nx, int ny, int nz, const double* rho, const doubl
         Ke k;
         for (int i = 0; i < 576; ++i) k.k[i] = kp[i];
         const int64_t n = g.elems();
-        energy_kernel<true, MASK_DOF><<<unsigned((n + 127) / 128), 128, 0, stream>>>(
+        vx::launch(energy_kernel<true, MASK_DOF>, unsigned((n + 127) / 128), 128, 0, stream, 
             g, k, u, mask, ce, nullptr, 0.0, 0.0, 0.0, nullptr);
         VX_CHECK_LAUNCH("vx_product(ce)");
     }
     if (diag) {
         BlocksT<double> kd{};
         for (int i = 0; i < 24; ++i) kd.c[i] = kp[25 * i];
-        diag_kernel<double, true, MASK_DOF, true><<<unsigned((g.nodes() + 255) / 256), 256, 0, stream>>>(
+        vx::launch(diag_kernel<double, true, MASK_DOF, true>, unsigned((g.nodes() + 255) / 256), 256, 0, stream, 
             g, kd, rho, nullptr, mask, emin, emax - emin, penal, 2, diag);
         VX_CHECK_LAUNCH("vx_product(diag)");
     }

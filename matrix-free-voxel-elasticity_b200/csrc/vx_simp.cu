@@ -19,6 +19,7 @@ struct FilterTaps {
 // order of the reference's stencil loops (donor filter_r2.py:55-72).
 __global__ void cone_filter_kernel(Grid g, const __grid_constant__ FilterTaps t, const double* __restrict__ x,
                                    const double* __restrict__ s, int mode, double* __restrict__ y) {
+    vx::pdl_begin();
     const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= g.elems()) return;
     const int ez = int(e % g.nz), ey = int((e / g.nz) % g.ny), ex = int(e / (int64_t(g.nz) * g.ny));
@@ -48,6 +49,7 @@ __global__ void __launch_bounds__(256) oc_probe_kernel(int64_t n, const double* 
                                                        const double* __restrict__ dc, const double* __restrict__ dv,
                                                        const double* __restrict__ w, double move,
                                                        const double* __restrict__ S, double* __restrict__ partials) {
+    vx::pdl_begin();
     __shared__ double red[8];
     const double lmid = 0.5 * (S[OC_L2] + S[OC_L1]);
     double acc = 0.0;
@@ -67,6 +69,7 @@ __global__ void __launch_bounds__(256) oc_probe_kernel(int64_t n, const double* 
 // volume = sum / n; l1 or l2 := lmid; done when (l2 - l1) / (l1 + l2) <= tol (the top88 test,
 // experiments/session_h/run_w1b.py:53-62)
 __global__ void oc_finalize_kernel(int64_t G, const double* __restrict__ partials, double* __restrict__ S) {
+    vx::pdl_begin();
     __shared__ double red[8];
     double acc = 0.0;
     for (int64_t j = threadIdx.x; j < G; j += 256) acc += partials[j];
@@ -91,6 +94,7 @@ __global__ void oc_finalize_kernel(int64_t G, const double* __restrict__ partial
 __global__ void oc_apply_kernel(int64_t n, const double* __restrict__ x, const double* __restrict__ dc,
                                 const double* __restrict__ dv, double move, const double* __restrict__ S,
                                 double* __restrict__ x_new) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     x_new[i] = oc_design(x[i], dc[i], dv[i], S[OC_LMID], move);
@@ -126,7 +130,7 @@ extern "C" int vx_cone_filter(int nx, int ny, int nz, double rmin, const double*
                 ++t.n;
             }
     Grid g{nx, ny, nz};
-    cone_filter_kernel<<<unsigned((g.elems() + 255) / 256), 256, 0, stream>>>(g, t, x, s, mode, y);
+    vx::launch(cone_filter_kernel, unsigned((g.elems() + 255) / 256), 256, 0, stream, g, t, x, s, mode, y);
     VX_CHECK_LAUNCH("vx_cone_filter");
     return VX_OK;
 }
@@ -137,7 +141,7 @@ extern "C" int vx_oc_probe(int64_t n, const double* x, const double* dc, const d
                            double move, const double* S, double* partials, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_oc_probe: n must be positive");
     VX_CHECK_ARG(x && dc && dv && w && S && partials, VX_ERR_NULL_POINTER, "vx_oc_probe: NULL pointer");
-    oc_probe_kernel<<<unsigned(oc_ctas(n)), 256, 0, stream>>>(n, x, dc, dv, w, move, S, partials);
+    vx::launch(oc_probe_kernel, unsigned(oc_ctas(n)), 256, 0, stream, n, x, dc, dv, w, move, S, partials);
     VX_CHECK_LAUNCH("vx_oc_probe");
     return VX_OK;
 }
@@ -145,7 +149,7 @@ extern "C" int vx_oc_probe(int64_t n, const double* x, const double* dc, const d
 extern "C" int vx_oc_finalize(int64_t n, const double* partials, double* S, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_oc_finalize: n must be positive");
     VX_CHECK_ARG(partials && S, VX_ERR_NULL_POINTER, "vx_oc_finalize: NULL pointer");
-    oc_finalize_kernel<<<1, 256, 0, stream>>>(oc_ctas(n), partials, S);
+    vx::launch(oc_finalize_kernel, 1, 256, 0, stream, oc_ctas(n), partials, S);
     VX_CHECK_LAUNCH("vx_oc_finalize");
     return VX_OK;
 }
@@ -154,7 +158,7 @@ extern "C" int vx_oc_apply(int64_t n, const double* x, const double* dc, const d
                            const double* S, double* x_new, cudaStream_t stream) {
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_oc_apply: n must be positive");
     VX_CHECK_ARG(x && dc && dv && S && x_new, VX_ERR_NULL_POINTER, "vx_oc_apply: NULL pointer");
-    oc_apply_kernel<<<unsigned((n + 255) / 256), 256, 0, stream>>>(n, x, dc, dv, move, S, x_new);
+    vx::launch(oc_apply_kernel, unsigned((n + 255) / 256), 256, 0, stream, n, x, dc, dv, move, S, x_new);
     VX_CHECK_LAUNCH("vx_oc_apply");
     return VX_OK;
 }

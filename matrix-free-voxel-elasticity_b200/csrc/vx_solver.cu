@@ -47,6 +47,7 @@ __device__ double block_sum_ft(double v) {
 
 __global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const double* __restrict__ partials,
                                                       double* __restrict__ S) {
+    vx::pdl_begin();
     double s0 = 0.0, s1 = 0.0;
     for (int64_t j = threadIdx.x; j < G; j += FT) s0 += partials[j];
     s0 = block_sum_ft(s0);
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const d
 template <typename T>
 __global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __restrict__ x, const T* __restrict__ p,
                                  T* __restrict__ r, const T* __restrict__ q, int update_r) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (S[S_DONE] != 0.0 || S[S_BREAK] != 0.0) return;
@@ -109,6 +111,7 @@ __global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __r
 template <typename T, typename TZ>
 __global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, const TZ* __restrict__ z, T* __restrict__ p,
                                     TZ* __restrict__ z_old) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const TZ zr = z[i];
@@ -121,6 +124,7 @@ __global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, con
 template <typename T, typename TZ>
 __global__ void cg_direction_update_kernel(int64_t n, const double* __restrict__ S, const TZ* __restrict__ z,
                                            T* __restrict__ p, TZ* __restrict__ z_old, T* __restrict__ x) {
+    vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const T pi = p[i];
@@ -134,6 +138,7 @@ __global__ void cg_direction_update_kernel(int64_t n, const double* __restrict__
 template <typename T, typename TZ>
 __global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const TZ* __restrict__ zn,
                                                      const TZ* __restrict__ zo, double* __restrict__ partials) {
+    vx::pdl_begin();
     const int64_t G = gridDim.x;
     double a = 0.0, b = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
@@ -153,6 +158,7 @@ __global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restr
 template <typename T>
 __global__ void __launch_bounds__(FT) jacobi_precond_dot_kernel(int64_t n, const T* __restrict__ d, const T* __restrict__ r,
                                                                 T* __restrict__ z, double* __restrict__ partials) {
+    vx::pdl_begin();
     const int64_t G = gridDim.x;
     double a = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
@@ -169,6 +175,7 @@ __global__ void __launch_bounds__(FT) jacobi_precond_dot_kernel(int64_t n, const
 template <typename TX, typename TR>
 __global__ void vcycle_entry_kernel(int64_t n, const double* __restrict__ r64, TR* __restrict__ rmg,
                                     const TR* __restrict__ invd, double omega, TX* __restrict__ x) {
+    vx::pdl_begin();
     using A = arith_t<TX>;
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -183,6 +190,7 @@ template <typename TX, typename TR>
 __global__ void vcycle_entry_update_kernel(int64_t n, const double* __restrict__ S, double* __restrict__ r64,
                                            const double* __restrict__ q, TR* __restrict__ rmg,
                                            const TR* __restrict__ invd, double omega, TX* __restrict__ x) {
+    vx::pdl_begin();
     using A = arith_t<TX>;
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -200,6 +208,7 @@ __global__ void vcycle_entry_update_kernel(int64_t n, const double* __restrict__
 template <typename TX, typename TR>
 __global__ void scaled_product_kernel(int64_t n, double omega, const TR* __restrict__ a, const TR* __restrict__ b,
                                       TX* __restrict__ out) {
+    vx::pdl_begin();
     using A = arith_t<TX>;
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -207,11 +216,13 @@ __global__ void scaled_product_kernel(int64_t n, double omega, const TR* __restr
 }
 
 __global__ void set_scalars_kernel(double* S, int first, int count, double value) {
+    vx::pdl_begin();
     const int i = threadIdx.x;
     if (i < count) S[first + i] = value;
 }
 
 __global__ void condition_kernel(cudaGraphConditionalHandle h, const double* __restrict__ S) {
+    vx::pdl_begin();
     if (threadIdx.x == 0) {
         // S[S_CHECK] = iterations per loop body: the next body must not pass maxiter
         const bool go = S[S_DONE] == 0.0 && S[S_BREAK] == 0.0 && S[S_IT] + S[S_CHECK] <= S[S_MAXIT];
@@ -244,7 +255,7 @@ extern "C" int64_t vx_solver_partials(int64_t n) { return fixed_ctas(n); }
 extern "C" int vx_solver_finalize(int op, int64_t G, const double* partials, double* S, cudaStream_t stream) {
     VX_CHECK_ARG(op >= 0 && op <= FIN_RR_ONLY && G > 0, VX_ERR_INVALID_ARGUMENT, "vx_solver_finalize: bad op/G");
     VX_CHECK_ARG(partials && S, VX_ERR_NULL_POINTER, "vx_solver_finalize: NULL pointer");
-    finalize_kernel<<<1, FT, 0, stream>>>(op, G, partials, S);
+    vx::launch(finalize_kernel, 1, FT, 0, stream, op, G, partials, S);
     VX_CHECK_LAUNCH("vx_solver_finalize");
     return VX_OK;
 }
@@ -254,10 +265,10 @@ extern "C" int vx_cg_update(int prec, int64_t n, const double* S, void* x, const
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_update: n must be positive");
     VX_CHECK_ARG(S && x && p && (!update_r || (r && q)), VX_ERR_NULL_POINTER, "vx_cg_update: NULL pointer");
     if (prec == VX_F64)
-        cg_update_kernel<double><<<nb(n, 256), 256, 0, stream>>>(n, S, (double*)x, (const double*)p, (double*)r,
+        vx::launch(cg_update_kernel<double>, nb(n, 256), 256, 0, stream, n, S, (double*)x, (const double*)p, (double*)r,
                                                                  (const double*)q, update_r);
     else if (prec == VX_F32)
-        cg_update_kernel<float><<<nb(n, 256), 256, 0, stream>>>(n, S, (float*)x, (const float*)p, (float*)r,
+        vx::launch(cg_update_kernel<float>, nb(n, 256), 256, 0, stream, n, S, (float*)x, (const float*)p, (float*)r,
                                                                 (const float*)q, update_r);
     else { set_error("vx_cg_update: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cg_update");
@@ -269,14 +280,14 @@ extern "C" int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, 
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction: n must be positive");
     VX_CHECK_ARG(S && z && p, VX_ERR_NULL_POINTER, "vx_cg_direction: NULL pointer");
     if (prec == VX_F64 && zprec == VX_F64)
-        cg_direction_kernel<double, double><<<nb(n, 256), 256, 0, stream>>>(n, S, (const double*)z, (double*)p, (double*)z_old);
+        vx::launch(cg_direction_kernel<double, double>, nb(n, 256), 256, 0, stream, n, S, (const double*)z, (double*)p, (double*)z_old);
     else if (prec == VX_F64 && zprec == VX_F32)
-        cg_direction_kernel<double, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (double*)p, (float*)z_old);
+        vx::launch(cg_direction_kernel<double, float>, nb(n, 256), 256, 0, stream, n, S, (const float*)z, (double*)p, (float*)z_old);
     else if (prec == VX_F64 && zprec == VX_BF16_F32)
-        cg_direction_kernel<double, __nv_bfloat16><<<nb(n, 256), 256, 0, stream>>>(n, S, (const __nv_bfloat16*)z, (double*)p,
+        vx::launch(cg_direction_kernel<double, __nv_bfloat16>, nb(n, 256), 256, 0, stream, n, S, (const __nv_bfloat16*)z, (double*)p,
                                                                                    (__nv_bfloat16*)z_old);
     else if (prec == VX_F32 && zprec == VX_F32)
-        cg_direction_kernel<float, float><<<nb(n, 256), 256, 0, stream>>>(n, S, (const float*)z, (float*)p, (float*)z_old);
+        vx::launch(cg_direction_kernel<float, float>, nb(n, 256), 256, 0, stream, n, S, (const float*)z, (float*)p, (float*)z_old);
     else { set_error("vx_cg_direction: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cg_direction");
     return VX_OK;
@@ -288,7 +299,7 @@ extern "C" int vx_cg_direction_update(int zprec, int64_t n, const double* S, con
     VX_CHECK_ARG(S && z && p && x, VX_ERR_NULL_POINTER, "vx_cg_direction_update: NULL pointer");
     const bool ok = dispatch_prec(zprec, [&](auto t) {
         using X = typename decltype(t)::X;
-        cg_direction_update_kernel<double, X><<<nb(n, 256), 256, 0, stream>>>(n, S, (const X*)z, p, (X*)z_old, x);
+        vx::launch(cg_direction_update_kernel<double, X>, nb(n, 256), 256, 0, stream, n, S, (const X*)z, p, (X*)z_old, x);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction_update: unsupported precision %d", zprec);
     VX_CHECK_LAUNCH("vx_cg_direction_update");
@@ -301,14 +312,14 @@ extern "C" int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const v
     VX_CHECK_ARG(r && zn && partials, VX_ERR_NULL_POINTER, "vx_dots_pr: NULL pointer");
     const unsigned G = unsigned(fixed_ctas(n));
     if (prec == VX_F64 && zprec == VX_F64)
-        dots_pr_kernel<double, double><<<G, FT, 0, stream>>>(n, (const double*)r, (const double*)zn, (const double*)zo, partials);
+        vx::launch(dots_pr_kernel<double, double>, G, FT, 0, stream, n, (const double*)r, (const double*)zn, (const double*)zo, partials);
     else if (prec == VX_F64 && zprec == VX_F32)
-        dots_pr_kernel<double, float><<<G, FT, 0, stream>>>(n, (const double*)r, (const float*)zn, (const float*)zo, partials);
+        vx::launch(dots_pr_kernel<double, float>, G, FT, 0, stream, n, (const double*)r, (const float*)zn, (const float*)zo, partials);
     else if (prec == VX_F64 && zprec == VX_BF16_F32)
-        dots_pr_kernel<double, __nv_bfloat16><<<G, FT, 0, stream>>>(n, (const double*)r, (const __nv_bfloat16*)zn,
+        vx::launch(dots_pr_kernel<double, __nv_bfloat16>, G, FT, 0, stream, n, (const double*)r, (const __nv_bfloat16*)zn,
                                                                     (const __nv_bfloat16*)zo, partials);
     else if (prec == VX_F32 && zprec == VX_F32)
-        dots_pr_kernel<float, float><<<G, FT, 0, stream>>>(n, (const float*)r, (const float*)zn, (const float*)zo, partials);
+        vx::launch(dots_pr_kernel<float, float>, G, FT, 0, stream, n, (const float*)r, (const float*)zn, (const float*)zo, partials);
     else { set_error("vx_dots_pr: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_dots_pr");
     return VX_OK;
@@ -320,9 +331,9 @@ extern "C" int vx_jacobi_precond_dot(int prec, int64_t n, const void* d, const v
     VX_CHECK_ARG(d && r && z && partials, VX_ERR_NULL_POINTER, "vx_jacobi_precond_dot: NULL pointer");
     const unsigned G = unsigned(fixed_ctas(n));
     if (prec == VX_F64)
-        jacobi_precond_dot_kernel<double><<<G, FT, 0, stream>>>(n, (const double*)d, (const double*)r, (double*)z, partials);
+        vx::launch(jacobi_precond_dot_kernel<double>, G, FT, 0, stream, n, (const double*)d, (const double*)r, (double*)z, partials);
     else if (prec == VX_F32)
-        jacobi_precond_dot_kernel<float><<<G, FT, 0, stream>>>(n, (const float*)d, (const float*)r, (float*)z, partials);
+        vx::launch(jacobi_precond_dot_kernel<float>, G, FT, 0, stream, n, (const float*)d, (const float*)r, (float*)z, partials);
     else { set_error("vx_jacobi_precond_dot: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_jacobi_precond_dot");
     return VX_OK;
@@ -335,7 +346,7 @@ extern "C" int vx_vcycle_entry(int prec, int64_t n, const double* r64, void* r_m
     const bool ok = dispatch_prec(prec, [&](auto t) {
         using X = typename decltype(t)::X;
         using R = typename decltype(t)::R;
-        vcycle_entry_kernel<X, R><<<nb(n, 256), 256, 0, stream>>>(n, r64, (R*)r_mg, (const R*)inv_diag, omega, (X*)x);
+        vx::launch(vcycle_entry_kernel<X, R>, nb(n, 256), 256, 0, stream, n, r64, (R*)r_mg, (const R*)inv_diag, omega, (X*)x);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_vcycle_entry");
@@ -349,7 +360,7 @@ extern "C" int vx_vcycle_entry_update(int prec, int64_t n, const double* S, doub
     const bool ok = dispatch_prec(prec, [&](auto t) {
         using X = typename decltype(t)::X;
         using R = typename decltype(t)::R;
-        vcycle_entry_update_kernel<X, R><<<nb(n, 256), 256, 0, stream>>>(n, S, r64, q, (R*)r_mg, (const R*)inv_diag,
+        vx::launch(vcycle_entry_update_kernel<X, R>, nb(n, 256), 256, 0, stream, n, S, r64, q, (R*)r_mg, (const R*)inv_diag,
                                                                          omega, (X*)x);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_vcycle_entry_update: unsupported precision %d", prec);
@@ -364,7 +375,7 @@ extern "C" int vx_scaled_product(int prec, int64_t n, double omega, const void* 
     const bool ok = dispatch_prec(prec, [&](auto t) {
         using X = typename decltype(t)::X;
         using R = typename decltype(t)::R;
-        scaled_product_kernel<X, R><<<nb(n, 256), 256, 0, stream>>>(n, omega, (const R*)a, (const R*)b, (X*)out);
+        vx::launch(scaled_product_kernel<X, R>, nb(n, 256), 256, 0, stream, n, omega, (const R*)a, (const R*)b, (X*)out);
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_scaled_product: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_scaled_product");
@@ -375,7 +386,7 @@ extern "C" int vx_set_scalars(double* S, int first, int count, double value, cud
     VX_CHECK_ARG(S, VX_ERR_NULL_POINTER, "vx_set_scalars: NULL S");
     VX_CHECK_ARG(first >= 0 && count >= 1 && first + count <= S_COUNT, VX_ERR_INVALID_ARGUMENT,
                  "vx_set_scalars: slots out of range");
-    set_scalars_kernel<<<1, 32, 0, stream>>>(S, first, count, value);
+    vx::launch(set_scalars_kernel, 1, 32, 0, stream, S, first, count, value);
     VX_CHECK_LAUNCH("vx_set_scalars");
     return VX_OK;
 }
@@ -421,7 +432,7 @@ extern "C" int vx_graph_while_begin(cudaStream_t stream, void** handle) {
 extern "C" int vx_graph_while_end(void* handle, const double* S, cudaStream_t stream) {
     VX_CHECK_ARG(handle && S, VX_ERR_NULL_POINTER, "vx_graph_while_end: NULL pointer");
     auto* w = static_cast<WhileGraph*>(handle);
-    condition_kernel<<<1, 32, 0, stream>>>(w->handle, S);
+    vx::launch(condition_kernel, 1, 32, 0, stream, w->handle, S);
     cudaError_t e = cudaGetLastError();
     cudaGraph_t captured = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(stream, &captured);
