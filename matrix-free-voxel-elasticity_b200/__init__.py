@@ -11,7 +11,7 @@ from .layout import edof_author, element_nodes, n_elems, n_nodes, to_author, to_
 from .operators import (Product, VoxelOperator, cast, dofs_from_node_mask, dots, node_mask_from_dofs,
                         product, reduce_partials, simp_modulus)
 from . import problems, solver, voxel_mg  # noqa: E402
-from .solver import FCGSolver, JacobiPCG, JacobiPreconditioner, MGHierarchy, SolveResult, hierarchy_shapes
+from .solver import FCGSolver, JacobiPCG, JacobiPreconditioner, MGHierarchy, PCGIR, SolveResult, hierarchy_shapes
 from .api import ElasticitySolver, solve
 from . import serving, simp  # noqa: E402
 from .simp import Compliance, ConeFilter, OCUpdater, compliance, oc_top88, run_simp
@@ -19,6 +19,6 @@ from .simp import Compliance, ConeFilter, OCUpdater, compliance, oc_top88, run_s
 __all__ = ["XYZ", "Modal", "element", "quadrature", "edof_author", "element_nodes", "n_elems", "n_nodes",
            "to_author", "to_natural", "Product", "VoxelOperator", "cast", "dofs_from_node_mask", "dots",
            "node_mask_from_dofs", "product", "reduce_partials", "simp_modulus", "problems", "solver", "voxel_mg",
-           "FCGSolver", "JacobiPCG", "JacobiPreconditioner", "MGHierarchy", "SolveResult", "hierarchy_shapes",
+           "FCGSolver", "JacobiPCG", "JacobiPreconditioner", "MGHierarchy", "PCGIR", "SolveResult", "hierarchy_shapes",
            "ElasticitySolver", "solve", "simp", "Compliance", "ConeFilter", "OCUpdater", "compliance", "oc_top88",
            "run_simp", "serving"]

@@ -694,3 +694,86 @@ class JacobiPCG:
                 s = self._read()
         caller.wait_stream(self.stream)
         return PCGResult(self.x, int(s[S_IT]), bool(s[S_DONE]), float(s[S_REL]))
+
+
+@dataclass
+class IRResult:
+    x: torch.Tensor
+    outer: int
+    inner: int
+    converged: bool
+    rel: float
+
+    def __iter__(self):     # unpacks like the donor's (x, outer, inner_total, converged, rel)
+        return iter((self.x, self.outer, self.inner, self.converged, self.rel))
+
+
+class PCGIR:
+    """Mixed-precision iterative refinement (donor experiments/session_a/donor/src/gpu_fem/
+    simp_r2.py:298-385): the FP64 residual r = b - A x, an FP32 Jacobi-PCG correction of the scaled
+    system A d = r / |r| to `inner_tol`, x += |r| d; a divergence guard undoes a correction that
+    raised the residual and tightens the inner tolerance tenfold (giving up below 1e-5).  Every
+    vector operation is a library kernel; the outer loop reads one norm per pass.
+    Returns IRResult (x, outer, inner, converged, rel)."""
+
+    def __init__(self, op64: VoxelOperator, E64, node_mask, tol=1e-5, inner_tol=1e-1, max_outer=40,
+                 inner_maxiter=4000, check_every=50, graph=True):
+        if op64.dtype != torch.float64:
+            raise ValueError("the outer operator must be float64")
+        self.op64, self.E64, self.mask = op64, E64.contiguous(), node_mask
+        self.tol, self.inner_tol = float(tol), float(inner_tol)
+        self.max_outer, self.inner_maxiter = int(max_outer), int(inner_maxiter)
+        n = op64.ndof
+        self.n = n
+        op32 = VoxelOperator(op64.shape, op64.ke, torch.float32)
+        self.E32 = torch.empty(self.E64.numel(), dtype=torch.float32, device="cuda")
+        _lib.call("vx_cast", self.E64.numel(), _lib.VX_F64, self.E64.data_ptr(), _lib.VX_F32, self.E32.data_ptr(), 1.0, _s())
+        self.inner = JacobiPCG(op32, self.E32, node_mask, tol=inner_tol, maxiter=inner_maxiter,
+                               check_every=check_every, graph=graph)
+        f64 = dict(dtype=torch.float64, device="cuda")
+        self.x = torch.zeros(n, **f64)
+        self.r = torch.zeros(n, **f64)
+        self.corr = torch.zeros(n, **f64)                    # the last correction |r| d, for the undo
+        self.rhs32 = torch.zeros(n, dtype=torch.float32, device="cuda")
+        self.partials = torch.zeros(op64.partials_size, **f64)
+        self.norm = torch.zeros(1, **f64)
+
+    def _residual_norm(self, b):
+        self.op64.true_residual(self.x, b, self.E64, self.mask, self.r, self.partials)
+        _lib.call("vx_reduce_partials", self.partials.numel(), 1, self.partials.data_ptr(), self.norm.data_ptr(), _s())
+        return float(self.norm) ** 0.5
+
+    def solve(self, b: torch.Tensor, x0: torch.Tensor | None = None) -> IRResult:
+        b = b.contiguous()
+        nb = float(torch.linalg.vector_norm(b))
+        if nb <= 0:
+            self.x.zero_()
+            return IRResult(self.x, 0, 0, True, 0.0)
+        if x0 is None:
+            self.x.zero_()
+        else:
+            self.x.copy_(x0)
+        n, inner_total = self.n, 0
+        tol_in, rel_prev, have_last = self.inner_tol, None, False
+        outer = 0
+        for outer in range(1, self.max_outer + 1):
+            scale = self._residual_norm(b)
+            rel = scale / nb
+            if rel <= self.tol:
+                return IRResult(self.x, outer - 1, inner_total, True, rel)
+            if rel_prev is not None and rel > rel_prev and have_last:      # divergence guard: undo
+                _lib.call("vx_axpby", _lib.VX_F64, n, -1.0, self.corr.data_ptr(), 1.0, self.x.data_ptr(), _s())
+                have_last = False
+                tol_in *= 0.1
+                if tol_in < 1e-5:
+                    return IRResult(self.x, outer, inner_total, False, rel_prev)
+                continue
+            rel_prev = rel
+            _lib.call("vx_cast", n, _lib.VX_F64, self.r.data_ptr(), _lib.VX_F32, self.rhs32.data_ptr(), 1.0 / scale, _s())
+            d = self.inner.solve(self.rhs32, tol=tol_in)
+            inner_total += d.iterations
+            _lib.call("vx_cast", n, _lib.VX_F32, d.x.data_ptr(), _lib.VX_F64, self.corr.data_ptr(), scale, _s())
+            _lib.call("vx_axpby", _lib.VX_F64, n, 1.0, self.corr.data_ptr(), 1.0, self.x.data_ptr(), _s())
+            have_last = True
+        rel = self._residual_norm(b) / nb
+        return IRResult(self.x, outer, inner_total, bool(rel <= self.tol), rel)

@@ -253,3 +253,21 @@ def test_host_api_reuses_its_setup_for_new_inputs():
     assert np.all(u2[mask2 == 0] == 0)
     u1b, _ = vx.solve(shape, E1, force, mask1, **kw)               # and back
     assert rel(u1b, u1) < 1e-12
+
+
+def test_pcg_ir_matches_the_donor_record():
+    """Config 1 (32x16x16, i.i.d. densities), donor pcg_ir at tol 1e-8, inner tolerance 0.1: the
+    reference's run takes 6 outer passes and 1400 inner FP32 iterations.  The inner products here
+    are FP32 arithmetic (the donor rounds FP64 products to FP32), so the inner count may differ by a
+    few iterations; the outer count, convergence and the compliance (to 1e-8) must agree."""
+    g = golden("config1.npz")
+    shape = tuple(int(v) for v in g["shape"])
+    op = vx.VoxelOperator(shape, vo.quadrature([1, 1, 1], 0.3))
+    nm = vx.node_mask_from_dofs(cu(g["mask"]))
+    ir = vs.PCGIR(op, cu(g["E"]), nm, tol=1e-8, inner_tol=1e-1, max_outer=40, inner_maxiter=4000, check_every=50)
+    x, outer, inner, ok, r = ir.solve(cu(g["force"]))
+    print(f"pcg_ir: outer {outer} inner {inner} rel {r:.3e} (donor: {int(g['ir_outer'])}, {int(g['ir_inner'])})")
+    assert ok and r <= 1e-8 and outer == int(g["ir_outer"])
+    assert abs(inner - int(g["ir_inner"])) <= 0.05 * int(g["ir_inner"])
+    comp = float(cu(g["force"]) @ x)
+    assert abs(comp - float(g["fcg_compliance"])) <= 1e-8 * abs(float(g["fcg_compliance"]))
