@@ -46,6 +46,71 @@ def cantilever_line_load(shape):
     return mask.ravel(), force.ravel()
 
 
+def _clamped_face(nx, ny, nz):
+    """DOF mask with every DOF of the x = 0 face fixed (author layout, numpy)."""
+    mask = np.ones((nx + 1, ny + 1, nz + 1, 3))
+    mask[0] = 0.0
+    return mask
+
+
+def _face_indices(n_nodes, h, centre, half, tol=1e-12, exact=False):
+    """Node indices along one face axis whose coordinate i*h lies within the patch; the nearest
+    node when none does.  `exact` uses the |coord - centre| <= half test of the torsion patches."""
+    coords = np.arange(n_nodes) * h
+    if exact:
+        sel = np.abs(coords - centre) <= half + tol
+    else:
+        sel = (coords >= centre - half - tol) & (coords <= centre + half + tol)
+    idx = np.nonzero(sel)[0]
+    return idx if idx.size else np.array([int(round(centre / h))])
+
+
+def donor_cantilever(nelx, nely, nelz, Lx=2.0, Ly=1.0, Lz=0.5, load="patch", patch_frac=None,
+                     patch_size=0.1, total_load=-1.0):
+    """The donor SIMP benchmark's cantilever (experiments/session_a/donor/src/gpu_fem/simp_r2.py:64-131):
+    the x = 0 face clamped; a transverse (y) load on the x = nelx face, either at the node nearest
+    the face centre ("point") or spread evenly over the nodes of a square patch of fixed physical
+    side centred there ("patch"; side patch_frac * Lz when given, else patch_size).  Returns
+    (dof_mask, force, patch_nodes) as numpy float64 arrays in author layout."""
+    nx, ny, nz = int(nelx), int(nely), int(nelz)
+    mask = _clamped_face(nx, ny, nz)
+    force = np.zeros((nx + 1, ny + 1, nz + 1, 3))
+    hy, hz = Ly / ny, Lz / nz
+    if load == "point":
+        jy, jz = int(round((Ly / 2.0) / hy)), int(round((Lz / 2.0) / hz))
+        force[nx, jy, jz, 1] = total_load
+        count = 1
+    elif load == "patch":
+        side = float(patch_size) if patch_frac is None else float(patch_frac) * Lz
+        jy = _face_indices(ny + 1, hy, Ly / 2.0, side / 2.0)
+        jz = _face_indices(nz + 1, hz, Lz / 2.0, side / 2.0)
+        count = jy.size * jz.size
+        force[nx, jy[:, None], jz[None, :], 1] = total_load / count
+    else:
+        raise ValueError(f"unknown load model {load!r}")
+    return mask.reshape(-1), force.reshape(-1), count
+
+
+def donor_torsion(nelx, nely, nelz, Lx=3.0, Ly=1.0, Lz=1.0, patch_size=0.15, total_load=1.0):
+    """The donor's torsion shaft (simp_r2.py:134-178): the x = 0 face clamped; on the x = nelx face a
+    couple from two patches at y = Ly and y = 0 (the z band of width patch_size around Lz / 2),
+    forces (-1/2, +1/2) and (+1/2, -1/2) times total_load in (y, z), each spread evenly over its
+    patch.  Returns (dof_mask, force, patch_nodes)."""
+    nx, ny, nz = int(nelx), int(nely), int(nelz)
+    mask = _clamped_face(nx, ny, nz)
+    force = np.zeros((nx + 1, ny + 1, nz + 1, 3))
+    hy, hz = Ly / ny, Lz / nz
+    jz = _face_indices(nz + 1, hz, Lz / 2.0, patch_size / 2.0, exact=True)
+    count = 0
+    for y_target, sy, sz in ((Ly, -0.5, 0.5), (0.0, 0.5, -0.5)):
+        jy = _face_indices(ny + 1, hy, y_target, patch_size / 2.0, exact=True)
+        k = jy.size * jz.size
+        force[nx, jy[:, None], jz[None, :], 1] += total_load * sy / k
+        force[nx, jy[:, None], jz[None, :], 2] += total_load * sz / k
+        count += k
+    return mask.reshape(-1), force.reshape(-1), count
+
+
 def upsample_natural(rho, shape, factor):
     """Nearest-neighbour repeat of a natural-layout element field (make_inputs.py:42-50)."""
     nx, ny, nz = (int(s) for s in shape)

@@ -36,12 +36,41 @@ def load(name, path):
     return mod
 
 
+DONOR_CASES = (
+    ("cant_patch_a", "cantilever", (8, 4, 2), dict(load="patch")),
+    ("cant_patch_b", "cantilever", (16, 8, 4), dict(load="patch", patch_frac=0.5)),
+    ("cant_patch_c", "cantilever", (12, 6, 6), dict(load="patch", patch_size=0.3, total_load=-2.0)),
+    ("cant_point", "cantilever", (16, 8, 4), dict(load="point")),
+    ("torsion_a", "torsion", (12, 4, 4), dict()),
+    ("torsion_b", "torsion", (9, 6, 6), dict(patch_size=0.4, total_load=2.5)),
+)
+
+
+def donor_problems(ref):
+    """The donor's problem builders (simp_r2.py:64-178): supports and loads in author layout."""
+    sys.modules["cupy"] = np
+    simp = load("ref_simp_r2_problems", ref / "experiments/session_a/donor/src/gpu_fem/simp_r2.py")
+    del sys.modules["cupy"]
+    out = {}
+    for tag, kind, dims, kw in DONOR_CASES:
+        fn = simp.build_cantilever if kind == "cantilever" else simp.build_torsion
+        d = fn(*dims, **kw)
+        out[f"{tag}_fixed"] = np.asarray(d["fixed"])
+        out[f"{tag}_F"] = np.asarray(d["F"])
+        out[f"{tag}_patch_nodes"] = np.array(d["patch_nodes"])
+    np.savez_compressed(HERE / "donor_problems.npz", **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", type=Path, default=Path("/root/reference"))
     ap.add_argument("--skip-slow", action="store_true", help="skip the 128x64x64 GMG solves (~1 min)")
+    ap.add_argument("--only", choices=("donor_problems",), help="write one fixture file only")
     args = ap.parse_args()
     ref = args.ref.resolve()
+    if args.only == "donor_problems":
+        donor_problems(ref)
+        return
 
     subprocess.run(["make", "-C", str(REPO / "oracle"), f"REF={ref}"], check=True)
     mg = load("ref_voxel_mg", ref / "src/voxel_mg.py")
@@ -273,6 +302,7 @@ def main():
         res2["rho_head"] = rho2[:16].tolist()
         res2["shapes"] = shapes2
         (HERE / "config2.json").write_text(json.dumps(res2) + "\n")
+    donor_problems(ref)
     print("golden fixtures written to", HERE)
 
 

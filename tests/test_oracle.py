@@ -224,3 +224,19 @@ def test_line_load_recipe_and_upsample():
     k = golden("kat_inputs.npz")
     rho2, shape2 = vo.upsample(k["q64_rho"], tuple(k["q64_shape"]), 2)
     assert shape2 == (256, 128, 128) and rho2.size == 256 * 128 * 128
+
+
+# ----------------------------------------------------------------------------- donor problems
+@pytest.mark.parametrize("case", ["cant_patch_a", "cant_patch_b", "cant_patch_c", "cant_point", "torsion_a", "torsion_b"])
+def test_donor_problem_builders_match_the_donor(case):
+    """voxel_b200.problems.donor_cantilever / donor_torsion against the donor's own builders
+    (fixtures from tests/golden/make_golden.py): fixed DOFs and loads bit-exact."""
+    from voxel_b200 import problems
+    from tests.golden.make_golden import DONOR_CASES
+    g = golden("donor_problems.npz")
+    _, kind, dims, kw = next(c for c in DONOR_CASES if c[0] == case)
+    fn = problems.donor_cantilever if kind == "cantilever" else problems.donor_torsion
+    mask, force, count = fn(*dims, **kw)
+    assert np.array_equal(np.nonzero(mask == 0)[0], g[f"{case}_fixed"])
+    assert np.array_equal(force, g[f"{case}_F"])
+    assert count == int(g[f"{case}_patch_nodes"])
