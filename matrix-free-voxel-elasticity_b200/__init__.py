@@ -12,7 +12,7 @@ from .operators import (Product, VoxelOperator, cast, dofs_from_node_mask, dots,
                         product, reduce_partials, simp_modulus)
 from . import problems, solver, voxel_mg  # noqa: E402
 from .solver import FCGSolver, JacobiPCG, JacobiPreconditioner, MGHierarchy, PCGIR, SolveResult, hierarchy_shapes
-from .api import ElasticitySolver, solve
+from .api import ElasticitySolver, clear_solver_cache, solve
 from . import serving, simp  # noqa: E402
 from .simp import Compliance, ConeFilter, OCUpdater, compliance, oc_top88, run_simp
 
@@ -20,5 +20,5 @@ __all__ = ["XYZ", "Modal", "element", "quadrature", "edof_author", "element_node
            "to_author", "to_natural", "Product", "VoxelOperator", "cast", "dofs_from_node_mask", "dots",
            "node_mask_from_dofs", "product", "reduce_partials", "simp_modulus", "problems", "solver", "voxel_mg",
            "FCGSolver", "JacobiPCG", "JacobiPreconditioner", "MGHierarchy", "PCGIR", "SolveResult", "hierarchy_shapes",
-           "ElasticitySolver", "solve", "simp", "Compliance", "ConeFilter", "OCUpdater", "compliance", "oc_top88",
+           "ElasticitySolver", "clear_solver_cache", "solve", "simp", "Compliance", "ConeFilter", "OCUpdater", "compliance", "oc_top88",
            "run_simp", "serving"]

@@ -119,6 +119,12 @@ _SOLVERS = OrderedDict()      # set-up key -> ElasticitySolver, least recently u
 _SOLVER_CACHE_SIZE = 4
 
 
+def clear_solver_cache():
+    """Drop the solvers that solve() keeps for recent set-ups (their device memory returns to the
+    caching allocator)."""
+    _SOLVERS.clear()
+
+
 def solve(shape, E, force, mask, *, ke=None, precision="mixed", tol=1e-8, maxiter=200, check_every=1, pre=2,
           post=2, omega=0.6, max_coarse_x=16, levels=None):
     """Host-buffer entry point: E (Ne), force and 0/1 DOF mask (3N), numpy, author layout.
