@@ -312,6 +312,36 @@ int64_t vx_graph_body_nodes(void* handle);
 int vx_capture_status(cudaStream_t stream);
 int vx_graph_destroy(void* handle);
 
+/* ---------------------------------------------------------------------------- x-slab decomposition
+ * A slab holds elements ex in [a, b) and node planes a..b of a global grid (author layout: x is the
+ * slowest index, so a slab's vectors are contiguous slices of the global ones).  The planes a and b
+ * are shared with the neighbouring slabs.  On a shared plane the global operator is the sum of the
+ * two slabs' element-layer contributions; the reference runs one process on one grid
+ * (experiments/session_i/run_gpu.py:304 A, src/voxel_mg.py:120-178 Level/Multigrid), and these two
+ * entry points make a slab-local operator the global one.
+ *
+ * vx_layer_partial: out (3 (ny+1)(nz+1) values, arithmetic type: FP64 for VX_F64, FP32 otherwise)
+ * = M K_layer (M u) on node plane `side` (0 lower, 1 upper) of the single element layer whose
+ * modulus is E (ny*nz, auxiliary storage) and whose two node planes are u (iterate storage) and
+ * node_mask (NULL: all free).  `ke` is a HOST pointer to the 24x24 element matrix.
+ *
+ * vx_plane_fix: rewrites one shared plane (`nodes` nodes) of an operator form's output from
+ * s = lo + hi (the lower slab's contribution first, so both holders compute identical values),
+ * with A x = s on free DOFs and x on fixed ones:
+ *   mode 0  out = A x                                 (arithmetic type; vx_matvec's output)
+ *   mode 1  out = x + omega inv_diag (r - A x)        (iterate; vx_jacobi_sweep's output)
+ *   mode 2  out = scale * (free ? r - A x : 0)        (auxiliary; vx_residual's output; scale 1/2
+ *                                                      splits a shared plane before restriction)
+ *   mode 3  out = r - A x                             (VX_F64 only; vx_true_residual's output)
+ * vx_plane_sum: out = lo + hi (n values of the selector's auxiliary storage): the restricted
+ * right-hand side on a shared coarse plane. */
+int vx_layer_partial(int prec, int ny, int nz, const double* ke, const void* E, const void* u,
+                     const uint8_t* node_mask, int side, void* out, cudaStream_t stream);
+int vx_plane_fix(int prec, int mode, int64_t nodes, const void* lo, const void* hi, const uint8_t* node_mask,
+                 const void* x, const void* r, const void* inv_diag, double omega, double scale, void* out,
+                 cudaStream_t stream);
+int vx_plane_sum(int prec, int64_t n, const void* lo, const void* hi, void* out, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

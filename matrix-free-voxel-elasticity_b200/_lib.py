@@ -79,6 +79,10 @@ SIGNATURES = {
     "vx_oc_probe": (c_int, [c_int64, _P, _P, _P, _P, c_double, _P, _P, _P]),
     "vx_oc_finalize": (c_int, [c_int64, _P, _P, _P]),
     "vx_oc_apply": (c_int, [c_int64, _P, _P, _P, c_double, _P, _P, _P]),
+    # x-slab decomposition
+    "vx_layer_partial": (c_int, [c_int, c_int, c_int, _D, _P, _P, _P, c_int, _P, _P]),
+    "vx_plane_fix": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P, _P, c_double, c_double, _P, _P]),
+    "vx_plane_sum": (c_int, [c_int, c_int64, _P, _P, _P, _P]),
 }
 
 _lib = None

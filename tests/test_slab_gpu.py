@@ -1,0 +1,192 @@
+"""The x-slab decomposition on one B200: several slabs held by one process exchange their shared
+planes by device copies, which runs every kernel and every step of the multi-GPU path except the
+NCCL transport (covered by the gloo tests of test_slab.py).
+
+Bars: the two slab kernels against the oracle (FP64 1e-13, FP32 1e-5, bf16 inputs exact in the
+oracle, FP32 arithmetic 1e-5); the slab FP64 operator and V-cycle against the single-grid ones to
+1e-12 (summation order only) with shared planes bitwise equal in both holders; slab solves reach
+the FP64 relative residual 1e-8 in the single-grid iteration counts and the single-grid compliance
+to 1e-7 relative (the solve tolerance)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from oracle import voxel_oracle as vo
+
+pytestmark = pytest.mark.gpu
+vx = pytest.importorskip("voxel_b200")
+from voxel_b200 import _lib  # noqa: E402
+from voxel_b200 import solver as vs  # noqa: E402
+from voxel_b200.api import ElasticitySolver  # noqa: E402
+from voxel_b200.slab import SlabComm, SlabHierarchy, SlabSolver  # noqa: E402
+
+KE = vo.quadrature([1, 1, 1], 0.3)
+DT = {_lib.VX_F64: (torch.float64, torch.float64), _lib.VX_F32: (torch.float32, torch.float32),
+      _lib.VX_BF16_F32: (torch.bfloat16, torch.bfloat16), _lib.VX_F32_BF16AUX: (torch.float32, torch.bfloat16)}
+
+
+def _s():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _mask(shape, seed, p=0.06):
+    nx, ny, nz = shape
+    m = np.ones((nx + 1, ny + 1, nz + 1, 3))
+    m[0] = 0.0
+    m[np.random.default_rng(seed).random(m.shape) < p] = 0.0
+    return m.ravel()
+
+
+@pytest.mark.parametrize("prec", list(DT))
+@pytest.mark.parametrize("ny,nz", [(5, 7), (48, 40)])
+def test_layer_partial_matches_oracle(prec, ny, nz):
+    it, aux = DT[prec]
+    rng = np.random.default_rng(ny + prec)
+    P3 = 3 * (ny + 1) * (nz + 1)
+    E = torch.as_tensor(1e-3 + rng.random(ny * nz), device="cuda").to(aux)
+    u = torch.as_tensor(rng.standard_normal(2 * P3), device="cuda").to(it)
+    m = _mask((1, ny, nz), prec, 0.2)
+    nm = vx.node_mask_from_dofs(torch.as_tensor(m, device="cuda"))
+    ref = vo.product_raw((1, ny, nz), KE, u.double().cpu().numpy() * m, E.double().cpu().numpy()) * m
+    arith = torch.float64 if prec == _lib.VX_F64 else torch.float32
+    tol = 1e-13 if prec == _lib.VX_F64 else 1e-5
+    for side in (0, 1):
+        out = torch.empty(P3, dtype=arith, device="cuda")
+        _lib.call("vx_layer_partial", prec, ny, nz, _lib.dptr(np.ascontiguousarray(KE)), E.data_ptr(), u.data_ptr(),
+                  nm.data_ptr(), side, out.data_ptr(), _s())
+        want = ref[side * P3:(side + 1) * P3]
+        assert np.max(np.abs(out.double().cpu().numpy() - want)) <= tol * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("prec", [_lib.VX_F64, _lib.VX_F32])
+def test_plane_fix_modes(prec):
+    it, aux = DT[prec]
+    nodes = 1000
+    n3 = 3 * nodes
+    rng = np.random.default_rng(5)
+    t = lambda a, dt: torch.as_tensor(a, device="cuda").to(dt)          # noqa: E731
+    lo, hi, x, r, d = (rng.standard_normal(n3) for _ in range(5))
+    bits = rng.integers(0, 8, nodes).astype(np.uint8)
+    fr = ((bits[:, None] >> np.arange(3)) & 1).ravel().astype(bool)
+    ax = np.where(fr, lo + hi, x)
+    want = {0: ax, 1: x + 0.6 * d * (r - ax), 2: 0.5 * np.where(fr, r - ax, 0.0), 3: r - ax}
+    tol = 1e-15 if prec == _lib.VX_F64 else 1e-6
+    for mode, ref in want.items():
+        if mode == 3 and prec != _lib.VX_F64:
+            continue
+        out = torch.zeros(n3, dtype=it, device="cuda")
+        _lib.call("vx_plane_fix", prec, mode, nodes, t(lo, it).data_ptr(), t(hi, it).data_ptr(),
+                  t(bits, torch.uint8).data_ptr(), t(x, it).data_ptr(), t(r, aux).data_ptr(), t(d, aux).data_ptr(),
+                  0.6, 0.5, out.data_ptr(), _s())
+        assert np.max(np.abs(out.double().cpu().numpy() - ref)) <= tol * np.max(np.abs(ref)) * 4
+
+
+def _problem(shape, seed=0, interior_fixed=False):
+    rho = vx.problems.gaussian_random_field(shape, 8.0, seed)
+    E = vx.problems.simp_modulus(rho, 1e-9)
+    mask, force = vx.problems.cantilever_equal_split(shape)
+    if interior_fixed:
+        mask = mask * torch.as_tensor(_mask(shape, seed, 0.02), device="cuda")
+        force = force * mask
+    return E, mask, force
+
+
+def _hier(shape, E, mask, nparts, dtype=torch.float64, aux=None, **kw):
+    nm = vx.node_mask_from_dofs(mask)
+    return SlabHierarchy(shape, KE, E, nm, nparts, SlabComm(nparts), dtype, aux, **kw), nm
+
+
+def _split(H, v):
+    return {i: v[3 * L.a * L.P:3 * L.a * L.P + L.n].contiguous() for i, L in H._level(0)}
+
+
+def _join(H, parts):
+    return torch.cat([parts[i][:L.n_own] for i, L in H._level(0)])
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 3])
+def test_slab_operator_matches_the_single_grid(nparts):
+    shape = (48, 12, 20)
+    E, mask, _ = _problem(shape, 1, interior_fixed=True)
+    H, nm = _hier(shape, E, mask, nparts, max_coarse_x=12)
+    u = torch.randn(3 * vo.n_nodes(shape), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    y = vx.VoxelOperator(shape, KE).matvec(u, E, nm)
+    us = _split(H, u)
+    ys = {i: torch.empty_like(us[i]) for i in us}
+    H.apply64(0, us, ys)
+    got = _join(H, ys)
+    assert float((got - y).abs().max() / y.abs().max()) <= 1e-12
+    for i, L in H._level(0):
+        if L.has_hi:                                   # both holders of a shared plane agree exactly
+            assert torch.equal(ys[i][L.n - 3 * L.P:], ys[i + 1][:3 * L.P])
+
+
+@pytest.mark.parametrize("dtype,aux,tol", [(torch.float64, None, 1e-11), (torch.float32, None, 2e-5),
+                                           (torch.float32, torch.bfloat16, 3e-2), (torch.bfloat16, None, 3e-2)])
+def test_slab_vcycle_matches_the_single_grid(dtype, aux, tol):
+    shape = (128, 64, 64)
+    E, mask, force = _problem(shape)
+    nm = vx.node_mask_from_dofs(mask)
+    M = vs.MGHierarchy(shape, KE, E, nm, dtype, pre=2, post=2, omegas=0.6, aux_dtype=aux)
+    ref = M(force)
+    H = SlabHierarchy(shape, KE, E, nm, 4, SlabComm(4), dtype, aux, pre=2, post=2, omegas=0.6)
+    zs = H.emit(_split(H, force))
+    got = _join(H, {i: z.double() for i, z in zs.items()})
+    d = float(torch.linalg.vector_norm(got - ref) / torch.linalg.vector_norm(ref))
+    print(f"slab V-cycle ({dtype}, aux {aux}) vs single grid: {d:.2e}")
+    assert d <= tol
+    for i, L in H._level(0):
+        if L.has_hi:
+            assert torch.equal(zs[i][L.n - 3 * L.P:], zs[i + 1][:3 * L.P])
+
+
+def test_slab_spectral_omegas_match_the_single_grid():
+    shape = (128, 64, 64)
+    E, mask, _ = _problem(shape)
+    nm = vx.node_mask_from_dofs(mask)
+    M = vs.MGHierarchy(shape, KE, E, nm, torch.float32, omegas="spectral")
+    H = SlabHierarchy(shape, KE, E, nm, 3, SlabComm(3), torch.float32, omegas="spectral")
+    assert np.allclose(H.lambdas, M.lambdas, rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize("precision,nparts,extra", [("mixed", 4, 0), ("fp64", 2, 0), ("bf16", 3, 1),
+                                                    ("mixed", 1, 0)])
+def test_slab_config2_solve(precision, nparts, extra):
+    c = golden("config2.json")
+    shape = (128, 64, 64)
+    E, mask, force = _problem(shape)
+    s = SlabSolver(shape, E, mask, nparts, precision=precision, pre=2, post=2, omega=0.6, check_every=1)
+    res = s.solve(force)
+    x = s.gather()
+    comp = float(force @ x)
+    print(f"slab {precision} x{nparts}: {res.iterations} iterations, rel {res.rel:.3e}, compliance {comp!r}")
+    assert res.converged and res.rel <= 1e-8
+    assert res.iterations <= c["fp32"]["iterations"] + extra
+    assert abs(comp - c["fp64"]["compliance"]) <= 1e-7 * c["fp64"]["compliance"]
+    assert torch.all(x[mask == 0] == 0)
+
+
+def test_slab_solve_with_fixed_nodes_on_shared_planes():
+    shape = (64, 32, 32)
+    E, mask, force = _problem(shape, 2, interior_fixed=True)
+    one = ElasticitySolver(shape, E, mask, precision="mixed", tol=1e-10, maxiter=300)
+    r1 = one.solve(force)
+    x1 = r1.x.clone()
+    s = SlabSolver(shape, E, mask, 3, precision="mixed", tol=1e-10, maxiter=300)
+    r3 = s.solve(force)
+    x3 = s.gather()
+    print(f"fixed interior nodes: single grid {r1.iterations}, 3 slabs {r3.iterations} iterations")
+    assert r1.converged and r3.converged and abs(r1.iterations - r3.iterations) <= 1
+    assert float((x3 - x1).abs().max() / x1.abs().max()) <= 1e-8
+    assert torch.all(x3[mask == 0] == 0)
+
+
+def test_slab_warm_start_returns_at_once():
+    shape = (64, 32, 32)
+    E, mask, force = _problem(shape, 4)
+    s = SlabSolver(shape, E, mask, 2, precision="mixed")
+    r = s.solve(force)
+    x = s.gather()
+    r2 = s.solve(force, x0=x)
+    assert r.converged and r2.converged and r2.iterations == 0
