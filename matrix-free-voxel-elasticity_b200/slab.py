@@ -24,7 +24,6 @@ FP64 inverse Cholesky factor of the global coarsest matrix (replicated, as it is
 """
 from __future__ import annotations
 
-import ctypes
 
 import numpy as np
 import torch
@@ -33,7 +32,7 @@ import torch.distributed as dist
 from . import _lib
 from .element import quadrature
 from .operators import PREC, STORAGE, VoxelOperator, node_mask_from_dofs
-from .solver import (FIN_BETA_PR, FIN_NB, FIN_PQ, FIN_TRUE, S_BREAK, S_DONE, S_IT, S_MV, S_REL, S_TOL,
+from .solver import (FIN_BETA_PR, FIN_NB, FIN_PQ, FIN_RZ, FIN_TRUE, S_BREAK, S_DONE, S_IT, S_MV, S_REL, S_TOL,
                      SolveResult, _lower_inverse, hierarchy_shapes)
 
 PLANE_APPLY, PLANE_JACOBI, PLANE_RESIDUAL, PLANE_TRUE_RES = range(4)
@@ -175,7 +174,7 @@ class _SlabLevel:
         self.halo64 = self.halo if _ARITH[dtype] == torch.float64 else _Halo(3 * self.P, torch.float64,
                                                                            self.has_lo, self.has_hi)
         self.rhalo = None          # restricted right-hand side planes (auxiliary storage), coarse levels
-        self.E64 = self.E = self.mask = self.invd = None
+        self.E64 = self.E = self.mask = self.invd = self.invd64 = None
         self.r = self.x = self.xt = self.res = None
         self.omega = 0.0
 
@@ -302,6 +301,7 @@ class SlabHierarchy:
                 free = ((L.mask.to(torch.int32)[:, None] >> torch.arange(3, device="cuda")) & 1).reshape(-1).bool()
                 inv64 = torch.where(free, 1.0 / d, torch.ones_like(d))
                 L.invd = inv64 if self.aux_dtype == torch.float64 else inv64.to(self.aux_dtype)
+                L.invd64 = inv64                       # the spectral estimate runs in FP64
 
     def _coarse_setup(self):
         """The global coarsest grid's moduli and mask (gathered), its dense constrained matrix and the
@@ -343,7 +343,7 @@ class SlabHierarchy:
                 m = ((L.mask.to(torch.int32)[:, None] >> torch.arange(3, device="cuda")) & 1).reshape(-1).double()
                 ms[i] = m
                 vs[i] = torch.as_tensor(v0[lo:lo + L.n], device="cuda") * m
-                invs[i] = L.invd.to(torch.float64)
+                invs[i] = L.invd64
                 ws[i] = torch.empty(L.n, dtype=torch.float64, device="cuda")
             nrm = self._norm(l, vs)
             for i in vs:
@@ -563,7 +563,7 @@ class SlabSolver:
     def _direction(self, z, first):
         S = self.S.data_ptr()
         if first:
-            self._dots("r", lambda i: z[i], fin=5)                                   # FIN_RZ
+            self._dots("r", lambda i: z[i], zprec=self.zprec, fin=FIN_RZ)
         else:
             self._dots("r", lambda i: z[i], zo="z_old", zprec=self.zprec, fin=FIN_BETA_PR, count=2)
         for i, L in self._levels():

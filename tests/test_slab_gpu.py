@@ -76,9 +76,8 @@ def test_plane_fix_modes(prec):
         if mode == 3 and prec != _lib.VX_F64:
             continue
         out = torch.zeros(n3, dtype=it, device="cuda")
-        _lib.call("vx_plane_fix", prec, mode, nodes, t(lo, it).data_ptr(), t(hi, it).data_ptr(),
-                  t(bits, torch.uint8).data_ptr(), t(x, it).data_ptr(), t(r, aux).data_ptr(), t(d, aux).data_ptr(),
-                  0.6, 0.5, out.data_ptr(), _s())
+        held = [t(lo, it), t(hi, it), t(bits, torch.uint8), t(x, it), t(r, aux), t(d, aux)]   # alive during the call
+        _lib.call("vx_plane_fix", prec, mode, nodes, *[h.data_ptr() for h in held[:6]], 0.6, 0.5, out.data_ptr(), _s())
         assert np.max(np.abs(out.double().cpu().numpy() - ref)) <= tol * np.max(np.abs(ref)) * 4
 
 
