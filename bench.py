@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--host-loop", action="store_true",
                     help="launch the CG loop body from the host instead of the WHILE graph (the same kernels; "
                          "a profiler then lists every launch)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="x-slab decomposition of the workload's grid: under torchrun one slab per rank "
+                         "(exchange over NCCL), else this many slabs on one GPU (exchange by device copies)")
     ap.add_argument("--kernels", action="store_true",
                     help="only launch the hot kernels on the workload's data (for an ncu capture); prints their times")
     return ap.parse_args()
@@ -349,6 +352,59 @@ def run_b200(args, rank, world, local_rank):
         out["matvec_sweep"] = matvec_sweep(flush)
     if rank == 0 and world == 1 and not args.profile and args.workload != "gmg_576x288x288":
         out["cpu_baseline"] = cpu_baseline(args.workload)
+    return out
+
+
+def run_slab_bench(args, rank, world, local_rank):
+    """The workload's mixed GMG-PCG solve on an x-slab decomposition of its grid (strong scaling:
+    the global problem is fixed).  Under torchrun slab i is rank i's and shared planes travel over
+    NCCL; in one process `--slabs K` slabs share the GPU and exchange by device copies, which
+    measures the decomposition's own cost (layer contributions, plane fixes, owned-prefix dots,
+    the host-driven loop) against the single-grid solver."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    from voxel_b200 import _lib
+    from voxel_b200.api import ElasticitySolver
+    from voxel_b200.slab import SlabSolver
+
+    def rank_sync():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    nparts = world if world > 1 else args.slabs
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    shape, levels, rho, E, mask, force = build_inputs(args.workload)
+    del rho
+    kw = dict(tol=1e-8, maxiter=200, check_every=CHECK_EVERY, pre=2, post=2, omega=0.6, levels=levels)
+    s = SlabSolver(shape, E, mask, nparts, precision="mixed", **kw)
+    with ClockSampler(local_rank) as clocks:
+        launches0 = _lib.launches
+        times, res = time_solves(s, force, args.steps, args.warmup, flush, rank_sync)
+        launches = _lib.launches - launches0
+    t_max = max_over_ranks(float(np.mean(times)), world, "cuda")
+    x = s.gather()
+    out = {"metric": "time-to-1e-8 solve, mixed-precision GMG-PCG on an x-slab decomposition", "value": t_max,
+           "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * 1e3,
+           "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+           "dtype": "f64 outer / f32 preconditioner", "data": "synthetic",
+           "config": {"workload": args.workload, "description": WORKLOADS[args.workload][3], "slabs": nparts,
+                      "bounds": s.M.bounds, "check_every": CHECK_EVERY,
+                      "parallelism": f"x-slab x{nparts} over NCCL" if world > 1 else f"x-slab x{nparts} on one GPU",
+                      "l2": "flushed (256 MB write) between timed steps"},
+           "solve": {"iterations": res.iterations, "converged": res.converged, "rel_residual": res.rel,
+                     "compliance": float(force @ x), "step_s": times},
+           "gpu_launches": int(launches // (args.steps + args.warmup) * args.steps), "clocks": clocks.summary()}
+    if world == 1:
+        del s
+        torch.cuda.empty_cache()
+        for graph in (True, False):
+            one = ElasticitySolver(shape, E, mask, precision="mixed", graph=graph, **kw)
+            t1, r1 = time_solves(one, force, args.steps, args.warmup, flush, rank_sync)
+            out["single_grid_graph" if graph else "single_grid_host_loop"] = {
+                "value": float(np.mean(t1)), "iterations": r1.iterations, "compliance": float(force @ r1.x)}
+            del one
     return out
 
 
@@ -637,7 +693,7 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    out = run_b200(args, rank, world, local)
+    out = run_slab_bench(args, rank, world, local) if args.slabs else run_b200(args, rank, world, local)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
