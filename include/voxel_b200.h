@@ -333,13 +333,18 @@ int vx_graph_destroy(void* handle);
  *   mode 2  out = scale * (free ? r - A x : 0)        (auxiliary; vx_residual's output; scale 1/2
  *                                                      splits a shared plane before restriction)
  *   mode 3  out = r - A x                             (VX_F64 only; vx_true_residual's output)
+ * With `dot` (modes 0 and 3; NULL otherwise), dot[cta] (vx_plane_fix_partials(nodes) doubles)
+ * corrects the per-CTA sums that vx_apply_dot (x . out) or vx_true_residual (out^2) wrote for the
+ * slab: the plane's slab-local terms are subtracted and, when `owned` is non-zero, its rewritten
+ * terms added, so summing both kernels' partials over all slabs counts each shared DOF once.
  * vx_plane_sum: out = lo + hi (n values of the selector's auxiliary storage): the restricted
  * right-hand side on a shared coarse plane. */
 int vx_layer_partial(int prec, int ny, int nz, const double* ke, const void* E, const void* u,
                      const uint8_t* node_mask, int side, void* out, cudaStream_t stream);
+int64_t vx_plane_fix_partials(int64_t nodes);
 int vx_plane_fix(int prec, int mode, int64_t nodes, const void* lo, const void* hi, const uint8_t* node_mask,
                  const void* x, const void* r, const void* inv_diag, double omega, double scale, void* out,
-                 cudaStream_t stream);
+                 double* dot, int owned, cudaStream_t stream);
 int vx_plane_sum(int prec, int64_t n, const void* lo, const void* hi, void* out, cudaStream_t stream);
 
 #ifdef __cplusplus

@@ -81,7 +81,8 @@ SIGNATURES = {
     "vx_oc_apply": (c_int, [c_int64, _P, _P, _P, c_double, _P, _P, _P]),
     # x-slab decomposition
     "vx_layer_partial": (c_int, [c_int, c_int, c_int, _D, _P, _P, _P, c_int, _P, _P]),
-    "vx_plane_fix": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P, _P, c_double, c_double, _P, _P]),
+    "vx_plane_fix": (c_int, [c_int, c_int, c_int64, _P, _P, _P, _P, _P, _P, c_double, c_double, _P, _P, c_int, _P]),
+    "vx_plane_fix_partials": (c_int64, [c_int64]),
     "vx_plane_sum": (c_int, [c_int, c_int64, _P, _P, _P, _P]),
 }
 
@@ -129,7 +130,7 @@ KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noal
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",
-             "vx_oc_partials", "vx_graph_body_nodes"}
+             "vx_oc_partials", "vx_graph_body_nodes", "vx_plane_fix_partials"}
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 

@@ -58,36 +58,68 @@ __global__ void __launch_bounds__(128) layer_partial_kernel(int ny, int nz, cons
 
 enum PlaneMode { PLANE_APPLY = 0, PLANE_JACOBI = 1, PLANE_RESIDUAL = 2, PLANE_TRUE_RES = 3 };
 
+constexpr int PT = 256;   // threads per plane-fix CTA
+
 // One shared node plane (P nodes, 3 P DOFs) rewritten from s = lo + hi, with A x = s on free DOFs
 // and x on fixed ones -- the epilogues of the fused operator kernels:
 //   APPLY     out = A x                                   (TY = arithmetic type)
 //   JACOBI    out = x + omega invd (r - A x)              (TY = iterate storage)
 //   RESIDUAL  out = scale * (free ? r - A x : 0)          (TY = auxiliary storage)
 //   TRUE_RES  out = r - A x                               (TY = iterate storage, FP64 outer loop)
+// With `dot` (APPLY and TRUE_RES), dot[cta] corrects the fused kernel's per-CTA sums of x.out
+// (APPLY) or out^2 (TRUE_RES), which counted this plane with its slab-local values: minus the old
+// terms, plus the rewritten ones when this slab owns the plane (`owned`), so every shared DOF is
+// counted once over all slabs.
 template <typename X, typename R, typename TY, int MODE>
-__global__ void plane_fix_kernel(int64_t n3, const arith_t<X>* __restrict__ lo, const arith_t<X>* __restrict__ hi,
-                                 const uint8_t* __restrict__ node_mask, const X* __restrict__ x,
-                                 const R* __restrict__ r, const R* __restrict__ invd, double omega, double scale,
-                                 TY* __restrict__ out) {
+__global__ void __launch_bounds__(PT) plane_fix_kernel(int64_t n3, const arith_t<X>* __restrict__ lo,
+                                                       const arith_t<X>* __restrict__ hi,
+                                                       const uint8_t* __restrict__ node_mask, const X* __restrict__ x,
+                                                       const R* __restrict__ r, const R* __restrict__ invd,
+                                                       double omega, double scale, TY* __restrict__ out,
+                                                       double* __restrict__ dot, int owned) {
     vx::pdl_begin();
     using A = arith_t<X>;
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n3) return;
-    const unsigned bits = node_mask ? unsigned(node_mask[i / 3]) : 7u;
-    const bool fr = (bits >> (i % 3)) & 1u;
-    const A xr = A(Storage<X>::load(x + i));
-    const A ax = fr ? A(lo[i] + hi[i]) : xr;
-    A o;
-    if constexpr (MODE == PLANE_APPLY) {
-        o = ax;
-    } else if constexpr (MODE == PLANE_JACOBI) {
-        o = xr + A(omega) * A(Storage<R>::load(invd + i)) * (A(Storage<R>::load(r + i)) - ax);
-    } else if constexpr (MODE == PLANE_RESIDUAL) {
-        o = fr ? A(scale) * (A(Storage<R>::load(r + i)) - ax) : A(0);
-    } else {
-        o = A(Storage<R>::load(r + i)) - ax;
+    double corr = 0.0;
+    if (i < n3) {
+        const unsigned bits = node_mask ? unsigned(node_mask[i / 3]) : 7u;
+        const bool fr = (bits >> (i % 3)) & 1u;
+        const A xr = A(Storage<X>::load(x + i));
+        const A ax = fr ? A(lo[i] + hi[i]) : xr;
+        A o;
+        if constexpr (MODE == PLANE_APPLY) {
+            o = ax;
+        } else if constexpr (MODE == PLANE_JACOBI) {
+            o = xr + A(omega) * A(Storage<R>::load(invd + i)) * (A(Storage<R>::load(r + i)) - ax);
+        } else if constexpr (MODE == PLANE_RESIDUAL) {
+            o = fr ? A(scale) * (A(Storage<R>::load(r + i)) - ax) : A(0);
+        } else {
+            o = A(Storage<R>::load(r + i)) - ax;
+        }
+        if constexpr (MODE == PLANE_APPLY || MODE == PLANE_TRUE_RES) {
+            if (dot) {
+                const double old = double(Storage<TY>::load(out + i));
+                const double w = MODE == PLANE_APPLY ? double(xr) : double(o);
+                const double wo = MODE == PLANE_APPLY ? double(xr) : old;
+                corr = (owned ? w * double(o) : 0.0) - wo * old;
+            }
+        }
+        Storage<TY>::store(out + i, o);
     }
-    Storage<TY>::store(out + i, o);
+    if constexpr (MODE == PLANE_APPLY || MODE == PLANE_TRUE_RES) {
+        if (dot) {                                          // uniform across the CTA
+            __shared__ double red[PT / 32];
+            #pragma unroll
+            for (int o = 16; o > 0; o >>= 1) corr += __shfl_down_sync(0xffffffffu, corr, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = corr;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (int w = 0; w < PT / 32; ++w) t += red[w];
+                dot[blockIdx.x] = t;
+            }
+        }
+    }
 }
 
 // out = lo + hi in storage S (the restricted coarse right-hand side on a shared plane)
@@ -125,9 +157,11 @@ extern "C" int vx_layer_partial(int prec, int ny, int nz, const double* ke, cons
     return VX_OK;
 }
 
+extern "C" int64_t vx_plane_fix_partials(int64_t nodes) { return (3 * nodes + PT - 1) / PT; }
+
 extern "C" int vx_plane_fix(int prec, int mode, int64_t nodes, const void* lo, const void* hi,
                             const uint8_t* node_mask, const void* x, const void* r, const void* invd, double omega,
-                            double scale, void* out, cudaStream_t stream) {
+                            double scale, void* out, double* dot, int owned, cudaStream_t stream) {
     VX_CHECK_ARG(nodes > 0 && nodes < (int64_t(1) << 29), VX_ERR_INVALID_ARGUMENT, "vx_plane_fix: bad plane size");
     VX_CHECK_ARG(mode >= PLANE_APPLY && mode <= PLANE_TRUE_RES, VX_ERR_INVALID_ARGUMENT, "vx_plane_fix: bad mode %d", mode);
     VX_CHECK_ARG(lo && hi && x && out, VX_ERR_NULL_POINTER, "vx_plane_fix: NULL pointer");
@@ -135,8 +169,10 @@ extern "C" int vx_plane_fix(int prec, int mode, int64_t nodes, const void* lo, c
     VX_CHECK_ARG(mode != PLANE_JACOBI || invd, VX_ERR_NULL_POINTER, "vx_plane_fix: invd is required");
     VX_CHECK_ARG(mode != PLANE_TRUE_RES || prec == VX_F64, VX_ERR_INVALID_ARGUMENT,
                  "vx_plane_fix: the true residual is FP64 only");
+    VX_CHECK_ARG(!dot || mode == PLANE_APPLY || mode == PLANE_TRUE_RES, VX_ERR_INVALID_ARGUMENT,
+                 "vx_plane_fix: dot corrections exist for modes 0 and 3 only");
     const int64_t n3 = 3 * nodes;
-    const unsigned grid = unsigned((n3 + 255) / 256);
+    const unsigned grid = unsigned((n3 + PT - 1) / PT);
     const bool ok = dispatch_prec(prec, [&](auto t) {
         using X = typename decltype(t)::X;
         using R = typename decltype(t)::R;
@@ -145,20 +181,20 @@ extern "C" int vx_plane_fix(int prec, int mode, int64_t nodes, const void* lo, c
         const A* h = (const A*)hi;
         switch (mode) {
             case PLANE_APPLY:
-                vx::launch(plane_fix_kernel<X, R, A, PLANE_APPLY>, grid, 256, 0, stream, n3, l, h, node_mask,
-                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (A*)out);
+                vx::launch(plane_fix_kernel<X, R, A, PLANE_APPLY>, grid, PT, 0, stream, n3, l, h, node_mask,
+                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (A*)out, dot, owned);
                 break;
             case PLANE_JACOBI:
-                vx::launch(plane_fix_kernel<X, R, X, PLANE_JACOBI>, grid, 256, 0, stream, n3, l, h, node_mask,
-                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (X*)out);
+                vx::launch(plane_fix_kernel<X, R, X, PLANE_JACOBI>, grid, PT, 0, stream, n3, l, h, node_mask,
+                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (X*)out, dot, owned);
                 break;
             case PLANE_RESIDUAL:
-                vx::launch(plane_fix_kernel<X, R, R, PLANE_RESIDUAL>, grid, 256, 0, stream, n3, l, h, node_mask,
-                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (R*)out);
+                vx::launch(plane_fix_kernel<X, R, R, PLANE_RESIDUAL>, grid, PT, 0, stream, n3, l, h, node_mask,
+                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (R*)out, dot, owned);
                 break;
             default:
-                vx::launch(plane_fix_kernel<X, R, X, PLANE_TRUE_RES>, grid, 256, 0, stream, n3, l, h, node_mask,
-                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (X*)out);
+                vx::launch(plane_fix_kernel<X, R, X, PLANE_TRUE_RES>, grid, PT, 0, stream, n3, l, h, node_mask,
+                           (const X*)x, (const R*)r, (const R*)invd, omega, scale, (X*)out, dot, owned);
         }
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_plane_fix: unknown precision %d", prec);

@@ -32,8 +32,8 @@ import torch.distributed as dist
 from . import _lib
 from .element import quadrature
 from .operators import PREC, STORAGE, VoxelOperator, node_mask_from_dofs
-from .solver import (FIN_BETA_PR, FIN_NB, FIN_PQ, FIN_RZ, FIN_TRUE, S_BREAK, S_DONE, S_IT, S_MV, S_REL, S_TOL,
-                     SolveResult, _lower_inverse, hierarchy_shapes)
+from .solver import (FIN_BETA_PR, FIN_NB, FIN_PQ, FIN_RZ, FIN_TRUE, S_BREAK, S_CHECK, S_DONE, S_IT, S_MAXIT,
+                     S_MV, S_REL, S_TOL, SolveResult, _GraphLoop, _lower_inverse, hierarchy_shapes)
 
 PLANE_APPLY, PLANE_JACOBI, PLANE_RESIDUAL, PLANE_TRUE_RES = range(4)
 _ARITH = {torch.float64: torch.float64, torch.float32: torch.float32, torch.bfloat16: torch.float32}
@@ -190,19 +190,23 @@ class _SlabLevel:
             _lib.call("vx_layer_partial", prec, ny, nz, self.kp, _at(E, (nlx - 1) * ny * nz), _at(u, 3 * (nlx - 1) * P),
                       _at(self.mask, (nlx - 1) * P), 1, halo.own_hi.data_ptr(), _s())
 
-    def fix(self, prec, mode, halo, x, out, r=None, invd=None, omega=0.0, scale=1.0):
-        """Rewrite the shared planes of `out` from the two contributions (lower slab first)."""
+    def fix(self, prec, mode, halo, x, out, r=None, invd=None, omega=0.0, scale=1.0, dot=None, dot_at=0):
+        """Rewrite the shared planes of `out` from the two contributions (lower slab first).  With
+        `dot` (modes 0 and 3) the per-CTA corrections of the fused kernel's dot partials go to
+        dot[dot_at:] (lower plane, owned by this slab) and dot[dot_at + G:] (upper plane, owned by
+        the upper neighbour), G = vx_plane_fix_partials(P)."""
         nlx = self.shape[0]
         P = self.P
+        G = int(_lib.load().vx_plane_fix_partials(P))
         if self.has_lo:
             _lib.call("vx_plane_fix", prec, mode, P, halo.recv_lo.data_ptr(), halo.own_lo.data_ptr(),
                       _at(self.mask, 0), _at(x, 0), _at(r, 0), _at(invd, 0), float(omega), float(scale),
-                      _at(out, 0), _s())
+                      _at(out, 0), _at(dot, dot_at), 1, _s())
         if self.has_hi:
             o = 3 * nlx * P
             _lib.call("vx_plane_fix", prec, mode, P, halo.own_hi.data_ptr(), halo.recv_hi.data_ptr(),
                       _at(self.mask, nlx * P), _at(x, o), _at(r, o), _at(invd, o), float(omega), float(scale),
-                      _at(out, o), _s())
+                      _at(out, o), _at(dot, dot_at + G), 0, _s())
 
 
 class SlabHierarchy:
@@ -485,7 +489,7 @@ class SlabSolver:
     holds slab `rank` and exchanges with its neighbours over the process group."""
 
     def __init__(self, shape, E, mask, nparts, ke=None, precision="mixed", pre=2, post=2, omega=0.6,
-                 max_coarse_x=16, levels=None, tol=1e-8, maxiter=200, check_every=1, local=None):
+                 max_coarse_x=16, levels=None, tol=1e-8, maxiter=200, check_every=1, local=None, graph=True):
         from .api import _MG_STORAGE, _dev
         if precision not in _MG_STORAGE:
             raise ValueError(f"precision must be one of {tuple(_MG_STORAGE)} for the slab solver")
@@ -513,24 +517,31 @@ class SlabSolver:
                                p=torch.zeros(n, **f64), q=torch.zeros(n, **f64),
                                z_old=torch.zeros(n, dtype=dt, device="cuda"),
                                part=torch.zeros(2 * int(_lib.load().vx_solver_partials(L.n_own)), **f64),
-                               opp=torch.zeros(L.op64.partials_size, **f64),
+                               # fused-kernel partials, then the two shared planes' corrections (zero when absent)
+                               opp=torch.zeros(L.op64.partials_size + 2 * int(_lib.load().vx_plane_fix_partials(L.P)),
+                                               **f64),
                                sums=torch.zeros(2, **f64))
         self.S = torch.zeros(16, **f64)
         self.S_host = torch.zeros(16, dtype=torch.float64, pin_memory=True)
+        self.stream = torch.cuda.Stream()
+        self.use_graph = bool(graph) and not self.comm.distributed
+        self._graph = None
 
     # -------------------------------------------------------------- distributed pieces
     def _levels(self):
         return self.M._level(0)
 
-    def _reduce(self, fin, count, fill):
-        """fill(i, L, partials) writes each slab's dot partials over its owned prefix; the slab sums
+    def _reduce(self, fin, count, fill=None, buf="part"):
+        """fill(i, L, partials) writes each slab's dot partials over its owned prefix (or, with
+        buf="opp", a fused operator kernel and its plane corrections already did); the slab sums
         are reduced, summed over slabs and handed to vx_solver_finalize(fin)."""
         sums = []
         for i, L in self._levels():
             v = self.vec[i]
-            fill(i, L, v["part"].data_ptr())
-            G = int(_lib.load().vx_solver_partials(L.n_own))
-            _lib.call("vx_reduce_partials", G, count, v["part"].data_ptr(), v["sums"].data_ptr(), _s())
+            if fill is not None:
+                fill(i, L, v[buf].data_ptr())
+            G = int(_lib.load().vx_solver_partials(L.n_own)) if buf == "part" else v["opp"].numel()
+            _lib.call("vx_reduce_partials", G, count, v[buf].data_ptr(), v["sums"].data_ptr(), _s())
             sums.append(v["sums"][:count])
         acc = self.comm.allreduce_(sums)
         _lib.call("vx_solver_finalize", fin, 1, acc.data_ptr(), self.S.data_ptr(), _s())
@@ -540,22 +551,26 @@ class SlabSolver:
             "vx_dots_pr", _lib.VX_F64, zprec, L.n_own, self.vec[i][a].data_ptr(), b(i).data_ptr(),
             None if zo is None else self.vec[i][zo].data_ptr(), pp, _s()))
 
-    def _apply(self, src, dst):
-        M = self.M
-        M._op(0, lambda i, L: L.partials(_lib.VX_F64, self.vec[i][src], L.halo64, L.E64),
-              {i: L.halo64 for i, L in self._levels()},
-              lambda i, L: L.op64.matvec(self.vec[i][src], L.E64, L.mask, out=self.vec[i][dst]),
-              lambda i, L: L.fix(_lib.VX_F64, PLANE_APPLY, L.halo64, self.vec[i][src], self.vec[i][dst]))
+    def _apply_dot(self):
+        """q = A p and p.q: the fused apply-dot on each slab, its shared planes rewritten with their
+        dot terms corrected, the partials summed over slabs (FIN_PQ)."""
+        v = self.vec
+        self.M._op(0, lambda i, L: L.partials(_lib.VX_F64, v[i]["p"], L.halo64, L.E64),
+                   {i: L.halo64 for i, L in self._levels()},
+                   lambda i, L: L.op64.apply_dot(v[i]["p"], L.E64, L.mask, v[i]["q"], v[i]["opp"]),
+                   lambda i, L: L.fix(_lib.VX_F64, PLANE_APPLY, L.halo64, v[i]["p"], v[i]["q"], dot=v[i]["opp"],
+                                      dot_at=L.op64.partials_size))
+        self._reduce(FIN_PQ, 1, buf="opp")
 
     def _true_residual(self, out="r"):
-        M = self.M
-        M._op(0, lambda i, L: L.partials(_lib.VX_F64, self.vec[i]["x"], L.halo64, L.E64),
-              {i: L.halo64 for i, L in self._levels()},
-              lambda i, L: L.op64.true_residual(self.vec[i]["x"], self.vec[i]["b"], L.E64, L.mask, self.vec[i][out],
-                                                self.vec[i]["opp"]),
-              lambda i, L: L.fix(_lib.VX_F64, PLANE_TRUE_RES, L.halo64, self.vec[i]["x"], self.vec[i][out],
-                                 self.vec[i]["b"]))
-        self._dots(out, lambda i: self.vec[i][out], fin=FIN_TRUE)
+        """out = b - A x and |b - A x|^2 (FIN_TRUE), fused the same way."""
+        v = self.vec
+        self.M._op(0, lambda i, L: L.partials(_lib.VX_F64, v[i]["x"], L.halo64, L.E64),
+                   {i: L.halo64 for i, L in self._levels()},
+                   lambda i, L: L.op64.true_residual(v[i]["x"], v[i]["b"], L.E64, L.mask, v[i][out], v[i]["opp"]),
+                   lambda i, L: L.fix(_lib.VX_F64, PLANE_TRUE_RES, L.halo64, v[i]["x"], v[i][out], v[i]["b"],
+                                      dot=v[i]["opp"], dot_at=L.op64.partials_size))
+        self._reduce(FIN_TRUE, 1, buf="opp")
 
     def _precondition(self):
         return self.M.emit({i: self.vec[i]["r"] for i, _ in self._levels()})
@@ -575,8 +590,7 @@ class SlabSolver:
 
     def _iteration(self, check):
         S = self.S.data_ptr()
-        self._apply("p", "q")
-        self._dots("p", lambda i: self.vec[i]["q"], fin=FIN_PQ)
+        self._apply_dot()
         for i, L in self._levels():
             v = self.vec[i]
             _lib.call("vx_cg_update", _lib.VX_F64, L.n, S, v["x"].data_ptr(), v["p"].data_ptr(), v["r"].data_ptr(),
@@ -590,9 +604,31 @@ class SlabSolver:
         torch.cuda.current_stream().synchronize()
         return self.S_host.numpy().copy()
 
+    def _body(self, k):
+        for j in range(k):
+            self._iteration(j == k - 1)
+
     def solve(self, f, x0=None):
         """f (and x0): GLOBAL vectors (3N) or {slab index: local slice}.  Returns SolveResult whose x
-        is {slab index: local solution} (gather() assembles the global vector)."""
+        is {slab index: local solution} (gather() assembles the global vector).
+
+        With every slab in this process the loop runs as one CUDA-graph WHILE launch (bodies of
+        check_every iterations, as FCGSolver); across processes it is driven from the host, one
+        iteration at a time, reading the scalars at every check."""
+        k = self.check_every
+        full = self.maxiter // k
+        use_graph = self.use_graph and full > 0
+        caller = torch.cuda.current_stream()
+        st = self.stream
+        st.wait_stream(caller)
+        if use_graph and self._graph is None:
+            self._graph = _GraphLoop(st, self.S, lambda: self._body(k))
+        with torch.cuda.stream(st):
+            s = self._solve(f, x0, k, full, use_graph)
+        caller.wait_stream(st)
+        return self._result(s)
+
+    def _solve(self, f, x0, k, full, use_graph):
         S = self.S.data_ptr()
         for i, L in self._levels():
             v = self.vec[i]
@@ -604,6 +640,8 @@ class SlabSolver:
                 v["x"].copy_(x0[i] if isinstance(x0, dict) else x0[lo:lo + L.n])
         _lib.call("vx_set_scalars", S, 0, 16, 0.0, _s())
         _lib.call("vx_set_scalars", S, S_TOL, 1, self.tol, _s())
+        _lib.call("vx_set_scalars", S, S_MAXIT, 1, float(self.maxiter), _s())
+        _lib.call("vx_set_scalars", S, S_CHECK, 1, float(k), _s())
         self._dots("b", lambda i: self.vec[i]["b"], fin=FIN_NB)
         if x0 is None:
             for i, _ in self._levels():
@@ -611,21 +649,24 @@ class SlabSolver:
         else:
             self._true_residual()
         self._direction(self._precondition(), first=True)
-        it, s = 0, self._read()
+        s = self._read()
         if x0 is not None and s[S_DONE]:
-            return self._result(s)
-        while it < self.maxiter:
-            check = (it + 1) % self.check_every == 0
+            return s
+        if use_graph:
+            self._graph.launch(self.stream)
+            s = self._read()
+            self._graph.account(max(1, -(-int(s[S_IT]) // k)))
+        it = int(s[S_IT])
+        while not s[S_DONE] and not s[S_BREAK] and it < self.maxiter:
+            check = (it + 1) % k == 0
             self._iteration(check)
             it += 1
             if check or it == self.maxiter:
                 s = self._read()
-                if s[S_DONE] or s[S_BREAK]:
-                    break
         if not s[S_DONE]:
             self._true_residual("q")
             s = self._read()
-        return self._result(s)
+        return s
 
     def _result(self, s):
         rel = float(s[S_REL])

@@ -75,10 +75,21 @@ def test_plane_fix_modes(prec):
     for mode, ref in want.items():
         if mode == 3 and prec != _lib.VX_F64:
             continue
-        out = torch.zeros(n3, dtype=it, device="cuda")
+        out = t(rng.standard_normal(n3), it)
+        old = out.double().cpu().numpy()                   # as stored
         held = [t(lo, it), t(hi, it), t(bits, torch.uint8), t(x, it), t(r, aux), t(d, aux)]   # alive during the call
-        _lib.call("vx_plane_fix", prec, mode, nodes, *[h.data_ptr() for h in held[:6]], 0.6, 0.5, out.data_ptr(), _s())
-        assert np.max(np.abs(out.double().cpu().numpy() - ref)) <= tol * np.max(np.abs(ref)) * 4
+        with_dot = mode in (0, 3)
+        G = int(_lib.load().vx_plane_fix_partials(nodes))
+        dot = torch.zeros(G, dtype=torch.float64, device="cuda") if with_dot else None
+        _lib.call("vx_plane_fix", prec, mode, nodes, *[h.data_ptr() for h in held[:6]], 0.6, 0.5, out.data_ptr(),
+                  None if dot is None else dot.data_ptr(), 1, _s())
+        got = out.double().cpu().numpy()
+        assert np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref)) * 4
+        if with_dot:                 # owned plane: new terms in, the slab-local (old) terms out
+            xs = held[3].double().cpu().numpy()
+            w_new, w_old = (xs, xs) if mode == 0 else (got, old)
+            want_corr = float(np.sum(w_new * got) - np.sum(w_old * old))
+            assert abs(float(dot.sum()) - want_corr) <= 1e-10 * (np.sum(np.abs(w_new * got)) + np.sum(np.abs(w_old * old)))
 
 
 def _problem(shape, seed=0, interior_fixed=False):
@@ -189,3 +200,19 @@ def test_slab_warm_start_returns_at_once():
     x = s.gather()
     r2 = s.solve(force, x0=x)
     assert r.converged and r2.converged and r2.iterations == 0
+
+
+@pytest.mark.parametrize("check_every", [1, 5])
+def test_slab_graph_loop_matches_the_host_loop(check_every):
+    """The WHILE-graph loop (every slab in one process) and the host-driven loop (the path of one
+    slab per process) run the same kernels: identical iterations and bitwise-equal solutions."""
+    shape = (128, 64, 64)
+    E, mask, force = _problem(shape)
+    out = []
+    for graph in (True, False):
+        s = SlabSolver(shape, E, mask, 3, precision="mixed", check_every=check_every, graph=graph)
+        r = s.solve(force)
+        out.append((r.iterations, r.rel, s.gather().clone()))
+        r2 = s.solve(force)                                # a second solve reuses the captured graph
+        assert r2.iterations == r.iterations and torch.equal(s.gather(), out[-1][2])
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1] and torch.equal(out[0][2], out[1][2])
