@@ -242,6 +242,15 @@ int vx_true_residual(int prec, int nx, int ny, int nz, const double* blocks, con
                      const uint8_t* node_mask, const void* x, const void* b, void* res, double* partials,
                      cudaStream_t stream);
 int vx_reduce_partials(int64_t G, int count, const double* partials, double* out, cudaStream_t stream);
+/* The same two forms with the partial sums restricted to node planes x_lo <= ix < x_hi (0 <= x_lo
+ * <= x_hi <= nx + 1); the output vector is written everywhere.  An x-slab (below) leaves its
+ * shared planes out and adds them after they are rewritten (vx_plane_fix with `dot`). */
+int vx_apply_dot_planes(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                        const uint8_t* node_mask, const void* p, void* q, double* partials, int x_lo, int x_hi,
+                        cudaStream_t stream);
+int vx_true_residual_planes(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                            const uint8_t* node_mask, const void* x, const void* b, void* res, double* partials,
+                            int x_lo, int x_hi, cudaStream_t stream);
 
 /* res = b - A x and *norm2 = sum res^2 (a device double), like vx_true_residual followed by
  * vx_reduce_partials, but needing no scratch buffer from the caller: for code that may not
@@ -333,10 +342,10 @@ int vx_graph_destroy(void* handle);
  *   mode 2  out = scale * (free ? r - A x : 0)        (auxiliary; vx_residual's output; scale 1/2
  *                                                      splits a shared plane before restriction)
  *   mode 3  out = r - A x                             (VX_F64 only; vx_true_residual's output)
- * With `dot` (modes 0 and 3; NULL otherwise), dot[cta] (vx_plane_fix_partials(nodes) doubles)
- * corrects the per-CTA sums that vx_apply_dot (x . out) or vx_true_residual (out^2) wrote for the
- * slab: the plane's slab-local terms are subtracted and, when `owned` is non-zero, its rewritten
- * terms added, so summing both kernels' partials over all slabs counts each shared DOF once.
+ * With `dot` (modes 0 and 3; NULL otherwise), dot[cta] (vx_plane_fix_partials(nodes) doubles) =
+ * the CTA's sum of x . out (mode 0) or out^2 (mode 3) over the rewritten plane if `owned` is
+ * non-zero, else 0.  With vx_apply_dot_planes / vx_true_residual_planes leaving the slab's shared
+ * planes out of their sums, the two kernels' partials summed over all slabs count each DOF once.
  * vx_plane_sum: out = lo + hi (n values of the selector's auxiliary storage): the restricted
  * right-hand side on a shared coarse plane. */
 int vx_layer_partial(int prec, int ny, int nz, const double* ke, const void* E, const void* u,

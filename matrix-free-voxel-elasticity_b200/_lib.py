@@ -49,6 +49,8 @@ SIGNATURES = {
     "vx_partials_size": (c_int64, [c_int64]),
     "vx_dots": (c_int, [c_int, c_int64, c_int, POINTER(c_void_p), POINTER(c_void_p), _P, _P, _P]),
     "vx_reduce_partials": (c_int, [c_int64, c_int, _P, _P, _P]),
+    "vx_apply_dot_planes": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, c_int, c_int, _P]),
+    "vx_true_residual_planes": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, c_int, c_int, _P]),
     "vx_true_residual_noalloc": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
     "vx_axpby": (c_int, [c_int, c_int64, c_double, _P, c_double, _P, _P]),
     "vx_cast": (c_int, [c_int64, c_int, _P, c_int, _P, c_double, _P]),

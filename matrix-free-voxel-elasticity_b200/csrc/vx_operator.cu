@@ -17,6 +17,7 @@
 // dense_gather: the reference's node-owned dense 24x24 mapping (independent control path).
 // diag / energy / coarse-grid helpers.
 #include "vx_common.cuh"
+#include <climits>
 #include "vx_pair.cuh"
 
 #include <algorithm>
@@ -47,6 +48,7 @@ struct OpArgs {
     const TR* invd;           // JACOBI inverse diagonal
     TC omega;
     double* partials;         // TRUE_RES (|res|^2) / APPLY_DOT (p.q): one double per CTA
+    int dot_x0, dot_x1;       // node planes [dot_x0, dot_x1) enter the partial sums
     double emin, de, penal;   // SIMP modulus E = emin + de * rho^penal
     int cx;                   // owned node planes per CTA (x chunk)
     bool cubic;               // host side: the blocks have the cube pattern (CubeK)
@@ -275,14 +277,14 @@ parity_stream(const __grid_constant__ OpArgs<TC, TU, TE, TY> a) {
                         o = ax;
                     } else if constexpr (EPI == EPI_APPLY_DOT) {
                         o = ax;
-                        acc += double(uprev_raw[c]) * double(ax);
+                        if (ix - 1 >= a.dot_x0 && ix - 1 < a.dot_x1) acc += double(uprev_raw[c]) * double(ax);
                     } else if constexpr (EPI == EPI_JACOBI) {
                         o = uprev_raw[c] + a.omega * dd[c] * (rr[c] - ax);
                     } else if constexpr (EPI == EPI_RESIDUAL) {
                         o = free_dof ? rr[c] - ax : TC(0);
                     } else {  // EPI_TRUE_RES
                         o = rr[c] - ax;
-                        acc += double(o) * double(o);
+                        if (ix - 1 >= a.dot_x0 && ix - 1 < a.dot_x1) acc += double(o) * double(o);
                     }
                     Storage<TY>::store(yo + (REV ? 2 - c : c), o);
                 }
@@ -666,7 +668,7 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
                             o = ax;
                         } else if constexpr (EPI == EPI_APPLY_DOT) {
                             o = ax;
-                            acc += double(xr) * double(ax);
+                            if (ixo >= a.dot_x0 && ixo < a.dot_x1) acc += double(xr) * double(ax);
                         } else if constexpr (EPI == EPI_JACOBI) {
                             const TC r_ = h == 0 ? rr0[k] : rr1[k], d_ = h == 0 ? dd0[k] : dd1[k];
                             o = xr + a.omega * d_ * (r_ - ax);
@@ -676,7 +678,7 @@ parity_stream_xp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
                         } else {
                             const TC r_ = h == 0 ? rr0[k] : rr1[k];
                             o = r_ - ax;
-                            acc += double(o) * double(o);
+                            if (ixo >= a.dot_x0 && ixo < a.dot_x1) acc += double(o) * double(o);
                         }
                         Storage<TY>::store(yo + k, o);
                     }
@@ -1053,7 +1055,7 @@ namespace {
 template <int EPI>
 int fused_dispatch(const char* what, int prec, int nx, int ny, int nz, const double* blocks, const void* E,
                    const uint8_t* node_mask, const void* x, const void* r, const void* invd, double omega,
-                   void* out, double* partials, cudaStream_t stream) {
+                   void* out, double* partials, cudaStream_t stream, int dot_x0 = 0, int dot_x1 = INT_MAX) {
     int st = check_grid(nx, ny, nz);
     if (st) return st;
     VX_CHECK_ARG(blocks && E && x && out, VX_ERR_NULL_POINTER, "%s: NULL pointer", what);
@@ -1077,9 +1079,9 @@ int fused_dispatch(const char* what, int prec, int nx, int ny, int nz, const dou
             a.g = Grid{nx, ny, nz};
             a.u = (const X*)x; a.E = (const M*)E; a.y = (TY*)out; a.node_mask = node_mask;
             a.r = (const R*)r; a.invd = (const R*)invd; a.omega = TC(omega); a.partials = partials;
+            a.dot_x0 = dot_x0; a.dot_x1 = dot_x1;
             a.C = convert_blocks<TC>(blocks);
             a.cubic = cube_pattern(blocks);
-        a.cubic = cube_pattern(blocks);
             rc = node_mask ? launch_stream<TC, X, M, TY, EPI, MASK_NODE, false, false, R>(a, stream, what)
                            : launch_stream<TC, X, M, TY, EPI, MASK_NONE, false, false, R>(a, stream, what);
         }
@@ -1124,6 +1126,28 @@ extern "C" int vx_true_residual(int prec, int nx, int ny, int nz, const double* 
     VX_CHECK_ARG(b && partials, VX_ERR_NULL_POINTER, "vx_true_residual: NULL b / partials");
     return fused_dispatch<EPI_TRUE_RES>("vx_true_residual", prec, nx, ny, nz, blocks, E, node_mask, x, b,
                                         nullptr, 0.0, res, partials, stream);
+}
+
+// The reducing forms with the sums restricted to node planes x_lo <= ix < x_hi (the output is
+// written everywhere): an x-slab leaves its shared planes out and adds them once they are final.
+extern "C" int vx_apply_dot_planes(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                                   const uint8_t* node_mask, const void* p, void* q, double* partials, int x_lo,
+                                   int x_hi, cudaStream_t stream) {
+    VX_CHECK_ARG(partials, VX_ERR_NULL_POINTER, "vx_apply_dot_planes: NULL partials");
+    VX_CHECK_ARG(0 <= x_lo && x_lo <= x_hi && x_hi <= nx + 1, VX_ERR_INVALID_ARGUMENT,
+                 "vx_apply_dot_planes: bad plane range [%d, %d)", x_lo, x_hi);
+    return fused_dispatch<EPI_APPLY_DOT>("vx_apply_dot_planes", prec, nx, ny, nz, blocks, E, node_mask, p, nullptr,
+                                         nullptr, 0.0, q, partials, stream, x_lo, x_hi);
+}
+
+extern "C" int vx_true_residual_planes(int prec, int nx, int ny, int nz, const double* blocks, const void* E,
+                                       const uint8_t* node_mask, const void* x, const void* b, void* res,
+                                       double* partials, int x_lo, int x_hi, cudaStream_t stream) {
+    VX_CHECK_ARG(b && partials, VX_ERR_NULL_POINTER, "vx_true_residual_planes: NULL b / partials");
+    VX_CHECK_ARG(0 <= x_lo && x_lo <= x_hi && x_hi <= nx + 1, VX_ERR_INVALID_ARGUMENT,
+                 "vx_true_residual_planes: bad plane range [%d, %d)", x_lo, x_hi);
+    return fused_dispatch<EPI_TRUE_RES>("vx_true_residual_planes", prec, nx, ny, nz, blocks, E, node_mask, x, b,
+                                        nullptr, 0.0, res, partials, stream, x_lo, x_hi);
 }
 
 // ----------------------------------------------------------------------------- allocation-free form

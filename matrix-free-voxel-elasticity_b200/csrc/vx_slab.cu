@@ -66,10 +66,11 @@ constexpr int PT = 256;   // threads per plane-fix CTA
 //   JACOBI    out = x + omega invd (r - A x)              (TY = iterate storage)
 //   RESIDUAL  out = scale * (free ? r - A x : 0)          (TY = auxiliary storage)
 //   TRUE_RES  out = r - A x                               (TY = iterate storage, FP64 outer loop)
-// With `dot` (APPLY and TRUE_RES), dot[cta] corrects the fused kernel's per-CTA sums of x.out
-// (APPLY) or out^2 (TRUE_RES), which counted this plane with its slab-local values: minus the old
-// terms, plus the rewritten ones when this slab owns the plane (`owned`), so every shared DOF is
-// counted once over all slabs.
+// With `dot` (APPLY and TRUE_RES), dot[cta] = this CTA's sum of x.out (APPLY) or out^2 (TRUE_RES)
+// over the rewritten plane when this slab owns it (`owned`), else 0: the slab's fused kernel left
+// its shared planes out of its sums (vx_apply_dot_planes / vx_true_residual_planes), so every
+// shared DOF is counted once over all slabs.  (Subtracting the slab-local terms instead would
+// cancel: near convergence they are far larger than the true residual.)
 template <typename X, typename R, typename TY, int MODE>
 __global__ void __launch_bounds__(PT) plane_fix_kernel(int64_t n3, const arith_t<X>* __restrict__ lo,
                                                        const arith_t<X>* __restrict__ hi,
@@ -97,12 +98,7 @@ __global__ void __launch_bounds__(PT) plane_fix_kernel(int64_t n3, const arith_t
             o = A(Storage<R>::load(r + i)) - ax;
         }
         if constexpr (MODE == PLANE_APPLY || MODE == PLANE_TRUE_RES) {
-            if (dot) {
-                const double old = double(Storage<TY>::load(out + i));
-                const double w = MODE == PLANE_APPLY ? double(xr) : double(o);
-                const double wo = MODE == PLANE_APPLY ? double(xr) : old;
-                corr = (owned ? w * double(o) : 0.0) - wo * old;
-            }
+            if (dot && owned) corr = (MODE == PLANE_APPLY ? double(xr) : double(o)) * double(o);
         }
         Storage<TY>::store(out + i, o);
     }

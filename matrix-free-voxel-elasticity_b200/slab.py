@@ -166,6 +166,9 @@ class _SlabLevel:
         self.n = 3 * (nlx + 1) * self.P
         self.has_lo, self.has_hi = index > 0, index < nparts - 1
         self.n_own = 3 * (nlx + (0 if self.has_hi else 1)) * self.P
+        # node planes that are not shared: the fused reductions' range (shared planes are added
+        # by the plane fix, by their owner)
+        self.interior = (1 if self.has_lo else 0, nlx if self.has_hi else nlx + 1)
         self.ke = np.ascontiguousarray(ke)
         self.kp = _lib.dptr(self.ke)
         self.op = VoxelOperator(self.shape, self.ke, dtype, aux)
@@ -192,9 +195,9 @@ class _SlabLevel:
 
     def fix(self, prec, mode, halo, x, out, r=None, invd=None, omega=0.0, scale=1.0, dot=None, dot_at=0):
         """Rewrite the shared planes of `out` from the two contributions (lower slab first).  With
-        `dot` (modes 0 and 3) the per-CTA corrections of the fused kernel's dot partials go to
-        dot[dot_at:] (lower plane, owned by this slab) and dot[dot_at + G:] (upper plane, owned by
-        the upper neighbour), G = vx_plane_fix_partials(P)."""
+        `dot` (modes 0 and 3) the rewritten planes' dot terms go to dot[dot_at:] (the lower plane,
+        owned by this slab) and dot[dot_at + G:] (the upper plane, owned by the upper neighbour:
+        zeros), G = vx_plane_fix_partials(P)."""
         nlx = self.shape[0]
         P = self.P
         G = int(_lib.load().vx_plane_fix_partials(P))
@@ -557,7 +560,9 @@ class SlabSolver:
         v = self.vec
         self.M._op(0, lambda i, L: L.partials(_lib.VX_F64, v[i]["p"], L.halo64, L.E64),
                    {i: L.halo64 for i, L in self._levels()},
-                   lambda i, L: L.op64.apply_dot(v[i]["p"], L.E64, L.mask, v[i]["q"], v[i]["opp"]),
+                   lambda i, L: _lib.call("vx_apply_dot_planes", _lib.VX_F64, *L.shape, L.op64._bp, L.E64.data_ptr(),
+                                          L.mask.data_ptr(), v[i]["p"].data_ptr(), v[i]["q"].data_ptr(),
+                                          v[i]["opp"].data_ptr(), *L.interior, _s()),
                    lambda i, L: L.fix(_lib.VX_F64, PLANE_APPLY, L.halo64, v[i]["p"], v[i]["q"], dot=v[i]["opp"],
                                       dot_at=L.op64.partials_size))
         self._reduce(FIN_PQ, 1, buf="opp")
@@ -567,7 +572,10 @@ class SlabSolver:
         v = self.vec
         self.M._op(0, lambda i, L: L.partials(_lib.VX_F64, v[i]["x"], L.halo64, L.E64),
                    {i: L.halo64 for i, L in self._levels()},
-                   lambda i, L: L.op64.true_residual(v[i]["x"], v[i]["b"], L.E64, L.mask, v[i][out], v[i]["opp"]),
+                   lambda i, L: _lib.call("vx_true_residual_planes", _lib.VX_F64, *L.shape, L.op64._bp,
+                                          L.E64.data_ptr(), L.mask.data_ptr(), v[i]["x"].data_ptr(),
+                                          v[i]["b"].data_ptr(), v[i][out].data_ptr(), v[i]["opp"].data_ptr(),
+                                          *L.interior, _s()),
                    lambda i, L: L.fix(_lib.VX_F64, PLANE_TRUE_RES, L.halo64, v[i]["x"], v[i][out], v[i]["b"],
                                       dot=v[i]["opp"], dot_at=L.op64.partials_size))
         self._reduce(FIN_TRUE, 1, buf="opp")

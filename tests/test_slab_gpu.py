@@ -76,7 +76,6 @@ def test_plane_fix_modes(prec):
         if mode == 3 and prec != _lib.VX_F64:
             continue
         out = t(rng.standard_normal(n3), it)
-        old = out.double().cpu().numpy()                   # as stored
         held = [t(lo, it), t(hi, it), t(bits, torch.uint8), t(x, it), t(r, aux), t(d, aux)]   # alive during the call
         with_dot = mode in (0, 3)
         G = int(_lib.load().vx_plane_fix_partials(nodes))
@@ -85,11 +84,9 @@ def test_plane_fix_modes(prec):
                   None if dot is None else dot.data_ptr(), 1, _s())
         got = out.double().cpu().numpy()
         assert np.max(np.abs(got - ref)) <= tol * np.max(np.abs(ref)) * 4
-        if with_dot:                 # owned plane: new terms in, the slab-local (old) terms out
-            xs = held[3].double().cpu().numpy()
-            w_new, w_old = (xs, xs) if mode == 0 else (got, old)
-            want_corr = float(np.sum(w_new * got) - np.sum(w_old * old))
-            assert abs(float(dot.sum()) - want_corr) <= 1e-10 * (np.sum(np.abs(w_new * got)) + np.sum(np.abs(w_old * old)))
+        if with_dot:                 # owned plane: its rewritten terms x.out or out^2
+            w = held[3].double().cpu().numpy() if mode == 0 else got
+            assert abs(float(dot.sum()) - float(np.sum(w * got))) <= 1e-12 * np.sum(np.abs(w * got))
 
 
 def _problem(shape, seed=0, interior_fixed=False):
@@ -216,3 +213,32 @@ def test_slab_graph_loop_matches_the_host_loop(check_every):
         r2 = s.solve(force)                                # a second solve reuses the captured graph
         assert r2.iterations == r.iterations and torch.equal(s.gather(), out[-1][2])
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1] and torch.equal(out[0][2], out[1][2])
+
+
+@pytest.mark.parametrize("lo,hi", [(0, 33), (1, 32), (1, 33), (5, 6), (0, 0)])
+def test_reductions_over_a_node_plane_range(lo, hi):
+    """vx_apply_dot_planes / vx_true_residual_planes: the output as vx_apply_dot / vx_true_residual,
+    the partial sums over node planes lo <= ix < hi only."""
+    shape = (32, 16, 24)
+    E, mask, force = _problem(shape, 3)
+    nm = vx.node_mask_from_dofs(mask)
+    op = vx.VoxelOperator(shape, KE)
+    g = torch.Generator("cuda").manual_seed(4)
+    p = torch.randn(op.ndof, dtype=torch.float64, device="cuda", generator=g)
+    P3 = 3 * 17 * 25
+    G = op.partials_size
+    part = torch.zeros(G, dtype=torch.float64, device="cuda")
+    q = torch.empty_like(p)
+    _lib.call("vx_apply_dot_planes", _lib.VX_F64, *shape, op._bp, E.data_ptr(), nm.data_ptr(), p.data_ptr(),
+              q.data_ptr(), part.data_ptr(), lo, hi, _s())
+    q_ref = op.matvec(p, E, nm)
+    assert torch.equal(q, q_ref)
+    want = float(p[lo * P3:hi * P3] @ q_ref[lo * P3:hi * P3])
+    assert abs(float(part.sum()) - want) <= 1e-12 * float((p * q_ref).abs().sum())
+    res = torch.empty_like(p)
+    _lib.call("vx_true_residual_planes", _lib.VX_F64, *shape, op._bp, E.data_ptr(), nm.data_ptr(), p.data_ptr(),
+              force.data_ptr(), res.data_ptr(), part.data_ptr(), lo, hi, _s())
+    r_ref = force - q_ref
+    assert float((res - r_ref).abs().max()) <= 1e-13 * float(r_ref.abs().max())
+    want = float(r_ref[lo * P3:hi * P3] @ r_ref[lo * P3:hi * P3])
+    assert abs(float(part.sum()) - want) <= 1e-12 * float((r_ref * r_ref).sum()) + 1e-300
