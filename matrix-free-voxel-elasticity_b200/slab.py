@@ -72,7 +72,9 @@ class SlabComm:
 
     `local` lists the slab indices held by this process.  Slabs held by one process exchange by
     device copies; otherwise slab i lives on rank i of the default process group (one slab per
-    process) and neighbours exchange with send/recv (NCCL on GPUs, gloo on CPU tensors)."""
+    process) and neighbours exchange with send/recv: NCCL moves device buffers directly; with a
+    gloo group, device buffers are staged through host memory (each exchange then completes on the
+    host before the next launch)."""
 
     def __init__(self, nparts: int, local=None):
         self.nparts = int(nparts)
@@ -81,6 +83,7 @@ class SlabComm:
             local = [dist.get_rank()] if distributed else list(range(self.nparts))
         self.local = [int(i) for i in local]
         self.distributed = distributed
+        self.staged = distributed and dist.get_backend() != "nccl"
         if distributed:
             if dist.get_world_size() != self.nparts or self.local != [dist.get_rank()]:
                 raise ValueError("across processes, slab i must be the only slab of rank i "
@@ -104,8 +107,22 @@ class SlabComm:
                 else:
                     ops += [dist.P2POp(dist.isend, h.own_hi, i + 1), dist.P2POp(dist.irecv, h.recv_hi, i + 1)]
         if ops:
+            back = []
+            if self.staged:                     # host copies of device buffers for gloo
+                staged = []
+                for op in ops:
+                    t = op.tensor
+                    if t.is_cuda:
+                        h = t.cpu() if op.op is dist.isend else torch.empty(t.shape, dtype=t.dtype)
+                        if op.op is not dist.isend:
+                            back.append((t, h))
+                        t = h
+                    staged.append(dist.P2POp(op.op, t, op.peer))
+                ops = staged
             for w in dist.batch_isend_irecv(ops):
                 w.wait()
+            for t, h in back:
+                t.copy_(h)
 
     def allreduce_(self, tensors):
         """Sum the per-slab tensors (same shape) over all slabs, in slab order within a process;
@@ -114,7 +131,12 @@ class SlabComm:
         for t in tensors[1:]:
             acc.add_(t)
         if self.distributed:
-            dist.all_reduce(acc)
+            if self.staged and acc.is_cuda:
+                h = acc.cpu()
+                dist.all_reduce(h)
+                acc.copy_(h)
+            else:
+                dist.all_reduce(acc)
         for t in tensors[1:]:
             t.copy_(acc)
         return acc
@@ -128,6 +150,8 @@ class SlabComm:
                 off += t.numel()
             return out
         piece = pieces[0]
+        if self.staged:
+            piece = piece.cpu()
         sizes = torch.tensor([piece.numel()], dtype=torch.int64, device=piece.device)
         all_sizes = [torch.zeros_like(sizes) for _ in range(self.nparts)]
         dist.all_gather(all_sizes, sizes)
