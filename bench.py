@@ -378,7 +378,7 @@ def run_slab_bench(args, rank, world, local_rank):
     shape, levels, rho, E, mask, force = build_inputs(args.workload)
     del rho
     kw = dict(tol=1e-8, maxiter=200, check_every=CHECK_EVERY, pre=2, post=2, omega=0.6, levels=levels)
-    s = SlabSolver(shape, E, mask, nparts, precision="mixed", **kw)
+    s = SlabSolver(shape, E, mask, nparts, precision="mixed", graph=not args.host_loop, **kw)
     with ClockSampler(local_rank) as clocks:
         launches0 = _lib.launches
         times, res = time_solves(s, force, args.steps, args.warmup, flush, rank_sync)

@@ -242,7 +242,7 @@ class SlabHierarchy:
     the exchanges they need."""
 
     def __init__(self, shape, ke, E, node_mask, nparts, comm: SlabComm, dtype=torch.float32, aux_dtype=None,
-                 pre=2, post=2, omegas=None, max_coarse_x=16, shapes=None):
+                 pre=2, post=2, omegas=None, max_coarse_x=16, shapes=None, spectral_seed=20260923):
         aux_dtype = dtype if aux_dtype is None else aux_dtype
         if (dtype, aux_dtype) not in STORAGE:
             raise ValueError(f"unsupported V-cycle storage: iterate {dtype}, auxiliary {aux_dtype}")
@@ -289,7 +289,7 @@ class SlabHierarchy:
             om = [0.6] * n_smooth
             self.lambdas = None
         elif isinstance(omegas, str) and omegas == "spectral":
-            om, self.lambdas = self.spectral_omegas()
+            om, self.lambdas = self.spectral_omegas(seed=spectral_seed)
         elif np.isscalar(omegas):
             om, self.lambdas = [float(omegas)] * n_smooth, None
         else:
@@ -516,7 +516,8 @@ class SlabSolver:
     holds slab `rank` and exchanges with its neighbours over the process group."""
 
     def __init__(self, shape, E, mask, nparts, ke=None, precision="mixed", pre=2, post=2, omega=0.6,
-                 max_coarse_x=16, levels=None, tol=1e-8, maxiter=200, check_every=1, local=None, graph=True):
+                 max_coarse_x=16, levels=None, tol=1e-8, maxiter=200, check_every=1, local=None, graph=True,
+                 spectral_seed=20260923):
         from .api import _MG_STORAGE, _dev
         if precision not in _MG_STORAGE:
             raise ValueError(f"precision must be one of {tuple(_MG_STORAGE)} for the slab solver")
@@ -533,7 +534,7 @@ class SlabSolver:
             shapes = shapes[:levels]
         dt, aux = _MG_STORAGE[precision]
         self.M = SlabHierarchy(self.shape, self.ke, Eg, nm, nparts, self.comm, dt, aux, pre, post, omega,
-                               shapes=shapes)
+                               shapes=shapes, spectral_seed=spectral_seed)
         self.tol, self.maxiter, self.check_every = float(tol), int(maxiter), max(1, int(check_every))
         self.zprec = PREC[dt]
         f64 = dict(dtype=torch.float64, device="cuda")

@@ -293,3 +293,41 @@ def test_slab_solve_across_processes(world):
         assert it == c["fp32"]["iterations"] and rel <= 1e-8 and fixed_zero
         assert abs(comp - c["fp64"]["compliance"]) <= 1e-7 * c["fp64"]["compliance"]
     assert len({(g[4], g[5], g[6], g[8]) for g in got}) == 1        # every rank holds the same result
+
+
+def _slab_kat(case, nparts, precision="mixed"):
+    """The reference's published known answer (experiments/session_i, V(4,4), spectral omega from
+    the FP64 hierarchy) solved on x-slabs."""
+    k = golden("kat_inputs.npz")
+    kat = golden("kat_session_i.json")
+    base = "q64" if case.startswith("q64") else "q96"
+    rho_nat, shape = vx.problems.upsample_natural(k[f"{base}_rho"], tuple(int(s) for s in k[f"{base}_shape"]),
+                                                  int(case[-1]))
+    mask_nat, force_nat = vx.problems.cantilever_line_load(shape)
+    floor = kat["_protocol"]["material"]["Emin"]
+    cu = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")          # noqa: E731
+    E = cu(vx.to_author(floor + (1 - floor) * rho_nat ** 3, shape))
+    mask = cu(vx.to_author(mask_nat, shape, True))
+    force = cu(vx.to_author(force_nat, shape, True))
+    mgp = kat["_protocol"]["multigrid"]
+    s = SlabSolver(shape, E, mask, nparts, ke=k[f"{base}_ke"], precision=precision, pre=mgp["pre"], post=mgp["post"],
+                   omega="spectral", max_coarse_x=mgp["max_coarse_x"], tol=1e-8, maxiter=200, check_every=1,
+                   spectral_seed=kat["_protocol"]["order_seed"])
+    assert [list(s_) for s_ in s.M.shapes] == kat[case]["shapes"]
+    res = s.solve(force)
+    x = s.gather()
+    return res, float(force @ x), float(torch.linalg.vector_norm(x)), kat[case]["observations"]
+
+
+@pytest.mark.parametrize("case,nparts", [("q64x2", 3), ("q96x3", 4)])
+def test_slab_reference_published_kat(case, nparts):
+    """q64x2 (256x128x128, 14 iterations, 807.19637074) on 3 slabs and the headline q96x3
+    (576x288x288, 144.6M DOF, 20 iterations, 543.42238043-543.42238050) on 4 slabs: the published
+    iteration counts, compliances and solution norms (1e-9 relative)."""
+    res, comp, norm, obs = _slab_kat(case, nparts)
+    print(f"slab {case} x{nparts}: {res.iterations} iterations (published {obs[0]['iterations']}), compliance {comp!r}")
+    assert res.converged and res.iterations == obs[0]["iterations"]
+    ref_c = np.array([o["compliance"] for o in obs])
+    assert np.min(np.abs(comp - ref_c)) <= 1e-9 * ref_c.mean()
+    ref_n = np.array([o["solution_norm"] for o in obs])
+    assert np.min(np.abs(norm - ref_n)) <= 1e-9 * ref_n.mean()
