@@ -136,13 +136,18 @@ HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 
+_FNS = {}             # name -> bound entry point (getattr on a CDLL is not free)
+
+
 def call(name: str, *args) -> None:
     global launches
-    lib = load()
-    check(getattr(lib, name)(*args), name)
+    fn = _FNS.get(name)
+    if fn is None:
+        fn = _FNS[name] = getattr(load(), name)
+    check(fn(*args), name)
     if name not in HOST_ONLY:
         launches += KERNELS_PER_CALL.get(name, 1)
-    if CAPTURE_STREAM is not None and lib.vx_capture_status(CAPTURE_STREAM) == 2:
+    if CAPTURE_STREAM is not None and _lib.vx_capture_status(CAPTURE_STREAM) == 2:
         raise RuntimeError(f"{name} invalidated the stream capture")
 
 

@@ -25,7 +25,16 @@ STORAGE = {(torch.float64, torch.float64): _lib.VX_F64, (torch.float32, torch.fl
            (torch.bfloat16, torch.bfloat16): _lib.VX_BF16_F32, (torch.float32, torch.bfloat16): _lib.VX_F32_BF16AUX}
 
 
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_CUR_DEVICE = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def stream_ptr(device=None) -> int:
+    """cudaStream_t of the current stream (of the current device when `device` is None).  The
+    host-driven loops ask for it once per launch, so on the current device it is read with torch's
+    raw-stream accessor, without building a Stream object and resolving the device index."""
+    if device is None and _RAW_STREAM is not None and _CUR_DEVICE is not None and torch.cuda.is_initialized():
+        return _RAW_STREAM(_CUR_DEVICE())
     return torch.cuda.current_stream(device).cuda_stream
 
 

@@ -24,14 +24,13 @@ FP64 inverse Cholesky factor of the global coarsest matrix (replicated, as it is
 """
 from __future__ import annotations
 
-
 import numpy as np
 import torch
 import torch.distributed as dist
 
 from . import _lib
 from .element import quadrature
-from .operators import PREC, STORAGE, VoxelOperator, node_mask_from_dofs
+from .operators import PREC, STORAGE, VoxelOperator, node_mask_from_dofs, stream_ptr
 from .solver import (FIN_BETA_PR, FIN_NB, FIN_PQ, FIN_RZ, FIN_TRUE, S_BREAK, S_CHECK, S_DONE, S_IT, S_MAXIT,
                      S_MV, S_REL, S_TOL, SolveResult, _GraphLoop, _lower_inverse, hierarchy_shapes)
 
@@ -63,7 +62,7 @@ def _at(t, offset):
 
 
 def _s():
-    return torch.cuda.current_stream().cuda_stream
+    return stream_ptr()
 
 
 # ---------------------------------------------------------------------------------------- comm
@@ -193,6 +192,7 @@ class _SlabLevel:
         # node planes that are not shared: the fused reductions' range (shared planes are added
         # by the plane fix, by their owner)
         self.interior = (1 if self.has_lo else 0, nlx if self.has_hi else nlx + 1)
+        self.G_fix = int(_lib.load().vx_plane_fix_partials(self.P))
         self.ke = np.ascontiguousarray(ke)
         self.kp = _lib.dptr(self.ke)
         self.op = VoxelOperator(self.shape, self.ke, dtype, aux)
@@ -224,7 +224,7 @@ class _SlabLevel:
         zeros), G = vx_plane_fix_partials(P)."""
         nlx = self.shape[0]
         P = self.P
-        G = int(_lib.load().vx_plane_fix_partials(P))
+        G = self.G_fix
         if self.has_lo:
             _lib.call("vx_plane_fix", prec, mode, P, halo.recv_lo.data_ptr(), halo.own_lo.data_ptr(),
                       _at(self.mask, 0), _at(x, 0), _at(r, 0), _at(invd, 0), float(omega), float(scale),

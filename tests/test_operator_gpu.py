@@ -240,3 +240,15 @@ def test_invalid_arguments_raise():
         op.matvec(torch.ones(375, dtype=torch.float32, device="cuda"), E)
     with pytest.raises(ValueError):
         vx.VoxelOperator((0, 4, 4), KE)
+
+
+def test_stream_pointer_follows_the_current_stream():
+    """operators.stream_ptr (read once per launch by the host-driven loops) is the raw handle of
+    torch's current stream, on the default stream and inside a stream context."""
+    from voxel_b200.operators import stream_ptr
+    assert stream_ptr() == torch.cuda.current_stream().cuda_stream
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        assert stream_ptr() == s.cuda_stream == torch.cuda.current_stream().cuda_stream
+    assert stream_ptr() == torch.cuda.current_stream().cuda_stream
+    assert stream_ptr(torch.cuda.current_device()) == torch.cuda.current_stream().cuda_stream
