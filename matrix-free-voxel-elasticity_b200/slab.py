@@ -203,6 +203,7 @@ class _SlabLevel:
         self.rhalo = None          # restricted right-hand side planes (auxiliary storage), coarse levels
         self.E64 = self.E = self.mask = self.invd = self.invd64 = None
         self.r = self.x = self.xt = self.res = None
+        self._res_buf = None       # the buffer the V-cycle's residual went to (read by the restriction)
         self.omega = 0.0
 
     # -- the per-slab halves of an operator form
@@ -256,7 +257,7 @@ class SlabHierarchy:
         nl = len(self.shapes)
         self.bounds = slab_bounds(self.shapes[0][0], self.nparts, nl)
         self.side = torch.cuda.Stream()
-        gx, ny, nz = self.shapes[0]
+        _, ny, nz = self.shapes[0]
         P0 = (ny + 1) * (nz + 1)
         self.parts = {}
         for i in comm.local:
@@ -266,8 +267,9 @@ class SlabHierarchy:
                 f = 1 << l
                 L = _SlabLevel(i, self.nparts, (b // f - a // f, s[1], s[2]), a // f, self.ke * f, dtype, aux_dtype)
                 if l == 0:
-                    L.E64 = E[a * ny * nz:b * ny * nz].to(torch.float64).contiguous()
-                    L.mask = node_mask[a * P0:(b + 1) * P0].contiguous()
+                    # owned copies: a caller rewriting its global arrays does not change the solver
+                    L.E64 = E[a * ny * nz:b * ny * nz].to(torch.float64).clone()
+                    L.mask = node_mask[a * P0:(b + 1) * P0].clone()
                 else:
                     prev = levels[-1]
                     L.E64 = torch.empty(L.shape[0] * L.shape[1] * L.shape[2], dtype=torch.float64, device="cuda")
