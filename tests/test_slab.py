@@ -221,3 +221,12 @@ def test_comm_across_gloo_processes(world):
         assert recv_hi == (None if r == world - 1 else [r + 1 + 0.25] * 9)
         assert s == total
         assert out == want
+
+
+def test_slab_solver_rejects_bad_arguments_before_device_work():
+    """Unknown precisions and slab-to-process mappings fail with ValueError on the host."""
+    from voxel_b200.slab import SlabSolver
+    with pytest.raises(ValueError, match="precision"):
+        SlabSolver((32, 16, 16), None, None, 2, precision="jacobi")
+    with pytest.raises(ValueError):
+        SlabComm(2, local=[1])
