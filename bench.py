@@ -596,24 +596,28 @@ def run_simp_bench(args):
     t0 = time.perf_counter()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
-    x, rho, hist = simp.run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=steps, penal=3.0,
-                                 precision="mixed", solve_tol=1e-6, noise=0.01, seed=0, levels=levels)
-    ev1.record()
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
+    with ClockSampler(0) as clocks:
+        x, rho, hist = simp.run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=steps, penal=3.0,
+                                     precision="mixed", solve_tol=1e-6, noise=0.01, seed=0, levels=levels,
+                                     check_every=CHECK_EVERY)
+        ev1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
     per_step = [h_["seconds"] for h_ in hist]
     return {"metric": "SIMP iteration time (solve + autograd sensitivity + filter + OC bisection), 192x96x96",
             "value": float(np.mean(per_step[1:])), "unit": "s", "n_gpus": 1, "steps": steps, "warmup": 1,
             "ms_per_step": 1e3 * float(np.mean(per_step[1:])), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner", "data": "synthetic",
             "config": {"workload": "simp_192x96x96", "description": desc,
-                       "timing": "per-step wall time with a device synchronize per step; step 0 (graph capture) excluded"},
+                       "timing": "per-step wall time with a device synchronize per step; step 0 (graph capture) excluded",
+                       "check_every": CHECK_EVERY},
             "simp": {"total_s_incl_setup": wall, "device_s": ev0.elapsed_time(ev1) / 1e3,
                      "median_step_s": float(np.median(per_step[1:])),
                      "compliance_first_last": [hist[0]["compliance"], hist[-1]["compliance"]],
                      "volume_last": hist[-1]["volume"], "change_last": hist[-1]["change"],
                      "solve_iterations_mean": float(np.mean([h_["iterations"] for h_ in hist])),
                      "oc_probes_mean": float(np.mean([h_["oc_probes"] for h_ in hist]))},
+            "clocks": clocks.summary(),
             "fd_check": {"elements": 64, "step": h, "solve_tol": 1e-12, "max_rel_err": float(relerr.max()),
                          "median_rel_err": float(np.median(relerr)), "seconds": t_fd}}
 

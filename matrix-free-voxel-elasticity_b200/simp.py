@@ -194,11 +194,12 @@ def compliance(rho, state):
 
 def run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=100, emin=1e-9, penal=3.0,
              precision="mixed", solve_tol=1e-6, noise=0.01, seed=0, levels=None, pre=2, post=2, omega="spectral",
-             omega_every=10, omega_iterations=10, callback=None):
+             omega_every=10, omega_iterations=10, callback=None, check_every=1):
     """Density-filtered SIMP on the equal-split cantilever (run_w1b.simp_run, update='top88_gpu'):
     x starts at volfrac plus seeded uniform noise; each step solves (mixed GMG-PCG warm-started at
     solve_tol), differentiates the compliance through Compliance.backward, filters the sensitivity
-    and applies the top88 OC with its bisection to oc_tol.  Returns (x, rho, history)."""
+    and applies the top88 OC with its bisection to oc_tol.  check_every: the solves' true-residual
+    cadence (the reference fcg's default is 5).  Returns (x, rho, history)."""
     from .problems import cantilever_equal_split
     n = int(np.prod(shape))
     g = np.random.default_rng(seed)
@@ -208,7 +209,7 @@ def run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=100, em
     mask, force = cantilever_equal_split(shape)
     rho = filt.forward(x)
     solver = ElasticitySolver(shape, simp_modulus(rho, emin, 1.0, penal), mask, precision=precision, pre=pre, post=post,
-                              omega=omega, levels=levels, tol=solve_tol, maxiter=500, check_every=1)
+                              omega=omega, levels=levels, tol=solve_tol, maxiter=500, check_every=check_every)
     if omega == "spectral":
         solver.refresh_omegas(omega_iterations)
     state = SimpState(solver, force, emin=emin, e0=1.0, penal=penal)
