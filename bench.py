@@ -555,7 +555,7 @@ def run_kernels(args):
 
 
 def run_simp_bench(args):
-    """Config-4 SIMP run: 100 density-filtered SIMP iterations on the device, with the autograd
+    """The 192x96x96 SIMP run: 100 density-filtered SIMP iterations on the device, with the autograd
     sensitivity checked by central differences (64 seeded elements, step 1e-6) at the start design."""
     import torch
     import voxel_b200 as vx

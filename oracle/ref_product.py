@@ -1,6 +1,6 @@
 """ctypes binding of the reference's compiled C++ product (oracle/_ref/libreference.so).
 
-TEST / BASELINE INFRASTRUCTURE ONLY (see oracle/voxel_oracle.py).  The library is built from the
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY (see oracle/voxel_oracle.py).  The library is built from the
 reference's own sources by ``make -C oracle`` (experiments/session_a/inputs/reference.cc:12-39);
 its exported ABI is
     void element(double h, double nu, double* ke);

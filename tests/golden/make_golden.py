@@ -196,7 +196,7 @@ def main():
         fcg7_x=x7, fcg7_it=it7, fcg7_rel=rel7, fcg7_mv=mv7,
         fcg06_x=x06, fcg06_it=it06, fcg06_rel=rel06, fcg06_mv=mv06)
 
-    # ------------------------------------------------------------------ config 1 (32x16x16, Jacobi)
+    # ------------------------------------------------------------------ 32x16x16, Jacobi
     shape1 = (32, 16, 16)
     Ne1 = int(np.prod(shape1))
     rho1 = np.random.default_rng(0).uniform(0.01, 1.0, Ne1)
@@ -223,7 +223,7 @@ def main():
                                                   max_outer=40, inner_maxiter=4000, check_every=50)
     del sys.modules["cupy"]
     np.savez_compressed(
-        HERE / "config1.npz", shape=np.array(shape1), rho=rho1, E=E1, mask=m1, force=f1,
+        HERE / "jacobi_32x16x16.npz", shape=np.array(shape1), rho=rho1, E=E1, mask=m1, force=f1,
         fcg_x=xj, fcg_it=itj, fcg_ok=okj, fcg_rel=relj, fcg_mv=mvj, fcg_compliance=float(f1 @ xj),
         fcg_seconds=tj, pcg_x=xp_, pcg_it=itp, pcg_ok=okp, pcg_rel=relp,
         ir_x=xi, ir_outer=outer_i, ir_inner=inner_i, ir_ok=oki, ir_rel=reli)
@@ -268,7 +268,7 @@ def main():
                         "multigrid": proto["multigrid"], "order_seed": proto["order_seed"]}
     (HERE / "kat_session_i.json").write_text(json.dumps(kat, indent=1) + "\n")
 
-    # ------------------------------------------------------------------ config 2 (128x64x64 GMG)
+    # ------------------------------------------------------------------ 128x64x64, GMG
     if not args.skip_slow:
         sys.path.insert(0, str(REPO))
         from oracle.voxel_oracle import gaussian_random_field
@@ -301,7 +301,7 @@ def main():
         res2["rho_stats"] = [float(rho2.min()), float(rho2.max()), float(rho2.mean())]
         res2["rho_head"] = rho2[:16].tolist()
         res2["shapes"] = shapes2
-        (HERE / "config2.json").write_text(json.dumps(res2) + "\n")
+        (HERE / "gmg_128x64x64.json").write_text(json.dumps(res2) + "\n")
     donor_problems(ref)
     print("golden fixtures written to", HERE)
 

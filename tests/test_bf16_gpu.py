@@ -88,7 +88,7 @@ def test_bf16_transfers_and_coarse_solve(shape):
 
 
 def test_bf16_vcycle_is_a_close_preconditioner():
-    """M(r) of each storage mode against the FP64 V-cycle on the config-2 hierarchy."""
+    """M(r) of each storage mode against the FP64 V-cycle on the 128x64x64 hierarchy."""
     shape = (128, 64, 64)
     rho = vx.problems.gaussian_random_field(shape, 8.0, 0)
     E = vx.problems.simp_modulus(rho, 1e-9)
@@ -106,18 +106,18 @@ def test_bf16_vcycle_is_a_close_preconditioner():
 
 
 @pytest.mark.parametrize("precision,extra", [("bf16", 1), ("bf16-all", 12)])
-def test_bf16_config2_solve_reaches_the_fp64_residual(precision, extra):
+def test_bf16_gmg_128x64x64_solve_reaches_the_fp64_residual(precision, extra):
     """The FP64 outer loop reaches 1e-8 with either storage mode; "bf16" needs at most one more
     iteration than FP32 (emulated and measured: the same 15), "bf16-all" pays for rounding its
     iterates (about 21-25)."""
-    c = golden("config2.json")
+    c = golden("gmg_128x64x64.json")
     shape = (128, 64, 64)
     rho = vx.problems.gaussian_random_field(shape, 8.0, 0)
     E = vx.problems.simp_modulus(rho, 1e-9)
     mask, force = vx.problems.cantilever_equal_split(shape)
     s = ElasticitySolver(shape, E, mask, precision=precision, pre=2, post=2, omega=0.6, check_every=1)
     x, it, ok, r, mv = s.solve(force)
-    print(f"{precision} config 2: {it} iterations (fp32/fp64: 15), rel {r:.3e}")
+    print(f"{precision} 128x64x64: {it} iterations (fp32/fp64: 15), rel {r:.3e}")
     assert ok and r <= 1e-8 and it <= c["fp32"]["iterations"] + extra
     # the solution satisfies the FP64 residual bound: compliance agrees to the solve tolerance
     assert abs(float(force @ x) - c["fp64"]["compliance"]) <= 1e-7 * c["fp64"]["compliance"]

@@ -153,10 +153,10 @@ def test_fcg_smoke_iterates():
     assert it == int(g["fcg06_it"]) and rel(x, g["fcg06_x"]) < 1e-9
 
 
-# ----------------------------------------------------------------------------- config 1 (Jacobi)
+# ----------------------------------------------------------------------------- 32x16x16 Jacobi case
 @pytest.mark.slow
-def test_config1_jacobi_fcg_and_donor_pcg():
-    g = golden("config1.npz")
+def test_jacobi_32x16x16_fcg_and_donor_pcg():
+    g = golden("jacobi_32x16x16.npz")
     shape = tuple(g["shape"])
     ke = vo.quadrature([1, 1, 1], 0.3)
     rho = np.random.default_rng(0).uniform(0.01, 1.0, int(np.prod(shape)))
@@ -176,8 +176,8 @@ def test_config1_jacobi_fcg_and_donor_pcg():
 
 
 @pytest.mark.slow
-def test_config1_pcg_ir():
-    g = golden("config1.npz")
+def test_jacobi_32x16x16_pcg_ir():
+    g = golden("jacobi_32x16x16.npz")
     shape = tuple(g["shape"])
     ke = vo.quadrature([1, 1, 1], 0.3)
     mask, force, E = g["mask"], g["force"], g["E"]
@@ -210,8 +210,8 @@ def test_oc_top88():
 
 
 # ----------------------------------------------------------------------------- recipes
-def test_grf_recipe_matches_config2_record():
-    c = golden("config2.json")
+def test_grf_recipe_matches_the_gmg_128x64x64_record():
+    c = golden("gmg_128x64x64.json")
     rho = vo.gaussian_random_field((128, 64, 64), 8.0, 0)
     assert np.allclose([rho.min(), rho.max(), rho.mean()], c["rho_stats"], rtol=1e-14, atol=0)
     assert np.array_equal(rho[:16], np.array(c["rho_head"]))

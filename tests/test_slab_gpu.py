@@ -159,8 +159,8 @@ def test_slab_spectral_omegas_match_the_single_grid():
 
 @pytest.mark.parametrize("precision,nparts,extra", [("mixed", 4, 0), ("fp64", 2, 0), ("bf16", 3, 1),
                                                     ("mixed", 1, 0)])
-def test_slab_config2_solve(precision, nparts, extra):
-    c = golden("config2.json")
+def test_slab_gmg_128x64x64_solve(precision, nparts, extra):
+    c = golden("gmg_128x64x64.json")
     shape = (128, 64, 64)
     E, mask, force = _problem(shape)
     s = SlabSolver(shape, E, mask, nparts, precision=precision, pre=2, post=2, omega=0.6, check_every=1)
@@ -285,7 +285,7 @@ def test_slab_solve_across_processes(world):
         p.join(300)
         assert p.exitcode == 0
     got = sorted(q.get(timeout=10) for _ in range(world))
-    c = golden("config2.json")
+    c = golden("gmg_128x64x64.json")
     for g in got:
         _, distributed, staged, graph, it, rel, comp, fixed_zero, l1 = g
         print(f"rank {g[0]}/{world}: {it} iterations, rel {rel:.3e}, compliance {comp!r}")

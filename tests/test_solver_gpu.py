@@ -1,9 +1,9 @@
 """GPU parity of the solvers against the reference: golden V-cycle / fcg / pcg vectors generated
-from the reference's own code, the reference's measured config-1/config-2 records, and the
+from the reference's own code, the reference's measured 32x16x16 Jacobi and 128x64x64 GMG records, and the
 reference's published known answers (experiments/session_i: q64x2, q96x1, q96x3).
 
 Tolerances: V-cycle FP64 1e-12 relative (FP32 1e-5); solutions that take the same iterations
-as the reference agree to 1e-8 relative in displacement and compliance;
+as the reference agree to 1e-8 relative in displacement and compliance (the solve bar);
 published KATs agree in iteration count and to 1e-9 in compliance and solution norm (the
 reference's own arms spread by ~1e-10)."""
 import json
@@ -111,8 +111,8 @@ def test_transfer_mirror_matches_reference():
     assert np.array_equal(vmg.coarsen_mask(None, cu(t["cm_mask"]), (8, 4, 4)).cpu().numpy(), t["cm_maskc"])
 
 
-def _config1():
-    g = golden("config1.npz")
+def _jacobi_32x16x16():
+    g = golden("jacobi_32x16x16.npz")
     shape = tuple(int(s) for s in g["shape"])
     rho = vx.problems.uniform_density(shape, seed=0)
     assert np.array_equal(rho.cpu().numpy(), g["rho"])
@@ -121,8 +121,8 @@ def _config1():
     return g, shape, vx.problems.simp_modulus(rho, 1e-9), mask, force
 
 
-def test_config1_jacobi_fcg_650_iterations():
-    g, shape, E, mask, force = _config1()
+def test_jacobi_32x16x16_fcg_650_iterations():
+    g, shape, E, mask, force = _jacobi_32x16x16()
     s = ElasticitySolver(shape, E, mask, precision="jacobi", tol=1e-8, maxiter=5000, check_every=50)
     x, it, ok, r, mv = s.solve(force)
     assert ok and it == int(g["fcg_it"]) == 650
@@ -131,8 +131,8 @@ def test_config1_jacobi_fcg_650_iterations():
     assert rel(x, g["fcg_x"]) < 1e-8
 
 
-def test_config1_donor_jacobi_pcg():
-    g, shape, E, mask, force = _config1()
+def test_jacobi_32x16x16_donor_jacobi_pcg():
+    g, shape, E, mask, force = _jacobi_32x16x16()
     op = vx.VoxelOperator(shape, vo.quadrature([1, 1, 1], 0.3))
     nm = vx.node_mask_from_dofs(mask)
     pcg = vs.JacobiPCG(op, E, nm, tol=1e-8, maxiter=5000, check_every=50)
@@ -142,8 +142,8 @@ def test_config1_donor_jacobi_pcg():
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_config2_gmg_matches_reference_record(precision):
-    c = golden("config2.json")
+def test_gmg_128x64x64_matches_reference_record(precision):
+    c = golden("gmg_128x64x64.json")
     shape = (128, 64, 64)
     rho = vx.problems.gaussian_random_field(shape, 8.0, 0)
     assert np.allclose([float(rho.min()), float(rho.max()), float(rho.mean())], c["rho_stats"], rtol=1e-12)
@@ -256,11 +256,11 @@ def test_host_api_reuses_its_setup_for_new_inputs():
 
 
 def test_pcg_ir_matches_the_donor_record():
-    """Config 1 (32x16x16, i.i.d. densities), donor pcg_ir at tol 1e-8, inner tolerance 0.1: the
+    """The 32x16x16 case (i.i.d. densities), donor pcg_ir at tol 1e-8, inner tolerance 0.1: the
     reference's run takes 6 outer passes and 1400 inner FP32 iterations.  The inner products here
     are FP32 arithmetic (the donor rounds FP64 products to FP32), so the inner count may differ by a
     few iterations; the outer count, convergence and the compliance (to 1e-8) must agree."""
-    g = golden("config1.npz")
+    g = golden("jacobi_32x16x16.npz")
     shape = tuple(int(v) for v in g["shape"])
     op = vx.VoxelOperator(shape, vo.quadrature([1, 1, 1], 0.3))
     nm = vx.node_mask_from_dofs(cu(g["mask"]))
