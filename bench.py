@@ -3,18 +3,27 @@
 roofline of the dominant kernel.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload gmg_128x64x64|gmg_576x288x288|jacobi_32x16x16] [--no-large]
+                    [--workload gmg_576x288x288|gmg_128x64x64|jacobi_32x16x16|...] [--no-large]
 
-One step = one complete solve (hierarchy already built, inputs resident) of the workload; the
-timed region is K steps bracketed by a barrier + synchronize, timed with CUDA events, max over
-ranks.  L2 (126 MB) is flushed by writing a 256 MB buffer between timed steps, outside the
-event bracket.  `e2e` is the same solve through the public host-buffer API (voxel_b200.solve):
-pinned host inputs in, host solution out, hierarchy setup included.  With N > 1 (torchrun) every
-rank solves its own replica of the workload (the path does not need a collective): weak scaling.
+Default workload: the 576x288x288 cantilever (144.6M DOF, 6-level V(2,2)), the largest
+single-GPU configuration.  One step = one complete solve (hierarchy already built, inputs
+resident) of the workload; the timed region is K steps bracketed by a barrier + synchronize,
+timed with CUDA events, max over ranks.  The workload's vectors are far larger than L2
+(126 MB), and L2 is flushed by writing a 256 MB buffer between timed steps, outside the event
+bracket.  `e2e` is the same solve through the public host-buffer API (voxel_b200.solve):
+pinned host inputs in, host solution out, hierarchy refresh included.  With N > 1 (torchrun)
+every rank solves its own replica of the workload (the path does not need a collective): weak
+scaling.
 
-`--impl reference` times the reference algorithm's CPU implementation -- the NumPy restatement
-of src/voxel_mg.py (oracle/voxel_oracle.py) -- on this host's cores, on the same workload
-(rank 0 only).
+CPU baseline: on the 144.6M-DOF grid the reference's NumPy solve needs tens of GB of temporaries
+and about an hour, so the reference's own compiled C++ product (reference.cc, oracle/_ref,
+single-threaded) is timed on a 1/16 slab of the grid and scaled to one solve by the operator
+applications the solve performs -- an extrapolation, labelled as such.  The 128x64x64 section
+keeps a measured CPU solve (the NumPy restatement of src/voxel_mg.py, all host threads).
+
+`--impl reference` times the reference's CPU implementation on the same workload (rank 0 only):
+the C++ product sample above for the 144.6M-DOF grid, the NumPy restatement's full solve for the
+smaller grids.
 """
 from __future__ import annotations
 
@@ -63,7 +72,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="gmg_128x64x64")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="gmg_576x288x288")
     ap.add_argument("--no-large", action="store_true", help="skip the 144.6M-DOF section")
     ap.add_argument("--profile", action="store_true", help="short run for a profiler: no CPU baseline, no large")
     ap.add_argument("--host-loop", action="store_true",
@@ -135,11 +144,12 @@ def build_inputs(name, device="cuda"):
     return shape, levels, rho, E, mask, force
 
 
-# DRAM bytes per grid node of one launch, from ncu captures of the same kernels on the 256x128x128
-# grid (4,276,737 nodes; profiles/parity_stream_xp_*_256x128x128_ncu.md): dram__bytes_read.sum +
-# dram__bytes_write.sum / nodes.  Scaled by the node count of the measured launch.
+# DRAM bytes per grid node of one launch, from single-kernel ncu captures of the same kernels on the
+# 256x128x128 grid (4,276,737 nodes): dram__bytes_read.sum + dram__bytes_write.sum / nodes.  Scaled by
+# the node count of the measured launch (the traffic of these streaming kernels grows with the nodes).
 NCU_TRAFFIC_PER_NODE = {"jacobi_sweep_f32": (175.528960e6 + 36.767744e6) / 4276737,
                         "apply_dot_f64": (140.506880e6 + 71.061504e6) / 4276737}
+NCU_TRAFFIC_SOURCE = "ncu dram bytes of the same kernel on 256x128x128, per node, scaled by nodes"
 
 
 def peaks():
@@ -251,13 +261,21 @@ def kernel_table(solver, vx, torch, flush, reps=10):
 
 
 # ----------------------------------------------------------------------------------- arms
+def solve_arm(shape, E, mask, force, precision, kw, args, flush, rank_sync):
+    """Build a solver of `precision`, time it (CUDA events, L2 flushed), return (solver, times, result)."""
+    from voxel_b200.api import ElasticitySolver
+    s = ElasticitySolver(shape, E, mask, precision=precision, **kw)
+    times, res = time_solves(s, force, args.steps, args.warmup, flush, rank_sync)
+    return s, times, res
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
     torch.cuda.set_device(local_rank)
     import voxel_b200 as vx
     from voxel_b200 import _lib
-    from voxel_b200.api import ElasticitySolver
+    from voxel_b200.api import ElasticitySolver, clear_solver_cache
 
     def rank_sync():
         if world > 1:
@@ -266,6 +284,7 @@ def run_b200(args, rank, world, local_rank):
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MB > L2
     shape, levels, rho, E, mask, force = build_inputs(args.workload)
+    del rho
     precision = "jacobi" if levels is None else "mixed"
     kw = dict(tol=1e-8, maxiter=5000 if levels is None else 200, check_every=50 if levels is None else CHECK_EVERY,
               graph=not args.host_loop)
@@ -288,26 +307,31 @@ def run_b200(args, rank, world, local_rank):
            "ms_per_step": t_max * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64 outer / f32 preconditioner" if levels is not None else "f64", "data": "synthetic",
            "config": {"workload": args.workload, "description": WORKLOADS[args.workload][3],
-                      "check_every": kw["check_every"], "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                      "l2": "flushed (256 MB write) between timed steps"},
+                      "check_every": kw["check_every"]},
+           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+           "l2": "inputs larger than L2, and flushed (256 MB write) between timed steps",
            "solve": {"iterations": res.iterations, "converged": res.converged, "rel_residual": res.rel,
                      "matvecs": res.matvecs, "compliance": compliance, "step_s": times},
            "gpu_launches": int(launches_per_solve * args.steps)}
 
-    # FP64 arm (same hierarchy shapes, FP64 V-cycle)
+    # FP64 and bf16-storage arms (same hierarchy shapes)
     if levels is not None:
-        s64 = ElasticitySolver(shape, E, mask, precision="fp64", **kw)
-        times64, r64 = time_solves(s64, force, args.steps, args.warmup, flush, rank_sync)
+        del solver
+        torch.cuda.empty_cache()
+        s64, times64, r64 = solve_arm(shape, E, mask, force, "fp64", kw, args, flush, rank_sync)
         out["fp64"] = {"value": float(np.mean(times64)), "iterations": r64.iterations,
                        "compliance": float(force @ r64.x), "rel_residual": r64.rel}
         out["speedup_mixed_vs_fp64"] = float(np.mean(times64)) / t_local
         del s64
-        sb = ElasticitySolver(shape, E, mask, precision="bf16", **kw)     # bf16 moduli and auxiliaries
-        times_b, rb = time_solves(sb, force, args.steps, args.warmup, flush, rank_sync)
+        torch.cuda.empty_cache()
+        sb, times_b, rb = solve_arm(shape, E, mask, force, "bf16", kw, args, flush, rank_sync)
         out["bf16"] = {"value": float(np.mean(times_b)), "iterations": rb.iterations,
                        "compliance": float(force @ rb.x), "rel_residual": rb.rel,
                        "speedup_vs_fp64": float(np.mean(times64)) / float(np.mean(times_b))}
         del sb
+        torch.cuda.empty_cache()
+        solver = ElasticitySolver(shape, E, mask, precision=precision, **kw)
+        solver.solve(force)
 
     # roofline of the dominant kernel (largest share of one solve) on the solver's own data
     table = kernel_table(solver, vx, torch, flush)
@@ -318,18 +342,21 @@ def run_b200(args, rank, world, local_rank):
     tpn = NCU_TRAFFIC_PER_NODE.get(dom)
     out["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": b_dom / t_dom / 1e9, "peak": hbm, "unit": "GB/s",
                        "frac": b_dom / t_dom / 1e9 / hbm, "traffic": None if tpn is None else tpn * solver.op64.nodes,
-                       "traffic_source": "ncu dram bytes of the same kernel on 256x128x128, scaled by nodes",
-                       "peak_kind": peak_kind,
+                       "traffic_source": NCU_TRAFFIC_SOURCE, "peak_kind": peak_kind,
                        "bytes_per_launch": b_dom, "launch_s": t_dom,
-                       "kernels": {k: {"launch_us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9,
+                       "kernels": {k: {"launch_us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9, "frac_hbm": v[1] / v[0] / 1e9 / hbm,
                                        "per_solve": counts.get(k, 0)} for k, v in table.items()}}
     out["matvec"] = {"GDOF/s_f64_apply": 3 * solver.op64.nodes / table["apply_dot_f64"][0] / 1e9}
     out["clocks"] = clocks.summary()
+    products = products_per_solve(res, levels, 2, 2, kw["check_every"])
+    del solver
+    torch.cuda.empty_cache()
 
-    # e2e through the public host-buffer API (pinned inputs, setup + solve + result read back)
+    # e2e through the public host-buffer API (pinned inputs, refresh + solve + result read back)
     Eh = E.cpu().pin_memory()
     fh = force.cpu().pin_memory()
     mh = mask.cpu().pin_memory()
+    del E, mask
     e2e = []
     api_kw = dict(kw)
     api_kw.pop("levels", None)
@@ -341,17 +368,102 @@ def run_b200(args, rank, world, local_rank):
         torch.cuda.synchronize()
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
+        del u
     out["e2e"] = {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(Eh.numel() * 8 + fh.numel() * 8 + mh.numel() * 8),
-                  "d2h_bytes_per_step": int(fh.numel() * 8), "includes": "H2D of E/force/mask, hierarchy setup, solve, D2H of u",
-                  "compliance": info["compliance"]}
+                  "d2h_bytes_per_step": int(fh.numel() * 8), "includes": "H2D of E/force/0-1 DOF mask, hierarchy refresh, solve, D2H of u",
+                  "compliance": info["compliance"], "step_s": e2e}
+    clear_solver_cache()
+    del Eh, fh, mh
+    torch.cuda.empty_cache()
 
-    if rank == 0 and world == 1 and not args.profile and not args.no_large and args.workload != "gmg_576x288x288":
-        del solver
-        torch.cuda.empty_cache()
-        out["large"] = large_section(args, flush, rank_sync)
+    if rank == 0 and world == 1 and not args.profile and not args.no_large:
+        if args.workload == "gmg_576x288x288":
+            out["gmg_128x64x64"] = small_section(args, flush, rank_sync)
+        else:
+            out["large"] = large_section(args, flush, rank_sync)
         out["matvec_sweep"] = matvec_sweep(flush)
-    if rank == 0 and world == 1 and not args.profile and args.workload != "gmg_576x288x288":
-        out["cpu_baseline"] = cpu_baseline(args.workload)
+    if rank == 0 and world == 1 and not args.profile:
+        if args.workload == "gmg_576x288x288":
+            out["cpu_baseline"] = cpu_reference_product_baseline(args.workload, products, steps=1)
+        else:
+            out["cpu_baseline"] = cpu_baseline(args.workload)
+    return out
+
+
+def products_per_solve(res, levels, pre, post, check_every):
+    """Fine-grid operator applications of one mixed GMG-FCG solve (the unit the CPU baseline's
+    product time is scaled by): per iteration one outer A p, a true residual every `check_every`
+    iterations, and per V-cycle (pre - 1) + 1 + post products on every smoothed level (the first
+    pre-sweep starts from x = 0 and needs none), each coarser level 1/8 of the one above."""
+    it = int(res.iterations) if res is not None else REFERENCE_ITERATIONS
+    levels_f = sum(8.0 ** -l for l in range(levels - 1))
+    per_cycle = ((pre - 1) + 1 + post) * levels_f
+    return float(it * (1.0 + per_cycle) + it / check_every + 1 + per_cycle + 1)
+
+
+# FCG iterations of the 576x288x288 workload's mixed solve to 1e-8 (measured on the B200: the b200
+# arm's solve.iterations); the reference arm scales its C++ product time by it.
+REFERENCE_ITERATIONS = 20
+
+
+def cpu_reference_product_baseline(workload, products, steps=1):
+    """The reference's own C++ product (experiments/session_a/inputs/reference.cc, compiled into
+    oracle/_ref by oracle/Makefile; single-threaded) on a 1/16 slab of the workload's grid: the
+    slab's natural-layout z extent is nz/16 (the per-element cost is uniform).  Returns the slab
+    time scaled to the full grid and, by `products`, to one solve (extrapolated, not measured).
+    Without oracle/_ref the NumPy restatement of the reference product takes its place (kind port)."""
+    sys.path.insert(0, str(REPO))
+    from oracle import ref_product, voxel_oracle as vo
+    (nx, ny, nz), _, _, _ = WORKLOADS[workload]
+    slab = (nx, ny, max(1, nz // 16))
+    scale = nz / slab[2]
+    rng = np.random.default_rng(0)
+    ne = slab[0] * slab[1] * slab[2]
+    rho = 1e-3 + (1 - 1e-3) * rng.random(ne)
+    u = rng.standard_normal(3 * (slab[0] + 1) * (slab[1] + 1) * (slab[2] + 1))
+    mask = np.ones((slab[2] + 1, slab[1] + 1, slab[0] + 1, 3))
+    mask[:, :, 0, :] = 0.0                                     # natural layout, clamped x = 0 face
+    mask = mask.ravel()
+    ke = vo.quadrature([1, 1, 1], 0.3)
+    if ref_product.available():
+        ref = ref_product.ReferenceProduct()
+        fn, kind, what = (lambda: ref.product(slab, rho, u, ke, mask, 1e-9)), "reference", \
+            "reference.cc product() (oracle/_ref, g++ -O3, one thread)"
+    else:
+        fn, kind, what = (lambda: vo.c_reference_product(slab, rho, u, ke, mask, 1e-9)), "port", \
+            "NumPy restatement of reference.cc product() (oracle/voxel_oracle.py)"
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    t_slab = float(np.mean(ts))
+    t_full = t_slab * scale
+    return {"value": t_full * products, "unit": "s", "cores": 1, "kind": kind, "extrapolated": True,
+            "sample": f"{what} on a {slab[0]}x{slab[1]}x{slab[2]} slab (1/{scale:g} of the grid's elements), "
+                      f"scaled by element count to one full-grid product ({t_full:.3f} s) and by the "
+                      f"{products:.1f} fine-grid operator applications of one solve; the CPU solve itself is not run",
+            "product_s": t_full, "slab_s": ts, "products_per_solve": products, "host_cpus": os.cpu_count()}
+
+
+def small_section(args, flush, rank_sync):
+    """128x64x64 (1.64M DOF): mixed and FP64 solves on the B200 and the reference algorithm's
+    measured CPU solve (NumPy restatement, all host threads) on the same inputs."""
+    import torch
+    name = "gmg_128x64x64"
+    shape, levels, rho, E, mask, force = build_inputs(name)
+    del rho
+    kw = dict(tol=1e-8, maxiter=200, check_every=CHECK_EVERY, pre=2, post=2, omega=0.6, levels=levels)
+    out = {"workload": name, "description": WORKLOADS[name][3]}
+    for prec in ("mixed", "fp64"):
+        s, times, res = solve_arm(shape, E, mask, force, prec, kw, args, flush, rank_sync)
+        out[prec] = {"s": float(np.mean(times)), "iterations": res.iterations, "rel": res.rel,
+                     "compliance": float(force @ res.x)}
+        del s
+    torch.cuda.empty_cache()
+    cpu = cpu_baseline(name)
+    out["cpu_port"] = cpu
+    out["speedup_mixed_vs_cpu"] = cpu["value"] / out["mixed"]["s"]
     return out
 
 
@@ -522,20 +634,27 @@ def run_reference(args, rank):
     if args.workload in ("serving", "simp_192x96x96"):
         return {"impl": "reference", "unavailable": f"no CPU arm for {args.workload}: the CPU port of one solve of its "
                 "largest grid alone takes minutes; the CPU baseline is timed on the gmg and jacobi workloads"}
+    shape, _, levels, desc = WORKLOADS[args.workload]
     times = []
     for i in range(args.warmup + args.steps):
-        if i < args.warmup:
+        if args.workload == "gmg_576x288x288":
+            # one step = the reference's C++ product on a 1/16 slab, scaled to one solve
+            r = cpu_reference_product_baseline(args.workload, products_per_solve(None, levels, 2, 2, CHECK_EVERY))
+        elif i < args.warmup:
             continue            # the NumPy path has no warm-up state; warm-up steps are skipped
-        r = cpu_baseline(args.workload)
-        times.append(r["value"])
+        else:
+            r = cpu_baseline(args.workload)
+        if i >= args.warmup:
+            times.append(r["value"])
     v = float(np.mean(times))
     r["value"] = v
-    shape, _, levels, desc = WORKLOADS[args.workload]
     return {"impl": "reference", "metric": "time-to-1e-8 solve, mixed-precision GMG-PCG (FP32 V-cycle in FP64 flexible CG)"
             if levels is not None else "time-to-1e-8 solve, FP64 Jacobi-PCG", "value": v, "unit": "s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer / f32 preconditioner",
-            "data": "synthetic", "config": {"workload": args.workload, "description": desc, "check_every": CHECK_EVERY},
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 outer / f32 preconditioner" if levels is not None else "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "description": desc,
+                                            "check_every": 50 if levels is None else CHECK_EVERY},
             "cpu_baseline": r, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "step_s": times}
 

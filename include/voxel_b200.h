@@ -252,15 +252,25 @@ int vx_true_residual_planes(int prec, int nx, int ny, int nz, const double* bloc
                             const uint8_t* node_mask, const void* x, const void* b, void* res, double* partials,
                             int x_lo, int x_hi, cudaStream_t stream);
 
+/* Fault flag of the streaming operator kernels.  Their warps hand partial sums to each other
+ * through shared-memory barriers whose waits are bounded; a wait that ran out (which a correct run
+ * never does) sets this flag, and the output of that launch is invalid.  *status receives the flag
+ * (0 or 1); a non-zero `clear` resets it.  Synchronous with respect to the device.  No counterpart
+ * in the reference (its kernels have no waits between threads). */
+int vx_device_status(int* status, int clear);
+
 /* res = b - A x and *norm2 = sum res^2 (a device double), like vx_true_residual followed by
  * vx_reduce_partials, but needing no scratch buffer from the caller: for code that may not
  * allocate device memory (a request loop that must never call cudaMalloc mid-flight, a plugin
  * inside another framework's memory arena, a process under a hard memory cap).  The partial sums
  * live in a fixed array compiled into the library: 16384 doubles (128 KiB) on every device that
- * loads it, kept until the process exits.  Grids that need more than 16384 CTA partials
- * (vx_operator_partials(prec, ...)) are rejected with VX_ERR_INVALID_ARGUMENT.  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls share the one array: calls whose executions overlap on the GPU
+ * loads it, kept until the process exits.  The streaming kernel keeps one partial per persistent CTA
+ * (vx_operator_partials(prec, ...), at most one per SM), so every grid the library accepts fits;
+ * a launch that would need more than 16384 partials is rejected with VX_ERR_INVALID_ARGUMENT.  The
+ * first call on each device looks up the array's device address (cudaGetSymbolAddress) and keeps
+ * it for the process: make that first call before any stream capture, and do not use the entry
+ * point across a reset of the device's primary context (cudaDeviceReset), which would leave the
+ * kept address stale.  All calls share the one array: calls whose executions overlap on the GPU
  * (different streams, concurrent host threads) race and must be serialised by the caller.
  * No counterpart in the reference (it allocates every temporary through CuPy). */
 int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const double* blocks, const void* E,

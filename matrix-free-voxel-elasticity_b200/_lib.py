@@ -52,6 +52,7 @@ SIGNATURES = {
     "vx_apply_dot_planes": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, c_int, c_int, _P]),
     "vx_true_residual_planes": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, c_int, c_int, _P]),
     "vx_true_residual_noalloc": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
+    "vx_device_status": (c_int, [POINTER(c_int), c_int]),
     "vx_axpby": (c_int, [c_int, c_int64, c_double, _P, c_double, _P, _P]),
     "vx_cast": (c_int, [c_int64, c_int, _P, c_int, _P, c_double, _P]),
     # solver kernels with device-resident scalars and WHILE graphs
@@ -132,7 +133,7 @@ KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noal
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",
-             "vx_oc_partials", "vx_graph_body_nodes", "vx_plane_fix_partials"}
+             "vx_oc_partials", "vx_graph_body_nodes", "vx_plane_fix_partials", "vx_device_status"}
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 
@@ -149,6 +150,13 @@ def call(name: str, *args) -> None:
         launches += KERNELS_PER_CALL.get(name, 1)
     if CAPTURE_STREAM is not None and _lib.vx_capture_status(CAPTURE_STREAM) == 2:
         raise RuntimeError(f"{name} invalidated the stream capture")
+
+
+def device_status(clear: bool = True) -> int:
+    """The streaming kernels' fault flag (0 unless a bounded device wait ran out); waits for the device."""
+    v = c_int(0)
+    check(load().vx_device_status(ctypes.byref(v), int(bool(clear))), "vx_device_status")
+    return int(v.value)
 
 
 def dptr(a) -> _D:

@@ -21,6 +21,7 @@
 #include "vx_pair.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 #include <cmath>
 
@@ -320,6 +321,11 @@ struct OpArgs2 {
     Blocks2<TC> C2;
     CubeK<TC> K;
 };
+}  // namespace vx
+
+#include "vx_wave.cuh"
+
+namespace vx {
 
 // true if the 72 parity coefficients have the cube pattern above (to 1e-14 of the largest); the
 // constants are then taken from fixed positions
@@ -718,63 +724,136 @@ inline dim3 stream_grid(const Grid& g, Tiling t, int cx) {
     return dim3((g.nz + 1 + t.tz - 1) / t.tz, (g.ny + 1 + t.ty - 1) / t.ty, (g.nx + 1 + cx - 1) / cx);
 }
 
-// CTAs (= partial sums) of a fused reducing launch of precision `prec` on grid g
+// SM count of the current device (cached per device).
+inline int sm_count() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+    if (dev >= 64) {
+        int n = 148;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n;
+    }
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
+
+// Launch-time opt-in to more than 48 KB of dynamic shared memory, once per kernel and device (the
+// attribute is per device; `done` is the kernel's own bit set of configured devices, updated
+// atomically, so concurrent first launches at worst set the attribute twice).  The solvers run
+// every loop body once un-captured before capturing it, so the first call for a kernel never
+// happens inside a stream capture.
+inline int smem_opt_in(std::atomic<uint64_t>& done, const void* kern, size_t smem, const char* what) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return VX_OK;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) {
+        set_error("%s: cudaFuncSetAttribute: %s", what, cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    done.fetch_or(bit, std::memory_order_acq_rel);
+    return VX_OK;
+}
+
+template <typename TC>
+inline WaveSched wave_sched_for(const Grid& g) {
+    return wave_sched(g, WaveCfg<TC>::NW, WaveCfg<TC>::PL, sm_count());
+}
+template <typename TC>
+inline int64_t wave_ctas(const Grid& g) {
+    const WaveSched w = wave_sched_for<TC>(g);
+    return std::min<int64_t>(sm_count(), w.items);
+}
+
+// CTAs (= partial sums) of a fused reducing launch of precision `prec` on grid g: the reducing
+// forms (VX_F64, VX_F32) run the persistent wavefront kernel, one CTA per SM at most
 int64_t stream_ctas(const Grid& g, int prec) {
+    if (prec == VX_F32) return wave_ctas<float>(g);
+    if (prec == VX_F64) return wave_ctas<double>(g);
     const Tiling t = tiling(prec, true);
     dim3 d = stream_grid(g, t, stream_cx(g, t));
     return int64_t(d.x) * d.y * d.z;
+}
+
+template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK>
+OpArgs2<TC, TU, TE, TY, TR> packed_args(const OpArgs<TC, TU, TE, TY, TR>& a) {
+    OpArgs2<TC, TU, TE, TY, TR> a2;
+    a2.a = a;
+    for (int i = 0; i < 72; ++i) {
+        if constexpr (std::is_same<TC, float>::value) a2.C2.c[i] = make_float2(a.C.c[i], a.C.c[i]);
+        else a2.C2.c[i] = a.C.c[i];
+    }
+    if (a.cubic) a2.K = cube_constants<TC>(a.C);
+    return a2;
 }
 
 template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK, bool REV, bool SIMP, typename TR = TY>
 int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const char* what) {
     constexpr bool v2 = !REV && !SIMP && MASK != MASK_DOF;
     static_assert(v2 || std::is_same<TR, TY>::value, "parity_stream takes r and invd of the output type");
+    // iterates in FP64 / FP32: the wavefront kernel (u staged by cp.async, 4- or 8-byte words)
+    constexpr bool wave = v2 && (std::is_same<TU, double>::value || std::is_same<TU, float>::value);
     OpArgs<TC, TU, TE, TY, TR> a = a_in;
     const bool cubic = a.cubic;
-    const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
-    a.cx = stream_cx(a.g, t);
-    size_t smem, threads;
-    const void* kern;
-    if constexpr (v2) {
-        kern = cubic ? (const void*)parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true>
-                     : (const void*)parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false>;
-        threads = XpCfg<TC>::NW * 32;
-        smem = size_t(2) * XpCfg<TC>::NW * 6 * 32 * sizeof(V2<TC>);
-    } else {
-        kern = (const void*)parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
-        threads = NW * 32;
-        smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
-    }
-    // dynamic + static shared memory exceeds the 48 KB default: opt in once per instantiation.  The
-    // solvers run every loop body once un-captured before capturing it, so this call never happens
-    // inside a stream capture.
-    static bool configured[2] = {false, false};
-    if (!configured[cubic]) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) {
-            set_error("%s: cudaFuncSetAttribute: %s", what, cudaGetErrorString(e));
-            return VX_ERR_CUDA;
-        }
-        configured[cubic] = true;
-    }
-    if constexpr (v2) {
-        OpArgs2<TC, TU, TE, TY, TR> a2;
-        a2.a = a;
-        for (int i = 0; i < 72; ++i) {
-            if constexpr (std::is_same<TC, float>::value) a2.C2.c[i] = make_float2(a.C.c[i], a.C.c[i]);
-            else a2.C2.c[i] = a.C.c[i];
-        }
+    static std::atomic<uint64_t> configured[2];            // per kernel of this instantiation: devices opted in
+    if constexpr (wave) {
+        using Lc = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, true>;
+        const WaveSched ws = wave_sched_for<TC>(a.g);
+        const unsigned G = unsigned(std::min<int64_t>(sm_count(), ws.items));
+        const OpArgs2<TC, TU, TE, TY, TR> a2 = packed_args<TC, TU, TE, TY, TR, EPI, MASK>(a);
+        const unsigned threads = WaveCfg<TC>::NW * 32;
         if (cubic) {
-            a2.K = cube_constants<TC>(a.C);
-            vx::launch(parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true>, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a2);
+            auto k = parity_wave<TC, TU, TE, TY, TR, EPI, MASK, true>;
+            int st = smem_opt_in(configured[1], (const void*)k, Lc::BYTES, what);
+            if (st) return st;
+            vx::launch(k, G, threads, Lc::BYTES, s, a2, ws);
         } else {
-            vx::launch(parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false>, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a2);
+            auto k = parity_wave<TC, TU, TE, TY, TR, EPI, MASK, false>;
+            int st = smem_opt_in(configured[0], (const void*)k, Lc::BYTES, what);
+            if (st) return st;
+            vx::launch(k, G, threads, Lc::BYTES, s, a2, ws);
         }
+        VX_CHECK_LAUNCH(what);
+        return VX_OK;
     } else {
-        vx::launch(parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a);
+        const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
+        a.cx = stream_cx(a.g, t);
+        size_t smem, threads;
+        if constexpr (v2) {
+            threads = XpCfg<TC>::NW * 32;
+            smem = size_t(2) * XpCfg<TC>::NW * 6 * 32 * sizeof(V2<TC>);
+        } else {
+            threads = NW * 32;
+            smem = size_t(2) * NW * 6 * 32 * sizeof(TC);
+        }
+        if constexpr (v2) {
+            const OpArgs2<TC, TU, TE, TY, TR> a2 = packed_args<TC, TU, TE, TY, TR, EPI, MASK>(a);
+            if (cubic) {
+                auto k = parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, true>;
+                int st = smem_opt_in(configured[1], (const void*)k, smem, what);
+                if (st) return st;
+                vx::launch(k, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a2);
+            } else {
+                auto k = parity_stream_xp<TC, TU, TE, TY, TR, EPI, MASK, false>;
+                int st = smem_opt_in(configured[0], (const void*)k, smem, what);
+                if (st) return st;
+                vx::launch(k, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a2);
+            }
+        } else {
+            auto k = parity_stream<TC, TU, TE, TY, EPI, MASK, REV, SIMP>;
+            int st = smem_opt_in(configured[0], (const void*)k, smem, what);
+            if (st) return st;
+            vx::launch(k, stream_grid(a.g, t, a.cx), unsigned(threads), smem, s, a);
+        }
+        VX_CHECK_LAUNCH(what);
+        return VX_OK;
     }
-    VX_CHECK_LAUNCH(what);
-    return VX_OK;
 }
 
 template <typename TC>
@@ -1216,4 +1295,22 @@ extern "C" int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const 
                                       nullptr, 0.0, res, scratch, stream);
     if (st) return st;
     return vx_reduce_partials(G, 1, scratch, norm2, stream);
+}
+
+// Fault flag of the streaming kernels' bounded waits (0 in every correct run): copied to *status;
+// cleared when `clear` is non-zero.  Synchronous with respect to the device.
+extern "C" int vx_device_status(int* status, int clear) {
+    VX_CHECK_ARG(status, VX_ERR_NULL_POINTER, "vx_device_status: NULL status");
+    int v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, vx::g_wave_fault, sizeof(int));
+    if (e == cudaSuccess && clear && v) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(vx::g_wave_fault, &zero, sizeof(int));
+    }
+    if (e != cudaSuccess) {
+        set_error("vx_device_status: %s", cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    *status = v;
+    return VX_OK;
 }

@@ -156,6 +156,8 @@ class SimpState:
         self.warm_start = warm_start
         self.u = None
         self.last = None
+        self.retried = False          # the last forward solve was retried from zero
+        self.iterations = 0           # its iterations, the retry included
         self.op = solver.op64
 
     def modulus(self, rho):
@@ -170,12 +172,26 @@ class Compliance(torch.autograd.Function):
     @staticmethod
     def forward(ctx, rho, state: SimpState):
         state.solver.update_modulus(state.modulus(rho.detach()))
-        res = state.solver.solve(state.force, state.u if state.warm_start else None)
+        warm = state.u if state.warm_start else None
+        res = state.solver.solve(state.force, warm)
+        state.retried = False
+        iterations = res.iterations
+        if not res.converged and warm is not None:
+            # fail-closed (donor simp_r2.py:682-707): a warm-started miss is retried from zero, and the
+            # retry's iterations are counted
+            state.retried = True
+            res = state.solver.solve(state.force, None)
+            iterations += res.iterations
         if not res.converged:
-            raise RuntimeError(f"linear solve did not converge (rel {res.rel:.3e} after {res.iterations} iterations)")
+            from .donor import LinearSolveNotConverged
+            raise LinearSolveNotConverged(
+                f"linear solve missed tol={state.solver.fcg.tol:g} (relative residual {res.rel:.3e} after "
+                f"{iterations} iterations{', retried from zero' if state.retried else ''}); "
+                "the result is invalid under the fail-closed rule")
         u = res.x.clone()
         state.u = u
         state.last = res
+        state.iterations = iterations
         ctx.state = state
         ctx.save_for_backward(rho.detach(), u)
         return torch.dot(state.force, u).reshape(())
@@ -229,7 +245,8 @@ def run_simp(shape, volfrac=0.12, rmin=1.5, move=0.2, oc_tol=1e-6, steps=100, em
         change = float((x_new - x).abs().max())
         x = x_new
         torch.cuda.synchronize()
-        history.append({"step": k, "compliance": float(c.detach()), "iterations": state.last.iterations,
+        history.append({"step": k, "compliance": float(c.detach()), "iterations": state.iterations,
+                        "retried_from_zero": state.retried,
                         "rel": state.last.rel, "change": change, "volume": float(rho.mean()),
                         "oc_probes": oc.probes, "seconds": time.perf_counter() - t0})
         if callback:

@@ -717,7 +717,9 @@ class PCGIR:
     Returns IRResult (x, outer, inner, converged, rel)."""
 
     def __init__(self, op64: VoxelOperator, E64, node_mask, tol=1e-5, inner_tol=1e-1, max_outer=40,
-                 inner_maxiter=4000, check_every=50, graph=True):
+                 inner_maxiter=4000, check_every=50, graph=True, inv_diag32=None, E32=None):
+        """inv_diag32 / E32: the inner FP32 system's inverse diagonal and modulus (default: the FP32
+        inverse diagonal and the FP32 rounding of E64)."""
         if op64.dtype != torch.float64:
             raise ValueError("the outer operator must be float64")
         self.op64, self.E64, self.mask = op64, E64.contiguous(), node_mask
@@ -726,10 +728,14 @@ class PCGIR:
         n = op64.ndof
         self.n = n
         op32 = VoxelOperator(op64.shape, op64.ke, torch.float32)
-        self.E32 = torch.empty(self.E64.numel(), dtype=torch.float32, device="cuda")
-        _lib.call("vx_cast", self.E64.numel(), _lib.VX_F64, self.E64.data_ptr(), _lib.VX_F32, self.E32.data_ptr(), 1.0, _s())
+        if E32 is None:
+            self.E32 = torch.empty(self.E64.numel(), dtype=torch.float32, device="cuda")
+            _lib.call("vx_cast", self.E64.numel(), _lib.VX_F64, self.E64.data_ptr(), _lib.VX_F32, self.E32.data_ptr(), 1.0, _s())
+        else:
+            self.E32 = E32.to(torch.float32).contiguous()
         self.inner = JacobiPCG(op32, self.E32, node_mask, tol=inner_tol, maxiter=inner_maxiter,
-                               check_every=check_every, graph=graph)
+                               check_every=check_every, graph=graph,
+                               inv_diag=None if inv_diag32 is None else inv_diag32.to(torch.float32).contiguous())
         f64 = dict(dtype=torch.float64, device="cuda")
         self.x = torch.zeros(n, **f64)
         self.r = torch.zeros(n, **f64)

@@ -5,9 +5,14 @@ Same names, arguments and return values as the reference module (src/voxel_mg.py
 tensors in author layout; masks are the reference's 0/1 DOF masks (3N floats) -- the node masks
 the kernels use are derived from them.  Every product and transfer runs in libvoxel_b200.
 
-For speed, use voxel_b200.solver (MGHierarchy / FCGSolver): the same algorithm with the whole
-solve captured in one CUDA graph.  This module keeps the reference's host-driven control flow,
-including its host synchronisations, so a caller can switch without changing code.
+Two routes.  Any callable `apply_A` / `precondition` runs the reference's host-driven loop (its
+control flow and host synchronisations), so a caller can switch without changing code.  When
+`fcg` receives a Dirichlet apply this module can see into -- `dirichlet(product, E, mask)` (the
+reference's `lambda u: P.raw(u * mask, E) * mask + u * (1 - mask)`) or a `Level.apply` -- and a
+`Multigrid` built from voxel_b200 Products, the solve runs on voxel_b200.solver's FCGSolver
+instead: fused CG kernels, device scalars and the whole loop in one CUDA-graph launch, with the
+same iterates.  `Multigrid.coarse_solve` applies the inverse Cholesky factor with two
+bandwidth-bound triangular passes (no library call).
 """
 from __future__ import annotations
 
@@ -18,7 +23,7 @@ from . import _lib
 from .element import XYZ  # noqa: F401  (re-exported like the reference's XYZ)
 from .layout import edof_author  # noqa: F401
 from .operators import PREC, Product, VoxelOperator, _ptr, node_mask_from_dofs, stream_ptr
-from .solver import hierarchy_shapes  # noqa: F401
+from .solver import FCGSolver, MGHierarchy, _lower_inverse, hierarchy_shapes  # noqa: F401
 
 
 
@@ -109,6 +114,28 @@ class Level:
         return self.product.raw(u * self.mask, self.E) * self.mask + u * self.fixed
 
 
+class Dirichlet:
+    """u -> M K(E) (M u) + (I - M) u for a voxel_b200 Product: the reference's outer operator
+    `lambda u: P.raw(u * mask, E) * mask + u * (1 - mask)` (experiments/session_i/run_gpu.py:304) as an
+    object that fcg can recognise and run on the device solver."""
+
+    def __init__(self, product, E, mask):
+        if not isinstance(product, Product):
+            raise ValueError("dirichlet() needs a voxel_b200 Product")
+        self.product, self.op = product, product.op
+        self.E = _t(E, product.dtype)
+        self.mask = _t(mask)
+        self.node_mask = _node_mask(mask, product.shape)
+
+    def __call__(self, u):
+        return self.op.matvec(u.contiguous(), self.E, self.node_mask)
+
+
+def dirichlet(product, E, mask):
+    """The Dirichlet apply of `product` (see Dirichlet)."""
+    return Dirichlet(product, E, mask)
+
+
 class Multigrid:
     """V-cycle preconditioner (src/voxel_mg.py:133-178).  `products` are per-level product objects
     (finest first) exposing raw(u, E) and diagonal(E); `coarse_factor` is the lower Cholesky factor
@@ -129,10 +156,49 @@ class Multigrid:
         n_smooth = len(self.levels) - 1
         self.omegas = list(omegas) if omegas is not None else [0.6] * n_smooth
         assert len(self.omegas) == n_smooth
+        # the coarse solve: L^-1 of the FP64 factor packed with its transpose (two triangular passes)
+        f64 = _t(coarse_factor, torch.float64)
+        n = f64.shape[0]
+        linv = _lower_inverse(f64).contiguous()
+        self._packed = torch.empty_like(linv)
+        _lib.call("vx_coarse_pack", n, linv.data_ptr(), self._packed.data_ptr(), stream_ptr())
+        self._coarse_y = torch.empty(n, dtype=torch.float64, device="cuda")
+        # what the device route needs: FP64 finest modulus, products of one element matrix ke * 2^l
+        self._shapes = [tuple(int(v) for v in sh) for sh in shapes]
+        self._E64 = _t(E_fine, torch.float64)
+        self._node_mask = self.levels[0].node_mask
+        ok = all(isinstance(p, Product) for p in products) and dtype in (torch.float32, torch.float64)
+        if ok:
+            ke0 = products[0].op.ke
+            ok = all(np.allclose(p.op.ke, ke0 * 2 ** l, rtol=1e-15, atol=0) for l, p in enumerate(products))
+        self._ke0 = products[0].op.ke if ok else None
+        self._device = {}
 
     def coarse_solve(self, r):
-        y = torch.linalg.solve_triangular(self.coarse_factor, r.reshape(-1, 1), upper=False)
-        return torch.linalg.solve_triangular(self.coarse_factor.T, y, upper=True).reshape(-1)
+        """A_c^-1 r from the packed inverse factor (the reference's two triangular solves)."""
+        r = r.contiguous()
+        z = torch.empty_like(r)
+        prec = _lib.VX_F64 if r.dtype == torch.float64 else _lib.VX_F32
+        _lib.call("vx_coarse_apply_factor", prec, r.numel(), self._packed.data_ptr(), _ptr(r, "r"), None,
+                  self._coarse_y.data_ptr(), z.data_ptr(), stream_ptr())
+        return z
+
+    def device_solver(self, op64, E64, node_mask, tol, maxiter, check_every, fixed_iterations):
+        """The FCGSolver over this hierarchy's data (cached per outer operator and settings), or None
+        when the hierarchy was not built from voxel_b200 Products of one element matrix."""
+        if self._ke0 is None:
+            return None
+        key = (id(op64), E64.data_ptr(), float(tol), int(maxiter), int(check_every), fixed_iterations)
+        s = self._device.get(key)
+        if s is None:
+            if "M" not in self._device:
+                self._device["M"] = MGHierarchy(self._shapes[0], self._ke0, self._E64, self._node_mask, self.dtype,
+                                                self.pre, self.post, list(self.omegas), shapes=self._shapes)
+            s = FCGSolver(op64, E64, node_mask, self._device["M"], tol=tol, maxiter=maxiter,
+                          check_every=check_every, fixed_iterations=fixed_iterations)
+            self._device[key] = s
+        self._device["M"].set_omegas(list(self.omegas))
+        return s
 
     def _sweep(self, L, x, r, w):
         if L.op is not None:
@@ -162,9 +228,30 @@ class Multigrid:
         return self.vcycle(r.to(self.dtype)).to(r.dtype)
 
 
+def _outer(apply_A):
+    """(op64, E64, node_mask) of an apply this module can see into, else None."""
+    if isinstance(apply_A, Dirichlet):
+        src = apply_A
+    elif isinstance(getattr(apply_A, "__self__", None), Level) and getattr(apply_A, "__func__", None) is Level.apply:
+        src = apply_A.__self__
+    else:
+        return None
+    if src.op is None or src.op.dtype != torch.float64:
+        return None
+    return src.op, src.E, src.node_mask
+
+
 def fcg(xp, apply_A, b, precondition, tol, maxiter, check_every=5, fixed_iterations=None):
     """Flexible PCG (Polak-Ribiere beta), FP64 outer, true-residual stopping test with residual
-    replacement (src/voxel_mg.py:181-217).  Returns (x, iterations, converged, rel, matvecs)."""
+    replacement (src/voxel_mg.py:181-217).  Returns (x, iterations, converged, rel, matvecs).
+    A `dirichlet(...)` / `Level.apply` outer operator with a voxel_b200 Multigrid runs on the
+    device solver (same iterates; see the module docstring)."""
+    outer = _outer(apply_A)
+    if outer is not None and isinstance(precondition, Multigrid) and b.dtype == torch.float64:
+        s = precondition.device_solver(*outer, tol, maxiter, check_every, fixed_iterations)
+        if s is not None:
+            x, it, ok, rel, mv = s.solve(b.contiguous())
+            return x.clone(), it, ok, rel, mv
     nb = float(torch.linalg.vector_norm(b))
     x = torch.zeros_like(b)
     r = b.clone()

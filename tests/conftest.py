@@ -28,3 +28,20 @@ def golden(name):
 @pytest.fixture(scope="session")
 def gold():
     return golden
+
+
+@pytest.fixture(autouse=True)
+def _streaming_fault_flag(request):
+    """After every GPU test: the streaming kernels' device fault flag (a bounded wait between warps
+    that ran out) must be clear."""
+    yield
+    if request.node.get_closest_marker("gpu") is None:
+        return
+    try:
+        import torch
+        if not torch.cuda.is_available() or not torch.cuda.is_initialized():
+            return
+        from voxel_b200 import _lib
+    except Exception:
+        return
+    assert _lib.device_status(clear=True) == 0, "a streaming operator kernel's bounded wait ran out"

@@ -14,6 +14,7 @@ import torch
 
 from conftest import golden
 from oracle import voxel_oracle as vo
+from physical import physical_check
 
 pytestmark = pytest.mark.gpu
 vx = pytest.importorskip("voxel_b200")
@@ -156,6 +157,9 @@ def test_gmg_128x64x64_matches_reference_record(precision):
     assert abs(float(force @ x) - ref["compliance"]) <= 1e-8 * ref["compliance"]
     idx = np.array(c["sample_index"])
     assert rel(x.cpu().numpy()[idx], np.array(ref["samples"])) < 1e-7
+    chk = physical_check(shape, vo.quadrature([1, 1, 1], 0.3), rho.cpu().numpy(), 1e-9, mask.cpu().numpy(),
+                         force.cpu().numpy(), x.cpu().numpy())
+    assert chk["passed"], chk
 
 
 def _kat(case, precision):
@@ -176,6 +180,9 @@ def _kat(case, precision):
     assert [list(s_) for s_ in s.levels] == kat[case]["shapes"]
     x, it, ok, r, mv = s.solve(force)
     obs = kat[case]["observations"]
+    chk = physical_check(shape, k[f"{base}_ke"], vx.to_author(rho_nat, shape), floor, mask.cpu().numpy(),
+                         force.cpu().numpy(), x.cpu().numpy())
+    assert chk["passed"], chk
     return x, it, ok, float(force @ x), obs
 
 
@@ -271,3 +278,59 @@ def test_pcg_ir_matches_the_donor_record():
     assert abs(inner - int(g["ir_inner"])) <= 0.05 * int(g["ir_inner"])
     comp = float(cu(g["force"]) @ x)
     assert abs(comp - float(g["fcg_compliance"])) <= 1e-8 * abs(float(g["fcg_compliance"]))
+
+
+def test_voxel_mg_fast_route_reproduces_the_golden_iterates(smoke):
+    """fcg with the reference's call shape routes to the device solver when its outer operator is
+    voxel_mg.dirichlet(...) or a Level.apply, and gives the golden fcg iterates."""
+    g, shapes, _ = smoke
+    prods = [vx.Product(s, g["ke"] * 2 ** i) for i, s in enumerate(shapes)]
+    A = vmg.assemble_dense(shapes[-1], g["ke"] * 2 ** (len(shapes) - 1),
+                           vmg.coarsen_modulus(None, vmg.coarsen_modulus(None, cu(g["E"]), shapes[0]), shapes[1]),
+                           vmg.coarsen_mask(None, vmg.coarsen_mask(None, cu(g["mask"]), shapes[0]), shapes[1]))
+    M = vmg.Multigrid(None, shapes, prods, cu(g["E"]), cu(g["mask"]), torch.linalg.cholesky(A), torch.float64,
+                      pre=4, post=4, omegas=g["omegas"])
+    # the packed-factor coarse solve equals the reference's two triangular solves
+    rc = torch.randn(A.shape[0], dtype=torch.float64, device="cuda")
+    assert rel(M.coarse_solve(rc), torch.linalg.solve(A, rc).cpu().numpy()) < 1e-12
+    for apply_A in (vmg.dirichlet(vx.Product(shapes[0], g["ke"]), cu(g["E"]), cu(g["mask"])), M.levels[0].apply):
+        assert vmg._outer(apply_A) is not None
+        x, it, ok, r, mv = vmg.fcg(None, apply_A, cu(g["force"]), M, 1e-8, 200)
+        assert ok and (it, mv) == (int(g["fcg_it"]), int(g["fcg_mv"]))
+        assert rel(x, g["fcg_x"]) < 1e-9
+    assert M._device                                        # the device route ran
+
+
+def test_voxel_mg_fast_route_speed_128x64x64():
+    """The mirror's device route on the 128x64x64 workload runs within 1.2x of ElasticitySolver."""
+    import time
+    shape = (128, 64, 64)
+    rho = vx.problems.gaussian_random_field(shape, 8.0, 0)
+    E = vx.problems.simp_modulus(rho, 1e-9)
+    mask, force = vx.problems.cantilever_equal_split(shape)
+    shapes = vx.hierarchy_shapes(shape, 16)
+    ke = vo.quadrature([1, 1, 1], 0.3)
+    prods = [vx.Product(s, ke * 2 ** i, torch.float32) for i, s in enumerate(shapes)]
+    Ec, mc = E, mask
+    for i in range(len(shapes) - 1):
+        Ec, mc = vmg.coarsen_modulus(None, Ec, shapes[i]), vmg.coarsen_mask(None, mc, shapes[i])
+    factor = torch.linalg.cholesky(vmg.assemble_dense(shapes[-1], ke * 2 ** (len(shapes) - 1), Ec, mc))
+    M = vmg.Multigrid(None, shapes, prods, E, mask, factor, torch.float32, pre=2, post=2)
+    A = vmg.dirichlet(vx.Product(shape, ke), E, mask)
+    es = ElasticitySolver(shape, E, mask, precision="mixed", pre=2, post=2, omega=0.6, check_every=5)
+
+    def t(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+        return best
+    t_mirror = t(lambda: vmg.fcg(None, A, force, M, 1e-8, 200))
+    t_solver = t(lambda: es.solve(force))
+    x, it, ok, r, mv = vmg.fcg(None, A, force, M, 1e-8, 200)
+    assert ok and it == es.solve(force).iterations == 15
+    assert t_mirror <= 1.2 * t_solver + 2e-4, (t_mirror, t_solver)
