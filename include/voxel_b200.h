@@ -259,6 +259,17 @@ int vx_true_residual_planes(int prec, int nx, int ny, int nz, const double* bloc
  * in the reference (its kernels have no waits between threads). */
 int vx_device_status(int* status, int clear);
 
+/* The coarsest level's exact solve, set up without library calls (replaces the host Cholesky and the
+ * two triangular solves of src/voxel_mg.py:152-159, experiments/session_i/run_gpu.py:281-286).
+ * A: the dense n x n constrained matrix (vx_assemble_dense, row-major, symmetric positive definite),
+ * bw: its half-bandwidth (a voxel grid's coarsest matrix: 3 ((ny+1)(nz+1) + (nz+1) + 1) + 2, at most
+ * n - 1).  Writes packed = tril(L^-1) + triu(L^-T, 1) with A = L L^T for vx_coarse_apply_factor, and
+ * *info (device int) = 0, or the 1-based column of the first non-positive pivot.  `work` holds
+ * vx_coarse_factor_workspace(n, bw) doubles.  Bands wider than the kernel's shared-memory window
+ * (about 5800) are rejected with VX_ERR_INVALID_ARGUMENT ("too wide"). */
+int64_t vx_coarse_factor_workspace(int n, int bw);
+int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* work, int* info, cudaStream_t stream);
+
 /* res = b - A x and *norm2 = sum res^2 (a device double), like vx_true_residual followed by
  * vx_reduce_partials, but needing no scratch buffer from the caller: for code that may not
  * allocate device memory (a request loop that must never call cudaMalloc mid-flight, a plugin

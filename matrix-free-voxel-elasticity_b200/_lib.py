@@ -53,6 +53,8 @@ SIGNATURES = {
     "vx_true_residual_planes": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, c_int, c_int, _P]),
     "vx_true_residual_noalloc": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
     "vx_device_status": (c_int, [POINTER(c_int), c_int]),
+    "vx_coarse_factor_workspace": (c_int64, [c_int, c_int]),
+    "vx_coarse_factor": (c_int, [c_int, c_int, _P, _P, _P, _P, _P]),
     "vx_axpby": (c_int, [c_int, c_int64, c_double, _P, c_double, _P, _P]),
     "vx_cast": (c_int, [c_int64, c_int, _P, c_int, _P, c_double, _P]),
     # solver kernels with device-resident scalars and WHILE graphs
@@ -133,7 +135,8 @@ KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noal
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",
-             "vx_oc_partials", "vx_graph_body_nodes", "vx_plane_fix_partials", "vx_device_status"}
+             "vx_oc_partials", "vx_graph_body_nodes", "vx_plane_fix_partials", "vx_device_status",
+             "vx_coarse_factor_workspace"}
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 
@@ -146,7 +149,9 @@ def call(name: str, *args) -> None:
     if fn is None:
         fn = _FNS[name] = getattr(load(), name)
     check(fn(*args), name)
-    if name not in HOST_ONLY:
+    if name == "vx_coarse_factor":          # band load, a factor and an update per 64-column block, inverse
+        launches += 2 * ((int(args[0]) + 63) // 64) + 1
+    elif name not in HOST_ONLY:
         launches += KERNELS_PER_CALL.get(name, 1)
     if CAPTURE_STREAM is not None and _lib.vx_capture_status(CAPTURE_STREAM) == 2:
         raise RuntimeError(f"{name} invalidated the stream capture")

@@ -150,7 +150,8 @@ def solve(shape, E, force, mask, *, ke=None, precision="mixed", tol=1e-8, maxite
         _SOLVERS.popitem(last=False)
     s.fcg.tol, s.fcg.maxiter = float(tol), int(maxiter)
     f = _dev(force)
-    res = s.solve(f)
+    s.fcg.launch(f, dot_with=f)                    # the compliance f . u comes back with the solver scalars
+    res = s.fcg.finish()
     u = res.x.cpu().numpy()
     return u, dict(iterations=res.iterations, converged=res.converged, rel=res.rel, matvecs=res.matvecs,
-                   compliance=float(np.dot(np.asarray(force, dtype=np.float64), u)))
+                   compliance=float(s.fcg.last_dot))

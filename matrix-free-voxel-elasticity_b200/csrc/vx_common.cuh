@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <atomic>
 #include <cstdio>
 #include <string>
 #include <utility>
@@ -61,6 +62,25 @@ inline cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Launch-time opt-in to more than 48 KB of dynamic shared memory, once per kernel and device (the
+// attribute is per device; `done` is the kernel's own bit set of configured devices, updated
+// atomically, so concurrent first launches at worst set the attribute twice).  The solvers run
+// every loop body once un-captured before capturing it, so the first call for a kernel never
+// happens inside a stream capture.
+inline int smem_opt_in(std::atomic<uint64_t>& done, const void* kern, size_t smem, const char* what) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return VX_OK;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) {
+        set_error("%s: cudaFuncSetAttribute: %s", what, cudaGetErrorString(e));
+        return VX_ERR_CUDA;
+    }
+    done.fetch_or(bit, std::memory_order_acq_rel);
+    return VX_OK;
 }
 
 // Grid extents: element grid (nx, ny, nz); nodes (nx+1)(ny+1)(nz+1); author layout, z fastest.

@@ -742,25 +742,6 @@ inline int sm_count() {
     return n;
 }
 
-// Launch-time opt-in to more than 48 KB of dynamic shared memory, once per kernel and device (the
-// attribute is per device; `done` is the kernel's own bit set of configured devices, updated
-// atomically, so concurrent first launches at worst set the attribute twice).  The solvers run
-// every loop body once un-captured before capturing it, so the first call for a kernel never
-// happens inside a stream capture.
-inline int smem_opt_in(std::atomic<uint64_t>& done, const void* kern, size_t smem, const char* what) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const uint64_t bit = dev < 64 ? uint64_t(1) << dev : 0;
-    if (bit && (done.load(std::memory_order_acquire) & bit)) return VX_OK;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) {
-        set_error("%s: cudaFuncSetAttribute: %s", what, cudaGetErrorString(e));
-        return VX_ERR_CUDA;
-    }
-    done.fetch_or(bit, std::memory_order_acq_rel);
-    return VX_OK;
-}
-
 template <typename TC>
 inline WaveSched wave_sched_for(const Grid& g) {
     return wave_sched(g, WaveCfg<TC>::NW, WaveCfg<TC>::PL, sm_count());

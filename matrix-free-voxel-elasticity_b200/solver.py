@@ -181,11 +181,28 @@ class MGHierarchy:
 
     def _coarse_inverse(self):
         """Factor the coarsest matrix A = L L^T (FP64 Cholesky) and pack L^-1 with its transpose for
-        vx_coarse_apply_factor; L^-1 comes from a recursive block inversion whose work is matrix
-        products.  Everything is queued on the current stream without a host synchronisation.
-        Returns the factorisation's device-side info tensor (0 when A is positive definite)."""
-        self.coarse_factor, info = torch.linalg.cholesky_ex(self.A_coarse)
-        linv = _lower_inverse(self.coarse_factor).contiguous()     # the kernel reads it row-major
+        vx_coarse_apply_factor.  The matrix is banded (a node couples to its 27 neighbours), so
+        vx_coarse_factor factors the band and forms L^-1 by banded forward substitution in the
+        library's own kernels.  A coarsest grid too wide for that kernel's shared-memory window takes
+        a dense Cholesky and a recursive block inversion instead.  Everything is queued on the current
+        stream without a host synchronisation.  Returns the factorisation's device-side info tensor
+        (0 when A is positive definite)."""
+        n = self.A_coarse.shape[0]
+        nx, ny, nz = self.levels[-1].shape
+        bw = min(n - 1, 3 * ((ny + 1) * (nz + 1) + (nz + 1) + 1) + 2)
+        if getattr(self, "_factor_work", None) is None:
+            need = int(_lib.load().vx_coarse_factor_workspace(n, bw))
+            self._factor_work = torch.empty(max(need, 1), dtype=torch.float64, device="cuda")
+            self._factor_info = torch.zeros(1, dtype=torch.int32, device="cuda")
+        try:
+            _lib.call("vx_coarse_factor", n, bw, self.A_coarse.data_ptr(), self.coarse_packed.data_ptr(),
+                      self._factor_work.data_ptr(), self._factor_info.data_ptr(), _s())
+            return self._factor_info
+        except ValueError as e:
+            if "too wide" not in str(e):
+                raise
+        factor, info = torch.linalg.cholesky_ex(self.A_coarse)
+        linv = _lower_inverse(factor).contiguous()                  # the kernel reads it row-major
         _lib.call("vx_coarse_pack", linv.shape[0], linv.data_ptr(), self.coarse_packed.data_ptr(), _s())
         return info
 
@@ -195,7 +212,8 @@ class MGHierarchy:
             for t in (L.x, L.xt, L.r, L.invd, L.res, L.E):
                 b += 0 if t is None else t.numel() * t.element_size()
             b += L.E64.numel() * 8 + L.mask.numel()
-        return b + self.coarse_packed.numel() * 8 * 4    # A, factor, packed inverse factor, transient L^-1
+        work = getattr(self, "_factor_work", None)
+        return b + self.coarse_packed.numel() * 8 * 2 + (0 if work is None else work.numel() * 8)   # A, packed, band
 
     def spectral_omegas(self, iterations=30, seed=20260923):
         """omega_l = 4 / (3 lambda_l), lambda_l from a seeded FP64 power iteration on D^-1 A over the

@@ -334,3 +334,45 @@ def test_voxel_mg_fast_route_speed_128x64x64():
     x, it, ok, r, mv = vmg.fcg(None, A, force, M, 1e-8, 200)
     assert ok and it == es.solve(force).iterations == 15
     assert t_mirror <= 1.2 * t_solver + 2e-4, (t_mirror, t_solver)
+
+
+@pytest.mark.parametrize("n,bw", [(1, 0), (5, 4), (70, 9), (200, 63), (517, 64), (1000, 130), (1911, 275)])
+def test_banded_coarse_factor_matches_the_dense_inverse_factor(n, bw):
+    """vx_coarse_factor (banded Cholesky + banded forward substitution, no library call) gives the
+    packed tril(L^-1) + triu(L^-T, 1) of a banded SPD matrix to FP64 rounding, for sizes that are
+    not multiples of the 64-column block and bands narrower and wider than a block."""
+    rng = np.random.default_rng(n + bw)
+    B = np.zeros((n, n))
+    for k in range(bw + 1):
+        d = rng.standard_normal(n - k)
+        B += np.diag(d, -k)
+    A = B @ B.T + n * np.eye(n)
+    A = np.triu(np.tril(A, bw), -bw)                       # keep the band (still SPD: diagonally dominant)
+    A += np.eye(n) * (np.abs(A).sum(1).max())
+    L = np.linalg.cholesky(A)
+    X = np.linalg.inv(L)
+    ref = np.tril(X) + np.triu(X.T, 1)
+    Ad = cu(A)
+    packed = torch.full_like(Ad, float("nan"))
+    work = torch.empty(int(vx._lib.load().vx_coarse_factor_workspace(n, bw)), dtype=torch.float64, device="cuda")
+    info = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    vx._lib.call("vx_coarse_factor", n, bw, Ad.data_ptr(), packed.data_ptr(), work.data_ptr(), info.data_ptr(),
+                 torch.cuda.current_stream().cuda_stream)
+    assert int(info) == 0
+    P = packed.cpu().numpy()
+    assert np.isfinite(P).all()
+    assert np.max(np.abs(P - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_banded_coarse_factor_flags_a_matrix_that_is_not_positive_definite():
+    n, bw = 150, 20
+    A = np.eye(n) * 4 + np.eye(n, k=1) + np.eye(n, k=-1)
+    A[97, 97] = -1.0
+    Ad = cu(A)
+    packed = torch.empty_like(Ad)
+    work = torch.empty(int(vx._lib.load().vx_coarse_factor_workspace(n, bw)), dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    vx._lib.call("vx_coarse_factor", n, bw, Ad.data_ptr(), packed.data_ptr(), work.data_ptr(), info.data_ptr(),
+                 torch.cuda.current_stream().cuda_stream)
+    assert int(info) == 98                                  # 1-based column of the first bad pivot
+    assert torch.isfinite(packed).all()
