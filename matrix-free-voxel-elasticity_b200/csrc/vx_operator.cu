@@ -784,22 +784,30 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
     const bool cubic = a.cubic;
     static std::atomic<uint64_t> configured[2];            // per kernel of this instantiation: devices opted in
     if constexpr (wave) {
-        using Lc = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, true>;
         const WaveSched ws = wave_sched_for<TC>(a.g);
         const unsigned G = unsigned(std::min<int64_t>(sm_count(), ws.items));
         const OpArgs2<TC, TU, TE, TY, TR> a2 = packed_args<TC, TU, TE, TY, TR, EPI, MASK>(a);
         const unsigned threads = WaveCfg<TC>::NW * 32;
-        if (cubic) {
-            auto k = parity_wave<TC, TU, TE, TY, TR, EPI, MASK, true>;
-            int st = smem_opt_in(configured[1], (const void*)k, Lc::BYTES, what);
+        // rows staged by bulk (TMA-engine) copies when the arrays are 16-byte aligned, else by cp.async
+        const bool bulk = aligned(a.u, 16) && aligned(a.E, 16) && (MASK == MASK_NONE || aligned(a.node_mask, 16));
+        auto go = [&](auto kern, size_t bytes, std::atomic<uint64_t>& flag) -> int {
+            int st = smem_opt_in(flag, (const void*)kern, bytes, what);
             if (st) return st;
-            vx::launch(k, G, threads, Lc::BYTES, s, a2, ws);
+            vx::launch(kern, G, threads, bytes, s, a2, ws);
+            return VX_OK;
+        };
+        static std::atomic<uint64_t> cfg_bulk[2];
+        int st;
+        if (bulk) {
+            using Lb = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, true, true>;
+            st = cubic ? go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, true, true>, Lb::BYTES, cfg_bulk[1])
+                       : go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, false, true>, Lb::BYTES, cfg_bulk[0]);
         } else {
-            auto k = parity_wave<TC, TU, TE, TY, TR, EPI, MASK, false>;
-            int st = smem_opt_in(configured[0], (const void*)k, Lc::BYTES, what);
-            if (st) return st;
-            vx::launch(k, G, threads, Lc::BYTES, s, a2, ws);
+            using La = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, true, false>;
+            st = cubic ? go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, true, false>, La::BYTES, configured[1])
+                       : go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, false, false>, La::BYTES, configured[0]);
         }
+        if (st) return st;
         VX_CHECK_LAUNCH(what);
         return VX_OK;
     } else {

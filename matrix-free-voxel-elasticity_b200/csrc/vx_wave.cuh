@@ -121,9 +121,48 @@ __device__ __forceinline__ T unstage(const stage_t<T>& s, const T* p) {
     }
 }
 
+// Bulk (TMA-engine) copy of `bytes` (a multiple of 16) from 16-byte aligned global memory into shared
+// memory, completing as transaction bytes on the mbarrier `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory before later async-proxy
+// writes to it (a staging slot that was read is refilled by bulk copies).
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// One staged row: elements [first, first + cnt) of an array of `total` elements of `es` bytes whose
+// base is 16-byte aligned.  The bulk copy starts at the 16-byte boundary at or below the first
+// element (`off` bytes before it) and covers whole 16-byte units; `bulk` is false when that would
+// read past the array's end (the row is then copied element by element).
+struct RowSpan {
+    const unsigned char* src;
+    uint32_t len;
+    uint32_t off;
+    bool bulk;
+};
+__device__ __forceinline__ RowSpan row_span(const void* base, int first, int cnt, int es, int total) {
+    const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+    const uintptr_t g0 = b + uintptr_t(first) * uintptr_t(es);
+    const uintptr_t a0 = g0 & ~uintptr_t(15);
+    const uint32_t off = uint32_t(g0 - a0);
+    const uint32_t len = (off + uint32_t(cnt) * uint32_t(es) + 15u) & ~15u;
+    RowSpan r;
+    r.src = reinterpret_cast<const unsigned char*>(a0);
+    r.len = len;
+    r.off = off;
+    r.bulk = a0 + len <= b + uintptr_t(total) * uintptr_t(es);
+    return r;
+}
+
 // ---------------------------------------------------------------- mbarriers (CTA scope)
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+                 ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
@@ -161,7 +200,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, volati
 }
 
 // ---------------------------------------------------------------- the kernel
-template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC>
+// Shared memory of one launch.  Per warp, a ring of DEPTH staging slots; a slot holds PL node planes.
+// cp.async staging (BULK = false): each thread's words, [slot][plane][item][lane].  Bulk staging
+// (BULK = true): whole rows as the bulk copies leave them -- own and upper u rows (96 values each),
+// the element modulus row, the two mask rows -- each starting `off` bytes into a 16-byte aligned
+// buffer.  Then the exchange buffers of every row and the mbarriers: full/empty of the exchange
+// (4 per row), the bulk staging's full barrier per row and slot, the abort flag.
+template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC, bool BULK>
 struct WaveLayout {
     using Cfg = WaveCfg<TC>;
     static constexpr int PL = Cfg::PL, NW = Cfg::NW, D = Cfg::DEPTH;
@@ -170,18 +215,23 @@ struct WaveLayout {
     static constexpr size_t U_B = sizeof(stage_t<TU>) * D * PL * 6 * 32;    // own + upper row, 3 components
     static constexpr size_t E_B = sizeof(stage_t<TE>) * D * PL * 32;
     static constexpr size_t M_B = HAS_M ? sizeof(uint32_t) * D * PL * 2 * 32 : 0;
-    static constexpr size_t WARP_B = (U_B + E_B + M_B + 15) / 16 * 16;
+    static constexpr uint32_t RBU = (15 + 96 * sizeof(TU) + 15) / 16 * 16;   // bulk row buffers
+    static constexpr uint32_t RBE = (15 + 32 * sizeof(TE) + 15) / 16 * 16;
+    static constexpr uint32_t RBM = HAS_M ? (15 + 32 + 15) / 16 * 16 : 0;
+    static constexpr uint32_t ROWSET = 2 * RBU + RBE + 2 * RBM;              // one plane's rows
+    static constexpr size_t WARP_B = BULK ? size_t(D) * PL * ROWSET : (U_B + E_B + M_B + 15) / 16 * 16;
     static constexpr size_t HS_B = sizeof(P) * 2 * 6 * 32;                  // per row, two buffers
     static constexpr size_t BAR_OFF = NW * (WARP_B + HS_B);
-    static constexpr size_t BYTES = BAR_OFF + sizeof(uint64_t) * 4 * NW + 16;
+    static constexpr int NBARS = 4 * NW + (BULK ? NW * D : 0);
+    static constexpr size_t BYTES = BAR_OFF + sizeof(uint64_t) * NBARS + 16;
 };
 
-template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC>
+template <typename TC, typename TU, typename TE, typename TY, typename TR, int EPI, int MASK, bool CUBIC, bool BULK>
 __global__ void __launch_bounds__(WaveCfg<TC>::NW * 32, 1)
 parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __grid_constant__ WaveSched ws) {
     vx::pdl_begin();
     using Cfg = WaveCfg<TC>;
-    using L = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, CUBIC>;
+    using L = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, CUBIC, BULK>;
     constexpr int PL = Cfg::PL, NWW = Cfg::NW, D = Cfg::DEPTH, A = D - 2;
     using P = typename Cfg::P;
     using SU = stage_t<TU>;
@@ -201,13 +251,18 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
     uint32_t* sm = reinterpret_cast<uint32_t*>(wb + L::U_B + L::E_B);
     P* hs = reinterpret_cast<P*>(smem_raw + NWW * L::WARP_B);             // [NWW][2][6][32]
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + L::BAR_OFF);  // full[NWW][2], empty[NWW][2]
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 4 * NWW);
+    uint64_t* sbar = bars + 4 * NWW + row * D;                            // bulk staging: this row's slots
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + L::NBARS);
 #define SU_(s, h, c) su[(((s) * PL + (h)) * 6 + (c)) * 32 + lane]
 #define SE_(s, h) se[((s) * PL + (h)) * 32 + lane]
 #define SM_(s, h, w) sm[(((s) * PL + (h)) * 2 + (w)) * 32 + lane]
 #define HS_(r, b, k) hs[(((r) * 2 + (b)) * 6 + (k)) * 32 + lane]
     if (threadIdx.x < 4 * NWW) mbar_init(bars + threadIdx.x, 32);
+    if constexpr (BULK) {
+        if (threadIdx.x < NWW * D) mbar_init(bars + 4 * NWW + threadIdx.x, 1);
+    }
     if (threadIdx.x == 0) *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     __syncthreads();
 
     const int nyz_nodes = (g.ny + 1) * (g.nz + 1);
@@ -222,6 +277,8 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
         int item, j, steps, x0, x1;
         int cn_own, cn_nb, ce;        // clamped column offsets: own node, upper node, own element
         int iy, iz;
+        int lo, hi, elo, ehi;         // bulk rows: first and last node / element column of the tile
+        int row_o, row_u, row_e;      // their row offsets within a plane (own, upper node row; element row)
     };
     auto open = [&](Cursor& c, int item) {
         c.item = item;
@@ -238,6 +295,14 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
         c.cn_own = iyc * (g.nz + 1) + izc;
         c.cn_nb = iyn * (g.nz + 1) + izc;
         c.ce = min(max(c.iy, 0), g.ny - 1) * g.nz + min(max(c.iz, 0), g.nz - 1);
+        const int z0 = zt * WAVE_TZ;
+        c.lo = max(z0 - 1, 0);
+        c.hi = min(z0 + 30, g.nz);
+        c.elo = max(z0 - 1, 0);
+        c.ehi = min(z0 + 30, g.nz - 1);
+        c.row_o = iyc * (g.nz + 1);
+        c.row_u = iyn * (g.nz + 1);
+        c.row_e = min(max(c.iy, 0), g.ny - 1) * g.nz;
     };
     auto advance = [&](Cursor& c) {
         if (c.item >= ws.items) return;
@@ -264,14 +329,95 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
         }
     };
 
+    // bulk staging of step j of cursor c into slot s: lane 0 issues one bulk copy per row (an edge
+    // row near the array's end is copied by the lanes, each the values it will read)
+    unsigned char* wbulk = wb;
+    auto stage_bulk = [&](const Cursor& c, int s) {
+        __syncwarp();
+        fence_proxy_async();
+        const int ln = min(max(c.iz, c.lo), c.hi) - c.lo, le = min(max(c.iz, c.elo), c.ehi) - c.elo;
+        const int ncols = c.hi - c.lo + 1, necols = c.ehi - c.elo + 1;
+        auto spans = [&](int h, RowSpan* sp) {
+            const int q = min(max(c.x0 + PL * c.j + h, 0), g.nx);
+            const int qe = min(max(c.x0 + PL * c.j + h - 1, 0), g.nx - 1);
+            sp[0] = row_span(a.u, 3 * (q * nyz_nodes + c.row_o + c.lo), 3 * ncols, int(sizeof(TU)), 3 * n_nodes);
+            sp[1] = row_span(a.u, 3 * (q * nyz_nodes + c.row_u + c.lo), 3 * ncols, int(sizeof(TU)), 3 * n_nodes);
+            sp[2] = row_span(a.E, qe * nyz_elems + c.row_e + c.elo, necols, int(sizeof(TE)), n_elems);
+            if constexpr (HAS_M) {
+                sp[3] = row_span(a.node_mask, q * nyz_nodes + c.row_o + c.lo, ncols, 1, n_nodes);
+                sp[4] = row_span(a.node_mask, q * nyz_nodes + c.row_u + c.lo, ncols, 1, n_nodes);
+            }
+        };
+        constexpr int NR = HAS_M ? 5 : 3;
+        const uint32_t dst_off[5] = {0u, L::RBU, 2 * L::RBU, 2 * L::RBU + L::RBE, 2 * L::RBU + L::RBE + L::RBM};
+        uint32_t tx = 0;
+        #pragma unroll
+        for (int h = 0; h < PL; ++h) {
+            RowSpan sp[5];
+            spans(h, sp);
+            #pragma unroll
+            for (int r = 0; r < NR; ++r) tx += sp[r].bulk ? sp[r].len : 0u;
+        }
+        if (lane == 0) mbar_arrive_expect_tx(sbar + s, tx);
+        #pragma unroll
+        for (int h = 0; h < PL; ++h) {
+            RowSpan sp[5];
+            spans(h, sp);
+            unsigned char* rows = wbulk + (size_t(s) * PL + h) * L::ROWSET;
+            #pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                unsigned char* dst = rows + dst_off[r];
+                if (sp[r].bulk) {
+                    if (lane == 0) bulk_g2s(dst, sp[r].src, sp[r].len, sbar + s);
+                } else if (r < 2) {
+                    #pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int i = 3 * ln + k;
+                        reinterpret_cast<TU*>(dst + sp[r].off)[i] = reinterpret_cast<const TU*>(sp[r].src + sp[r].off)[i];
+                    }
+                } else if (r == 2) {
+                    reinterpret_cast<TE*>(dst + sp[r].off)[le] = reinterpret_cast<const TE*>(sp[r].src + sp[r].off)[le];
+                } else {
+                    dst[sp[r].off + ln] = sp[r].src[sp[r].off + ln];
+                }
+            }
+        }
+    };
+    // bulk fills issued and not yet waited for (bit per slot), and the phase parity of each slot's
+    // latest fill: what an aborting warp still has to wait for before its CTA may exit
+    unsigned pending = 0u, pend_par = 0u;
+    auto issue = [&](const Cursor& c, int t) {
+        const int s = t % D;
+        if constexpr (BULK) {
+            stage_bulk(c, s);
+            pending |= 1u << s;
+            pend_par = (pend_par & ~(1u << s)) | ((unsigned(t / D) & 1u) << s);
+        } else {
+            stage_step(c, s);
+        }
+    };
+    // this thread may read stream step t's slot: its own copies landed (cp.async), or the warp's
+    // bulk copies completed on the slot's barrier (phase = how often the slot was filled before)
+    auto wait_step = [&](int t) -> bool {
+        if constexpr (BULK) {
+            const int s = t % D;
+            const bool ok = mbar_wait(sbar + s, unsigned(t / D) & 1u, abort_flag);
+            if (ok) pending &= ~(1u << s);
+            return ok;
+        } else {
+            cp_async_wait<A>();
+            return true;
+        }
+    };
+
     Cursor prod, cons;
     open(prod, blockIdx.x);
     open(cons, blockIdx.x);
     // prefill: the first A steps of the stream go to slots 0 .. A-1
     #pragma unroll
     for (int t = 0; t < A; ++t) {
-        if (prod.item < ws.items) stage_step(prod, t);
-        cp_async_commit();
+        if (prod.item < ws.items) issue(prod, t);
+        if constexpr (!BULK) cp_async_commit();
         advance(prod);
     }
 
@@ -281,10 +427,10 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
     bool live = true;
     for (int t = 0; live && cons.item < ws.items; ++t) {
         // ---- producer: stream step t + A into its slot (an empty group past the end keeps the count)
-        if (prod.item < ws.items) stage_step(prod, (t + A) % D);
-        cp_async_commit();
+        if (prod.item < ws.items) issue(prod, t + A);
+        if constexpr (!BULK) cp_async_commit();
         advance(prod);
-        cp_async_wait<A>();                                  // this thread's copies of step t have landed
+        if (!wait_step(t)) { live = false; break; }         // step t's staging has landed
         if (cons.j < 0) {                                    // first step of an item: staging only
             #pragma unroll
             for (int k = 0; k < 3; ++k) carry[k] = TC(0);
@@ -326,15 +472,37 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
             const int s = h == 0 ? sp : sc, hh = h == 0 ? PL - 1 : h - 1;
             const int q = min(max(e + h, 0), g.nx);
             unsigned mo = 7u, mn = 7u;
-            if constexpr (HAS_M) {
-                mo = unstage<uint8_t>(SM_(s, hh, 0), a.node_mask + (q * nyz_nodes + cons.cn_own));
-                mn = unstage<uint8_t>(SM_(s, hh, 1), a.node_mask + (q * nyz_nodes + cons.cn_nb));
+            const TU* pvo;
+            const TU* pvn;
+            if constexpr (BULK) {
+                const unsigned char* rows = wbulk + (size_t(s) * PL + hh) * L::ROWSET;
+                const int ln = min(max(cons.iz, cons.lo), cons.hi) - cons.lo;
+                const int no = q * nyz_nodes + cons.row_o + cons.lo, nn = q * nyz_nodes + cons.row_u + cons.lo;
+                const uint32_t oo = uint32_t(3 * (no & 15) * int(sizeof(TU))) & 15u;
+                const uint32_t on = uint32_t(3 * (nn & 15) * int(sizeof(TU))) & 15u;
+                pvo = reinterpret_cast<const TU*>(rows + oo) + 3 * ln;
+                pvn = reinterpret_cast<const TU*>(rows + L::RBU + on) + 3 * ln;
+                if constexpr (HAS_M) {
+                    mo = rows[2 * L::RBU + L::RBE + (no & 15) + ln];
+                    mn = rows[2 * L::RBU + L::RBE + L::RBM + (nn & 15) + ln];
+                }
+            } else {
+                if constexpr (HAS_M) {
+                    mo = unstage<uint8_t>(SM_(s, hh, 0), a.node_mask + (q * nyz_nodes + cons.cn_own));
+                    mn = unstage<uint8_t>(SM_(s, hh, 1), a.node_mask + (q * nyz_nodes + cons.cn_nb));
+                }
             }
             bo[h] = mo;
             #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const TC vo = TC(Storage<TU>::cvt(unstage<TU>(SU_(s, hh, k), a.u)));
-                const TC vn = TC(Storage<TU>::cvt(unstage<TU>(SU_(s, hh, 3 + k), a.u)));
+                TC vo, vn;
+                if constexpr (BULK) {
+                    vo = TC(Storage<TU>::load(pvo + k));
+                    vn = TC(Storage<TU>::load(pvn + k));
+                } else {
+                    vo = TC(Storage<TU>::cvt(unstage<TU>(SU_(s, hh, k), a.u)));
+                    vn = TC(Storage<TU>::cvt(unstage<TU>(SU_(s, hh, 3 + k), a.u)));
+                }
                 if (h < PL) ur[h][k] = vo;
                 uo[h][k] = ((mo >> k) & 1u) ? vo : TC(0);
                 un[h][k] = ((mn >> k) & 1u) ? vn : TC(0);
@@ -345,7 +513,16 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
         #pragma unroll
         for (int h = 0; h < PL; ++h) {
             const int ex = e + h;
-            const TC val = TC(Storage<TE>::cvt(unstage<TE>(SE_(sc, h), a.E + (min(max(ex, 0), g.nx - 1) * nyz_elems + cons.ce))));
+            TC val;
+            if constexpr (BULK) {
+                const unsigned char* rows = wbulk + (size_t(sc) * PL + h) * L::ROWSET;
+                const int le = min(max(cons.iz, cons.elo), cons.ehi) - cons.elo;
+                const int first = min(max(ex, 0), g.nx - 1) * nyz_elems + cons.row_e + cons.elo;
+                const uint32_t oe = uint32_t((first & 15) * int(sizeof(TE))) & 15u;
+                val = TC(Storage<TE>::load(reinterpret_cast<const TE*>(rows + 2 * L::RBU + oe) + le));
+            } else {
+                val = TC(Storage<TE>::cvt(unstage<TE>(SE_(sc, h), a.E + (min(max(ex, 0), g.nx - 1) * nyz_elems + cons.ce))));
+            }
             ev[h] = (elem_ok && ex >= 0 && ex < g.nx) ? val : TC(0);
         }
         const P E = Cfg::pk(ev);
@@ -513,6 +690,17 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
         advance(cons);
     }
     cp_async_wait_all();
+    if constexpr (BULK) {
+        // after an abort, bulk copies issued for later steps may still be landing in this warp's
+        // slots: wait for them (bounded, ignoring the abort) before the CTA's shared memory goes away
+        for (int s = 0; s < D; ++s) {
+            if (!((pending >> s) & 1u)) continue;
+            const unsigned par = (pend_par >> s) & 1u;
+            bool ok = false;
+            for (int i = 0; i < WAVE_WAIT_LIMIT && !ok; ++i) ok = __all_sync(0xffffffffu, mbar_try_wait(sbar + s, par));
+            if (!ok && lane == 0) atomicExch(&g_wave_fault, 1);
+        }
+    }
     if constexpr (EPI == EPI_TRUE_RES || EPI == EPI_APPLY_DOT) {
         block_sum_store<NWW * 32>(acc, a.partials + blockIdx.x);
     }
