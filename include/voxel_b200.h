@@ -270,6 +270,27 @@ int vx_device_status(int* status, int clear);
 int64_t vx_coarse_factor_workspace(int n, int bw);
 int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* work, int* info, cudaStream_t stream);
 
+/* ---------------------------------------------------------------------------- batches
+ * `slots` independent systems of one size solved in lockstep (the serving loop's batches): slot k's
+ * vectors start k * stride entries after the given pointers, its scalars at S + 16 k, its partial
+ * sums at partials + k * 2 vx_solver_partials(n) (vx_batch_dots_pr) -- one launch for the whole batch.
+ * The single-system forms above are the one-slot case.  No counterpart in the reference (it solves
+ * one system at a time). */
+int vx_batch_finalize(int op, int64_t G, int slots, const double* partials, int64_t pstride, double* S,
+                      cudaStream_t stream);
+int vx_batch_cg_update(int prec, int64_t n, int slots, int64_t stride, const double* S, void* x, const void* p,
+                       void* r, const void* q, int update_r, cudaStream_t stream);
+int vx_batch_cg_direction(int zprec, int64_t n, int slots, int64_t stride, const double* S, const void* z, double* p,
+                          void* z_old, cudaStream_t stream);
+int vx_batch_dots_pr(int zprec, int64_t n, int slots, int64_t stride, const double* r, const void* zn, const void* zo,
+                     double* partials, cudaStream_t stream);
+/* vx_coarse_apply_factor for `slots` coarse systems of n DOFs: packed factors back to back (slot k at
+ * m + k n^2), slot k's right-hand side, node mask and solution at k * vs DOFs, y of slots * n doubles. */
+int vx_batch_coarse_apply_factor(int prec, int n, int slots, int64_t vs, const double* m, const void* r,
+                                 const uint8_t* node_mask, double* y, void* z, cudaStream_t stream);
+/* vx_graph_while_end whose loop runs while any of `slots` systems (scalars S + 16 k) is running. */
+int vx_batch_graph_while_end(void* handle, const double* S, int slots, cudaStream_t stream);
+
 /* res = b - A x and *norm2 = sum res^2 (a device double), like vx_true_residual followed by
  * vx_reduce_partials, but needing no scratch buffer from the caller: for code that may not
  * allocate device memory (a request loop that must never call cudaMalloc mid-flight, a plugin

@@ -13,7 +13,7 @@ from .operators import (Product, VoxelOperator, cast, dofs_from_node_mask, dots,
 from . import problems, solver, voxel_mg  # noqa: E402
 from .solver import FCGSolver, JacobiPCG, JacobiPreconditioner, MGHierarchy, PCGIR, SolveResult, hierarchy_shapes
 from .api import ElasticitySolver, clear_solver_cache, solve
-from . import donor, records, serving, simp, slab  # noqa: E402
+from . import batch, donor, records, serving, simp, slab  # noqa: E402
 from .simp import Compliance, ConeFilter, OCUpdater, compliance, oc_top88, run_simp
 from .slab import SlabComm, SlabSolver, slab_bounds
 
@@ -22,4 +22,4 @@ __all__ = ["XYZ", "Modal", "element", "quadrature", "edof_author", "element_node
            "node_mask_from_dofs", "product", "reduce_partials", "simp_modulus", "problems", "solver", "voxel_mg",
            "FCGSolver", "JacobiPCG", "JacobiPreconditioner", "MGHierarchy", "PCGIR", "SolveResult", "hierarchy_shapes",
            "ElasticitySolver", "clear_solver_cache", "solve", "simp", "Compliance", "ConeFilter", "OCUpdater", "compliance", "oc_top88",
-           "run_simp", "donor", "records", "serving", "slab", "SlabComm", "SlabSolver", "slab_bounds"]
+           "run_simp", "batch", "donor", "records", "serving", "slab", "SlabComm", "SlabSolver", "slab_bounds"]

@@ -214,12 +214,16 @@ __global__ void coarse_pack_kernel(int n, const double* __restrict__ linv, doubl
     }
 }
 
-// pass 1: y = Linv r (row i, columns 0..i of M), one CTA per row, FP64 accumulation
+// pass 1: y = Linv r (row i, columns 0..i of M), one CTA per row, FP64 accumulation.
+// Batches: system blockIdx.y has its factor at m + slot * n^2, its vectors at slot * vs, y at slot * n.
 template <typename TR>
 __global__ void __launch_bounds__(CT) coarse_lower_kernel(int n, const double* __restrict__ m,
-                                                          const TR* __restrict__ r, double* __restrict__ y) {
+                                                          const TR* __restrict__ r, double* __restrict__ y, int64_t vs) {
     vx::pdl_begin();
     const int row = blockIdx.x;
+    m += int64_t(n) * n * blockIdx.y;
+    r += vs * blockIdx.y;
+    y += int64_t(n) * blockIdx.y;
     const double s = block_row_dot(m + int64_t(row) * n, 0, row + 1, [&](int j) { return double(Storage<TR>::load(r + j)); });
     if (threadIdx.x == 0) y[row] = s;
 }
@@ -228,10 +232,14 @@ __global__ void __launch_bounds__(CT) coarse_lower_kernel(int n, const double* _
 template <typename T>
 __global__ void __launch_bounds__(CT) coarse_upper_kernel(int n, const double* __restrict__ m,
                                                           const double* __restrict__ y,
-                                                          const uint8_t* __restrict__ mask, T* __restrict__ z) {
+                                                          const uint8_t* __restrict__ mask, T* __restrict__ z, int64_t vs) {
     vx::pdl_begin();
     using A = arith_t<T>;
     const int row = blockIdx.x;
+    m += int64_t(n) * n * blockIdx.y;
+    y += int64_t(n) * blockIdx.y;
+    z += vs * blockIdx.y;
+    if (mask) mask += (vs / 3) * blockIdx.y;
     const double s = block_row_dot(m + int64_t(row) * n, row, n, [&](int j) { return y[j]; });
     if (threadIdx.x == 0) {
         const bool fr = mask ? ((mask[row / 3] >> (row % 3)) & 1u) : true;
@@ -380,10 +388,29 @@ extern "C" int vx_coarse_apply_factor(int prec, int n, const double* m, const vo
     const bool ok = dispatch_prec(prec, [&](auto t) {             // r auxiliary, z an iterate
         using R = typename decltype(t)::R;
         using X = typename decltype(t)::X;
-        vx::launch(coarse_lower_kernel<R>, unsigned(n), CT, 0, stream, n, m, (const R*)r, y);
-        vx::launch(coarse_upper_kernel<X>, unsigned(n), CT, 0, stream, n, m, y, node_mask, (X*)z);
+        vx::launch(coarse_lower_kernel<R>, unsigned(n), CT, 0, stream, n, m, (const R*)r, y, int64_t(0));
+        vx::launch(coarse_upper_kernel<X>, unsigned(n), CT, 0, stream, n, m, y, node_mask, (X*)z, int64_t(0));
     });
     VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_coarse_apply_factor: unsupported precision %d", prec);
     VX_CHECK_LAUNCH("vx_coarse_apply_factor");
+    return VX_OK;
+}
+
+// The same for `slots` independent coarse systems: factors back to back (slot k at m + k n^2), the
+// right-hand side, mask and solution of slot k at k * vs DOFs (vs a multiple of 3), y holding
+// slots * n doubles.
+extern "C" int vx_batch_coarse_apply_factor(int prec, int n, int slots, int64_t vs, const double* m, const void* r,
+                                            const uint8_t* node_mask, double* y, void* z, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0 && slots >= 1 && slots <= 65535 && vs >= n && vs % 3 == 0, VX_ERR_INVALID_ARGUMENT,
+                 "vx_batch_coarse_apply_factor: bad n/slots/stride");
+    VX_CHECK_ARG(m && r && y && z, VX_ERR_NULL_POINTER, "vx_batch_coarse_apply_factor: NULL pointer");
+    const bool ok = dispatch_prec(prec, [&](auto t) {
+        using R = typename decltype(t)::R;
+        using X = typename decltype(t)::X;
+        vx::launch(coarse_lower_kernel<R>, dim3(n, slots), CT, 0, stream, n, m, (const R*)r, y, vs);
+        vx::launch(coarse_upper_kernel<X>, dim3(n, slots), CT, 0, stream, n, m, y, node_mask, (X*)z, vs);
+    });
+    VX_CHECK_ARG(ok, VX_ERR_INVALID_ARGUMENT, "vx_batch_coarse_apply_factor: unsupported precision %d", prec);
+    VX_CHECK_LAUNCH("vx_batch_coarse_apply_factor");
     return VX_OK;
 }

@@ -45,9 +45,13 @@ __device__ double block_sum_ft(double v) {
     return s;
 }
 
+// Slot blockIdx.y (a batch of independent systems solved in lockstep) uses S + 16 slot and
+// partials + slot * pstride; unbatched launches have one slot.
 __global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const double* __restrict__ partials,
-                                                      double* __restrict__ S) {
+                                                      double* __restrict__ S, int64_t pstride) {
     vx::pdl_begin();
+    S += S_COUNT * int64_t(blockIdx.y);
+    partials += pstride * int64_t(blockIdx.y);
     double s0 = 0.0, s1 = 0.0;
     for (int64_t j = threadIdx.x; j < G; j += FT) s0 += partials[j];
     s0 = block_sum_ft(s0);
@@ -94,12 +98,18 @@ __global__ void __launch_bounds__(FT) finalize_kernel(int op, int64_t G, const d
 
 // x += alpha p; r -= alpha q (r update skipped when it is about to be replaced by b - A x).
 // Nothing moves once the loop has converged or broken down.
+// Vector kernels of a batch: slot blockIdx.y works on its n entries at slot * vs and on S + 16 slot.
 template <typename T>
 __global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __restrict__ x, const T* __restrict__ p,
-                                 T* __restrict__ r, const T* __restrict__ q, int update_r) {
+                                 T* __restrict__ r, const T* __restrict__ q, int update_r, int64_t vs) {
     vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int64_t o = vs * int64_t(blockIdx.y);
+    S += S_COUNT * int64_t(blockIdx.y);
+    x += o;
+    p += o;
+    if (update_r) { r += o; q += o; }
     if (S[S_DONE] != 0.0 || S[S_BREAK] != 0.0) return;
     const T a = T(S[S_ALPHA]);
     x[i] = x[i] + a * p[i];
@@ -110,10 +120,15 @@ __global__ void cg_update_kernel(int64_t n, const double* __restrict__ S, T* __r
 // (a copy in z's own type is exact and moves half the bytes of an FP64 copy of an FP32 z)
 template <typename T, typename TZ>
 __global__ void cg_direction_kernel(int64_t n, const double* __restrict__ S, const TZ* __restrict__ z, T* __restrict__ p,
-                                    TZ* __restrict__ z_old) {
+                                    TZ* __restrict__ z_old, int64_t vs) {
     vx::pdl_begin();
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int64_t o = vs * int64_t(blockIdx.y);
+    S += S_COUNT * int64_t(blockIdx.y);
+    z += o;
+    p += o;
+    if (z_old) z_old += o;
     const TZ zr = z[i];
     p[i] = T(Storage<TZ>::cvt(zr)) + T(S[S_BETA]) * p[i];
     if (z_old) z_old[i] = zr;
@@ -135,11 +150,19 @@ __global__ void cg_direction_update_kernel(int64_t n, const double* __restrict__
 }
 
 // partials for r . zn and r . (zn - zo), fixed grid G (a function of n), fixed order
+// (slot blockIdx.y: vectors at slot * vs, partials at slot * 2G)
 template <typename T, typename TZ>
 __global__ void __launch_bounds__(FT) dots_pr_kernel(int64_t n, const T* __restrict__ r, const TZ* __restrict__ zn,
-                                                     const TZ* __restrict__ zo, double* __restrict__ partials) {
+                                                     const TZ* __restrict__ zo, double* __restrict__ partials, int64_t vs) {
     vx::pdl_begin();
     const int64_t G = gridDim.x;
+    {
+        const int64_t o = vs * int64_t(blockIdx.y);
+        r += o;
+        zn += o;
+        if (zo) zo += o;
+        partials += 2 * G * int64_t(blockIdx.y);
+    }
     double a = 0.0, b = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * FT + threadIdx.x; i < n; i += G * FT) {
         const double ri = double(r[i]), zi = double(Storage<TZ>::load(zn + i));
@@ -221,11 +244,16 @@ __global__ void set_scalars_kernel(double* S, int first, int count, double value
     if (i < count) S[first + i] = value;
 }
 
-__global__ void condition_kernel(cudaGraphConditionalHandle h, const double* __restrict__ S) {
+// Another loop body runs while any of the `slots` systems is still running.
+__global__ void condition_kernel(cudaGraphConditionalHandle h, const double* __restrict__ S, int slots) {
     vx::pdl_begin();
     if (threadIdx.x == 0) {
-        // S[S_CHECK] = iterations per loop body: the next body must not pass maxiter
-        const bool go = S[S_DONE] == 0.0 && S[S_BREAK] == 0.0 && S[S_IT] + S[S_CHECK] <= S[S_MAXIT];
+        bool go = false;
+        for (int k = 0; k < slots; ++k) {
+            const double* s = S + S_COUNT * k;
+            // S[S_CHECK] = iterations per loop body: the next body must not pass maxiter
+            go = go || (s[S_DONE] == 0.0 && s[S_BREAK] == 0.0 && s[S_IT] + s[S_CHECK] <= s[S_MAXIT]);
+        }
         cudaGraphSetConditional(h, go ? 1u : 0u);
     }
 }
@@ -255,7 +283,7 @@ extern "C" int64_t vx_solver_partials(int64_t n) { return fixed_ctas(n); }
 extern "C" int vx_solver_finalize(int op, int64_t G, const double* partials, double* S, cudaStream_t stream) {
     VX_CHECK_ARG(op >= 0 && op <= FIN_RR_ONLY && G > 0, VX_ERR_INVALID_ARGUMENT, "vx_solver_finalize: bad op/G");
     VX_CHECK_ARG(partials && S, VX_ERR_NULL_POINTER, "vx_solver_finalize: NULL pointer");
-    vx::launch(finalize_kernel, 1, FT, 0, stream, op, G, partials, S);
+    vx::launch(finalize_kernel, 1, FT, 0, stream, op, G, partials, S, int64_t(0));
     VX_CHECK_LAUNCH("vx_solver_finalize");
     return VX_OK;
 }
@@ -266,10 +294,10 @@ extern "C" int vx_cg_update(int prec, int64_t n, const double* S, void* x, const
     VX_CHECK_ARG(S && x && p && (!update_r || (r && q)), VX_ERR_NULL_POINTER, "vx_cg_update: NULL pointer");
     if (prec == VX_F64)
         vx::launch(cg_update_kernel<double>, nb(n, 256), 256, 0, stream, n, S, (double*)x, (const double*)p, (double*)r,
-                                                                 (const double*)q, update_r);
+                                                                 (const double*)q, update_r, int64_t(0));
     else if (prec == VX_F32)
         vx::launch(cg_update_kernel<float>, nb(n, 256), 256, 0, stream, n, S, (float*)x, (const float*)p, (float*)r,
-                                                                (const float*)q, update_r);
+                                                                (const float*)q, update_r, int64_t(0));
     else { set_error("vx_cg_update: unsupported precision %d", prec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cg_update");
     return VX_OK;
@@ -280,14 +308,14 @@ extern "C" int vx_cg_direction(int prec, int zprec, int64_t n, const double* S, 
     VX_CHECK_ARG(n > 0, VX_ERR_INVALID_ARGUMENT, "vx_cg_direction: n must be positive");
     VX_CHECK_ARG(S && z && p, VX_ERR_NULL_POINTER, "vx_cg_direction: NULL pointer");
     if (prec == VX_F64 && zprec == VX_F64)
-        vx::launch(cg_direction_kernel<double, double>, nb(n, 256), 256, 0, stream, n, S, (const double*)z, (double*)p, (double*)z_old);
+        vx::launch(cg_direction_kernel<double, double>, nb(n, 256), 256, 0, stream, n, S, (const double*)z, (double*)p, (double*)z_old, int64_t(0));
     else if (prec == VX_F64 && zprec == VX_F32)
-        vx::launch(cg_direction_kernel<double, float>, nb(n, 256), 256, 0, stream, n, S, (const float*)z, (double*)p, (float*)z_old);
+        vx::launch(cg_direction_kernel<double, float>, nb(n, 256), 256, 0, stream, n, S, (const float*)z, (double*)p, (float*)z_old, int64_t(0));
     else if (prec == VX_F64 && zprec == VX_BF16_F32)
         vx::launch(cg_direction_kernel<double, __nv_bfloat16>, nb(n, 256), 256, 0, stream, n, S, (const __nv_bfloat16*)z, (double*)p,
-                                                                                   (__nv_bfloat16*)z_old);
+                                                                                   (__nv_bfloat16*)z_old, int64_t(0));
     else if (prec == VX_F32 && zprec == VX_F32)
-        vx::launch(cg_direction_kernel<float, float>, nb(n, 256), 256, 0, stream, n, S, (const float*)z, (float*)p, (float*)z_old);
+        vx::launch(cg_direction_kernel<float, float>, nb(n, 256), 256, 0, stream, n, S, (const float*)z, (float*)p, (float*)z_old, int64_t(0));
     else { set_error("vx_cg_direction: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_cg_direction");
     return VX_OK;
@@ -312,14 +340,14 @@ extern "C" int vx_dots_pr(int prec, int zprec, int64_t n, const void* r, const v
     VX_CHECK_ARG(r && zn && partials, VX_ERR_NULL_POINTER, "vx_dots_pr: NULL pointer");
     const unsigned G = unsigned(fixed_ctas(n));
     if (prec == VX_F64 && zprec == VX_F64)
-        vx::launch(dots_pr_kernel<double, double>, G, FT, 0, stream, n, (const double*)r, (const double*)zn, (const double*)zo, partials);
+        vx::launch(dots_pr_kernel<double, double>, G, FT, 0, stream, n, (const double*)r, (const double*)zn, (const double*)zo, partials, int64_t(0));
     else if (prec == VX_F64 && zprec == VX_F32)
-        vx::launch(dots_pr_kernel<double, float>, G, FT, 0, stream, n, (const double*)r, (const float*)zn, (const float*)zo, partials);
+        vx::launch(dots_pr_kernel<double, float>, G, FT, 0, stream, n, (const double*)r, (const float*)zn, (const float*)zo, partials, int64_t(0));
     else if (prec == VX_F64 && zprec == VX_BF16_F32)
         vx::launch(dots_pr_kernel<double, __nv_bfloat16>, G, FT, 0, stream, n, (const double*)r, (const __nv_bfloat16*)zn,
-                                                                    (const __nv_bfloat16*)zo, partials);
+                                                                    (const __nv_bfloat16*)zo, partials, int64_t(0));
     else if (prec == VX_F32 && zprec == VX_F32)
-        vx::launch(dots_pr_kernel<float, float>, G, FT, 0, stream, n, (const float*)r, (const float*)zn, (const float*)zo, partials);
+        vx::launch(dots_pr_kernel<float, float>, G, FT, 0, stream, n, (const float*)r, (const float*)zn, (const float*)zo, partials, int64_t(0));
     else { set_error("vx_dots_pr: unsupported precisions %d/%d", prec, zprec); return VX_ERR_INVALID_ARGUMENT; }
     VX_CHECK_LAUNCH("vx_dots_pr");
     return VX_OK;
@@ -429,10 +457,11 @@ extern "C" int vx_graph_while_begin(cudaStream_t stream, void** handle) {
     return VX_OK;
 }
 
-extern "C" int vx_graph_while_end(void* handle, const double* S, cudaStream_t stream) {
+static int graph_while_end(void* handle, const double* S, int slots, cudaStream_t stream) {
     VX_CHECK_ARG(handle && S, VX_ERR_NULL_POINTER, "vx_graph_while_end: NULL pointer");
+    VX_CHECK_ARG(slots >= 1, VX_ERR_INVALID_ARGUMENT, "vx_graph_while_end: slots must be positive");
     auto* w = static_cast<WhileGraph*>(handle);
-    vx::launch(condition_kernel, 1, 32, 0, stream, w->handle, S);
+    vx::launch(condition_kernel, 1, 32, 0, stream, w->handle, S, slots);
     cudaError_t e = cudaGetLastError();
     cudaGraph_t captured = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(stream, &captured);
@@ -442,6 +471,71 @@ extern "C" int vx_graph_while_end(void* handle, const double* S, cudaStream_t st
         set_error("vx_graph_while_end: %s", cudaGetErrorString(e));
         return VX_ERR_CUDA;
     }
+    return VX_OK;
+}
+
+extern "C" int vx_graph_while_end(void* handle, const double* S, cudaStream_t stream) {
+    return graph_while_end(handle, S, 1, stream);
+}
+
+// The batch form: the loop runs while any of `slots` systems (scalars S + 16 k) is running.
+extern "C" int vx_batch_graph_while_end(void* handle, const double* S, int slots, cudaStream_t stream) {
+    return graph_while_end(handle, S, slots, stream);
+}
+
+// ----------------------------------------------------------------------------- batches
+// `slots` independent systems of n unknowns, slot k's vectors at k * stride, scalars at S + 16 k:
+// the kernels above with the slot in blockIdx.y (one launch for the whole batch).
+extern "C" int vx_batch_finalize(int op, int64_t G, int slots, const double* partials, int64_t pstride, double* S,
+                                 cudaStream_t stream) {
+    VX_CHECK_ARG(op >= 0 && op <= FIN_RR_ONLY && G > 0 && slots >= 1 && slots <= 65535, VX_ERR_INVALID_ARGUMENT,
+                 "vx_batch_finalize: bad op/G/slots");
+    VX_CHECK_ARG(partials && S, VX_ERR_NULL_POINTER, "vx_batch_finalize: NULL pointer");
+    vx::launch(finalize_kernel, dim3(1, slots), FT, 0, stream, op, G, partials, S, pstride);
+    VX_CHECK_LAUNCH("vx_batch_finalize");
+    return VX_OK;
+}
+
+extern "C" int vx_batch_cg_update(int prec, int64_t n, int slots, int64_t stride, const double* S, void* x,
+                                  const void* p, void* r, const void* q, int update_r, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0 && slots >= 1 && slots <= 65535, VX_ERR_INVALID_ARGUMENT, "vx_batch_cg_update: bad n/slots");
+    VX_CHECK_ARG(S && x && p && (!update_r || (r && q)), VX_ERR_NULL_POINTER, "vx_batch_cg_update: NULL pointer");
+    VX_CHECK_ARG(prec == VX_F64, VX_ERR_INVALID_ARGUMENT, "vx_batch_cg_update: unsupported precision %d", prec);
+    vx::launch(cg_update_kernel<double>, dim3(nb(n, 256), slots), 256, 0, stream, n, S, (double*)x, (const double*)p,
+               (double*)r, (const double*)q, update_r, stride);
+    VX_CHECK_LAUNCH("vx_batch_cg_update");
+    return VX_OK;
+}
+
+extern "C" int vx_batch_cg_direction(int zprec, int64_t n, int slots, int64_t stride, const double* S, const void* z,
+                                     double* p, void* z_old, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0 && slots >= 1 && slots <= 65535, VX_ERR_INVALID_ARGUMENT, "vx_batch_cg_direction: bad n/slots");
+    VX_CHECK_ARG(S && z && p, VX_ERR_NULL_POINTER, "vx_batch_cg_direction: NULL pointer");
+    if (zprec == VX_F64)
+        vx::launch(cg_direction_kernel<double, double>, dim3(nb(n, 256), slots), 256, 0, stream, n, S, (const double*)z, p,
+                   (double*)z_old, stride);
+    else if (zprec == VX_F32)
+        vx::launch(cg_direction_kernel<double, float>, dim3(nb(n, 256), slots), 256, 0, stream, n, S, (const float*)z, p,
+                   (float*)z_old, stride);
+    else { set_error("vx_batch_cg_direction: unsupported precision %d", zprec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_batch_cg_direction");
+    return VX_OK;
+}
+
+// per-slot partials of r . zn (and r . (zn - zo)) at slot * 2 vx_solver_partials(n)
+extern "C" int vx_batch_dots_pr(int zprec, int64_t n, int slots, int64_t stride, const double* r, const void* zn,
+                                const void* zo, double* partials, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0 && slots >= 1 && slots <= 65535, VX_ERR_INVALID_ARGUMENT, "vx_batch_dots_pr: bad n/slots");
+    VX_CHECK_ARG(r && zn && partials, VX_ERR_NULL_POINTER, "vx_batch_dots_pr: NULL pointer");
+    const unsigned G = unsigned(fixed_ctas(n));
+    if (zprec == VX_F64)
+        vx::launch(dots_pr_kernel<double, double>, dim3(G, slots), FT, 0, stream, n, r, (const double*)zn,
+                   (const double*)zo, partials, stride);
+    else if (zprec == VX_F32)
+        vx::launch(dots_pr_kernel<double, float>, dim3(G, slots), FT, 0, stream, n, r, (const float*)zn,
+                   (const float*)zo, partials, stride);
+    else { set_error("vx_batch_dots_pr: unsupported precision %d", zprec); return VX_ERR_INVALID_ARGUMENT; }
+    VX_CHECK_LAUNCH("vx_batch_dots_pr");
     return VX_OK;
 }
 

@@ -80,7 +80,10 @@ class MGHierarchy:
     coarsest solve accumulates in FP64 either way."""
 
     def __init__(self, shape, ke, E, node_mask=None, dtype=torch.float32, pre=2, post=2, omegas=None,
-                 max_coarse_x=16, shapes=None, aux_dtype=None):
+                 max_coarse_x=16, shapes=None, aux_dtype=None, coarse_blocks=None):
+        """coarse_blocks = B: the grid is B jobs stacked along x with one zero-modulus element layer
+        between neighbours at the coarsest level (see batch.BatchedSolver); the coarsest level is then
+        B independent dense systems, each with its own factor, solved by one batched launch."""
         aux_dtype = dtype if aux_dtype is None else aux_dtype
         if (dtype, aux_dtype) not in STORAGE:
             raise ValueError(f"unsupported V-cycle storage: iterate {dtype}, auxiliary {aux_dtype}")
@@ -115,17 +118,32 @@ class MGHierarchy:
             L.res = None if aux_dtype == dtype else torch.zeros(L.n, dtype=aux_dtype, device="cuda")
             self.levels.append(L)
         c = self.levels[-1]
-        A = torch.empty(c.n, c.n, dtype=torch.float64, device="cuda")
-        _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
-                  _ptr(c.E64, "E"), _ptr(c.mask, "mask"), A.data_ptr(), _s())
-        self.A_coarse = A
-        self.coarse_packed = torch.empty_like(A)              # tril(L^-1) + triu(L^-T, 1)
-        self._coarse_y = torch.zeros(c.n, dtype=torch.float64, device="cuda")
+        self.blocks = int(coarse_blocks) if coarse_blocks else 0
+        if self.blocks:
+            nxc, nyc, nzc = c.shape
+            if (nxc + 1) % self.blocks:
+                raise ValueError(f"coarsest grid {c.shape} does not split into {self.blocks} jobs")
+            pc = (nxc + 1) // self.blocks                       # job pitch: nx_job + 1 separator element
+            self.job_coarse = (pc - 1, nyc, nzc)
+            nb_ = 3 * pc * (nyc + 1) * (nzc + 1)
+            self.A_coarse = torch.empty(self.blocks, nb_, nb_, dtype=torch.float64, device="cuda")
+            self._coarse_y = torch.zeros(self.blocks * nb_, dtype=torch.float64, device="cuda")
+            self.coarse_packed = torch.empty_like(self.A_coarse)
+            self._factor_info = torch.zeros(self.blocks, dtype=torch.int32, device="cuda")
+            for k in range(self.blocks):
+                self._assemble_block(k)
+        else:
+            A = torch.empty(c.n, c.n, dtype=torch.float64, device="cuda")
+            _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
+                      _ptr(c.E64, "E"), _ptr(c.mask, "mask"), A.data_ptr(), _s())
+            self.A_coarse = A
+            self.coarse_packed = torch.empty_like(A)              # tril(L^-1) + triu(L^-T, 1)
+            self._coarse_y = torch.zeros(c.n, dtype=torch.float64, device="cuda")
         # the same calls as update_modulus, so a refreshed pooled hierarchy and a fresh one are
         # bitwise identical; the factorisation is checked once here (the check synchronises)
         info = self._coarse_inverse()
-        if int(info) != 0:
-            raise ValueError(f"coarsest-level matrix is not positive definite (cholesky info {int(info)})")
+        if int(info.abs().max()) != 0:
+            raise ValueError(f"coarsest-level matrix is not positive definite (cholesky info {info.tolist()})")
         n_smooth = len(self.levels) - 1
         if omegas is None:
             self.omegas = [0.6] * n_smooth                      # the reference default (voxel_mg.py:148)
@@ -173,11 +191,30 @@ class MGHierarchy:
             inv64 = L.op64.diagonal(L.E64, L.mask, inverse=True)
             L.invd.copy_(inv64)
         c = self.levels[-1]
-        _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
-                  c.E64.data_ptr(), c.mask.data_ptr(), self.A_coarse.data_ptr(), _s())
+        if self.blocks:
+            for k in range(self.blocks):
+                self._assemble_block(k)
+        else:
+            _lib.call("vx_assemble_dense", *c.shape, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
+                      c.E64.data_ptr(), c.mask.data_ptr(), self.A_coarse.data_ptr(), _s())
         # no error check here (it would synchronise the stream); a non-SPD coarse matrix shows up as a
         # non-finite residual and a non-converged solve
         self._coarse_inverse()
+
+    def _assemble_block(self, k):
+        """Coarsest dense matrix of stacked job k (from its own segment of the coarsest moduli and mask)."""
+        c = self.levels[-1]
+        nx, ny, nz = self.job_coarse
+        pc = nx + 1
+        E_off = k * pc * ny * nz
+        m_off = k * pc * (ny + 1) * (nz + 1)
+        _lib.call("vx_assemble_dense", nx, ny, nz, _lib.dptr(np.ascontiguousarray(self.ke * 2 ** (len(self.shapes) - 1))),
+                  c.E64.data_ptr() + 8 * E_off, c.mask.data_ptr() + m_off, self.A_coarse[k].data_ptr(), _s())
+
+    def refresh_block(self, k):
+        """Re-assemble and re-factor stacked job k's coarsest system (after its moduli changed)."""
+        self._assemble_block(k)
+        self._factor_block(k)
 
     def _coarse_inverse(self):
         """Factor the coarsest matrix A = L L^T (FP64 Cholesky) and pack L^-1 with its transpose for
@@ -187,6 +224,10 @@ class MGHierarchy:
         a dense Cholesky and a recursive block inversion instead.  Everything is queued on the current
         stream without a host synchronisation.  Returns the factorisation's device-side info tensor
         (0 when A is positive definite)."""
+        if self.blocks:
+            for k in range(self.blocks):
+                self._factor_block(k)
+            return self._factor_info
         n = self.A_coarse.shape[0]
         nx, ny, nz = self.levels[-1].shape
         bw = min(n - 1, 3 * ((ny + 1) * (nz + 1) + (nz + 1) + 1) + 2)
@@ -205,6 +246,16 @@ class MGHierarchy:
         linv = _lower_inverse(factor).contiguous()                  # the kernel reads it row-major
         _lib.call("vx_coarse_pack", linv.shape[0], linv.data_ptr(), self.coarse_packed.data_ptr(), _s())
         return info
+
+    def _factor_block(self, k):
+        n = self.A_coarse.shape[1]
+        nx, ny, nz = self.job_coarse
+        bw = min(n - 1, 3 * ((ny + 1) * (nz + 1) + (nz + 1) + 1) + 2)
+        if getattr(self, "_factor_work", None) is None:
+            self._factor_work = torch.empty(int(_lib.load().vx_coarse_factor_workspace(n, bw)), dtype=torch.float64,
+                                            device="cuda")
+        _lib.call("vx_coarse_factor", n, bw, self.A_coarse[k].data_ptr(), self.coarse_packed[k].data_ptr(),
+                  self._factor_work.data_ptr(), self._factor_info[k:k + 1].data_ptr(), _s())
 
     def footprint_bytes(self) -> int:
         b = 0
@@ -251,9 +302,7 @@ class MGHierarchy:
             if self.aux_dtype != torch.float64:
                 _lib.call("vx_cast", L0.n, _lib.VX_F64, _ptr(r64, "r"), PREC[self.aux_dtype], L0.r.data_ptr(), 1.0, _s())
                 src = L0.r
-            _lib.call("vx_coarse_apply_factor", self.prec, L0.n, self.coarse_packed.data_ptr(), src.data_ptr(),
-                      L0.mask.data_ptr(), self._coarse_y.data_ptr(),
-                      L0.x.data_ptr(), _s())
+            self._coarse_apply(L0, src)
             return L0.x
         r0 = r64 if self.dtype == torch.float64 else L0.r
         r_mg = None if self.dtype == torch.float64 else L0.r.data_ptr()
@@ -269,9 +318,7 @@ class MGHierarchy:
     def _level(self, l, r):
         L = self.levels[l]
         if l == len(self.levels) - 1:
-            _lib.call("vx_coarse_apply_factor", self.prec, L.n, self.coarse_packed.data_ptr(), r.data_ptr(),
-                      L.mask.data_ptr(), self._coarse_y.data_ptr(),
-                      L.x.data_ptr(), _s())
+            self._coarse_apply(L, r)
             return L.x
         bufs = [L.x, L.xt]
         ci = 0
@@ -291,6 +338,15 @@ class MGHierarchy:
             L.op.jacobi(bufs[ci], r, L.invd, L.E, L.mask, L.omega, out=bufs[1 - ci])
             ci ^= 1
         return bufs[ci]
+
+    def _coarse_apply(self, L, r):
+        if self.blocks:
+            nb_ = self.A_coarse.shape[1]
+            _lib.call("vx_batch_coarse_apply_factor", self.prec, nb_, self.blocks, nb_, self.coarse_packed.data_ptr(),
+                      r.data_ptr(), L.mask.data_ptr(), self._coarse_y.data_ptr(), L.x.data_ptr(), _s())
+        else:
+            _lib.call("vx_coarse_apply_factor", self.prec, L.n, self.coarse_packed.data_ptr(), r.data_ptr(),
+                      L.mask.data_ptr(), self._coarse_y.data_ptr(), L.x.data_ptr(), _s())
 
     def __call__(self, r64):
         """z = M(r) as a fresh FP64 tensor (the reference's Multigrid.__call__ casts back to r's dtype)."""
