@@ -308,3 +308,113 @@ def request_stream(n=256, shapes=((48, 24, 24), (96, 48, 48), (160, 80, 80), (25
         s = shapes[rng.integers(len(shapes))]
         reqs.append(Request(i, s, dens[s][rng.integers(densities_per_shape)], float(tols[rng.integers(len(tols))]), t))
     return reqs
+
+
+# ------------------------------------------------------------------------------ batched serving
+def default_slots(shape, max_slots=16, dofs_per_batch=32e6):
+    """Slots of a shape's batch: as many jobs as fit about `dofs_per_batch` stacked DOFs, at most max_slots."""
+    nx, ny, nz = shape
+    per = 3.0 * (nx + 1) * (ny + 1) * (nz + 1)
+    return int(max(1, min(max_slots, dofs_per_batch // per)))
+
+
+def serve_batched(requests, shapes=None, slots=None, precision="mixed", chunk=4, maxiter=200, budget_bytes=150e9,
+                  prewarm=None, keep_solution=False, clock=time.perf_counter, poll_s=50e-6):
+    """Continuous batching with fused launches: one batch.BatchedSolver per grid shape (its own stream
+    and captured chunk graph) holds up to slots[shape] jobs; every kernel of a chunk serves all the
+    shape's jobs at once.  Requests are admitted FIFO per shape into free slots between chunks,
+    finished jobs leave their slot at once, and the shapes' batches run concurrently.  A shape's
+    batch is built on its first request unless listed in `prewarm` (default: every shape), so a
+    cold shape pays its set-up inside the stream.  The batches' footprint must fit the budget.
+    Returns (completions sorted by request id, summary)."""
+    import torch
+    from .batch import BatchedSolver
+    from .problems import cantilever_equal_split, simp_modulus
+    shapes = sorted({tuple(r.shape) for r in requests} if shapes is None else {tuple(s) for s in shapes})
+    slots = {s: (slots or {}).get(s, default_slots(s)) for s in shapes}
+    prewarm = set(shapes) if prewarm is None else {tuple(s) for s in prewarm}
+    forces = {s: cantilever_equal_split(s)[1] for s in shapes}
+    solvers, used = {}, 0.0
+
+    def build(shape):
+        nonlocal used
+        bs = BatchedSolver(shape, slots[shape], precision=precision, chunk=chunk, maxiter=maxiter)
+        used += bs.footprint_bytes()
+        if used > budget_bytes:
+            raise ValueError(f"batches need {used / 1e9:.1f} GB, over the {budget_bytes / 1e9:.0f} GB budget")
+        # one throw-away job captures the chunk graph before any request is timed on it
+        E1 = torch.ones(shape[0] * shape[1] * shape[2], dtype=torch.float64, device="cuda")
+        bs.solve([(E1, forces[shape], 1e-2)])
+        bs.retire(0)
+        solvers[shape] = bs
+        return bs
+
+    for s in shapes:
+        if s in prewarm:
+            build(s)
+    torch.cuda.synchronize()
+    pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
+    active = {s: {} for s in shapes}             # shape -> slot -> (request, admitted time)
+    inflight = {s: False for s in shapes}
+    done = []
+    peak = 0
+    t0 = clock()
+    while pending or any(active.values()):
+        now = clock() - t0
+        progressed = False
+        # admission: arrived requests into free slots of their shape (FIFO per shape)
+        joins = {}
+        still = deque()
+        while pending and pending[0].arrival <= now:
+            r = pending.popleft()
+            s = tuple(r.shape)
+            free = slots[s] - len(active[s]) - len(joins.get(s, []))
+            if free > 0 and not inflight[s]:
+                joins.setdefault(s, []).append(r)
+            else:
+                still.append(r)
+        pending.extendleft(reversed(still))
+        for s, rs in joins.items():
+            bs = solvers.get(s) or build(s)
+            free_slots = [k for k in range(slots[s]) if k not in active[s]]
+            jobs = []
+            for k, r in zip(free_slots, rs):
+                rho = r.density if isinstance(r.density, torch.Tensor) else torch.as_tensor(r.density)
+                E = simp_modulus(rho.to("cuda", torch.float64), 1e-9)
+                jobs.append((k, E, forces[s], r.tol))
+                active[s][k] = (r, clock() - t0)
+            bs.admit(jobs)
+            progressed = True
+        peak = max(peak, sum(len(a) for a in active.values()))
+        # launch a chunk for every shape with jobs and nothing in flight
+        for s in shapes:
+            if active[s] and not inflight[s]:
+                solvers[s].run()
+                inflight[s] = True
+                progressed = True
+        # completion
+        for s in shapes:
+            if inflight[s] and solvers[s].ready():
+                inflight[s] = False
+                bs = solvers[s]
+                fin, *_ = bs.poll()
+                for k in list(active[s]):
+                    if fin[k]:
+                        r, adm = active[s].pop(k)
+                        x, it, ok, rel, comp = bs.result(k)
+                        bs.retire(k)
+                        done.append(Completion(r.rid, s, r.tol, r.arrival, adm, clock() - t0, it, ok, rel, comp,
+                                               x if keep_solution else None))
+                progressed = True
+        if not progressed:
+            if not any(active.values()) and pending:
+                wait = pending[0].arrival - (clock() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.01))
+            else:
+                time.sleep(poll_s)
+    makespan = clock() - t0
+    out = summarize(done, makespan)
+    out.update(peak_inflight=peak, slots={"x".join(map(str, s)): slots[s] for s in shapes},
+               batches_gb=used / 1e9, cold_shapes=["x".join(map(str, s)) for s in shapes if s not in prewarm])
+    return sorted(done, key=lambda c: c.rid), out

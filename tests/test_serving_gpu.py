@@ -1,8 +1,8 @@
 """The serving loop on the device: a mixed-size request stream run concurrently (jobs overlapping on
 separate streams, pooled solvers reused) gives each request the result it gets alone.
 Tolerance: equal iteration counts and displacement relative difference <= 1e-10.  Every kernel of
-the solve is deterministic; the coarsest-level Cholesky factor and inverse come from cuSOLVER at
-setup, whose last bits may depend on the stream it runs on."""
+the solve is deterministic; the batched loop sums its dot products in another grouping than the
+single-job solver, so the two agree to rounding, not bitwise."""
 import numpy as np
 import pytest
 import torch
@@ -43,3 +43,22 @@ def test_budget_limits_concurrency():
     done, summary = serving.serve(reqs, precision="mixed", max_slots=6, budget_bytes=2.2 * big)
     assert summary["requests"] == 12 and summary["all_converged"]
     assert summary["peak_budget_gb"] * 1e9 <= 2.2 * big
+
+
+def test_batched_serving_results_equal_results_alone():
+    """serve_batched: the jobs of a shape share every launch of their batch (stacked grid); each result
+    equals the job solved alone, and jobs of several shapes and more jobs than slots go through."""
+    reqs = _requests()
+    slots = {(16, 8, 8): 2, (32, 16, 16): 3, (48, 24, 24): 2}
+    done, summary = serving.serve_batched(reqs, slots=slots, keep_solution=True, chunk=2)
+    assert summary["requests"] == 12 and summary["all_converged"]
+    assert summary["peak_inflight"] > 3
+    for c in done:
+        r = reqs[c.rid]
+        mask, force = vx.problems.cantilever_equal_split(r.shape)
+        s = vx.ElasticitySolver(r.shape, vx.problems.simp_modulus(r.density, 1e-9), mask, precision="mixed",
+                                tol=r.tol, maxiter=200, check_every=1)
+        alone = s.solve(force)
+        assert alone.iterations == c.iterations, (c.rid, alone.iterations, c.iterations)
+        diff = float(torch.linalg.vector_norm(alone.x - c.x) / torch.linalg.vector_norm(alone.x))
+        assert diff <= 1e-10, (c.rid, diff)
