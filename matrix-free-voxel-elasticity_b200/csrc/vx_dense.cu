@@ -7,7 +7,8 @@
 // The factorisation therefore costs about n bw^2 / 2 multiply-adds instead of n^3 / 6:
 //   * band_load:      the lower band of A into band storage lb[i (bw+1) + (j - i + bw)] = L[i][j];
 //   * per block column k of CB = 64 columns, two launches:
-//       band_potrf:   one CTA factors the CB x CB diagonal block in shared memory and inverts it;
+//       band_potrf:   one CTA (a thread per row) factors the CB x CB diagonal block in shared memory
+//                     and inverts it;
 //       band_update:  one CTA per lower tile (I, J) of the rows the block column reaches (at most
 //                     bw below it) forms the panel rows L_I = A_I L_kk^-T and L_J the same way (a
 //                     64 x 64 product with the block's inverse), writes L_I (diagonal tiles only),
@@ -26,7 +27,7 @@ namespace vx {
 
 constexpr int CB = 64;            // block columns of the banded Cholesky
 constexpr int CBP = CB + 1;       // padded shared-memory row
-constexpr int POTRF_T = 1024;
+constexpr int POTRF_T = 256;    // copies by all threads; the first CB own a row of the diagonal block
 constexpr int UPDATE_T = 256;
 constexpr int INV_STAGES = 4;     // L rows in flight in band_inverse
 
@@ -44,6 +45,9 @@ __global__ void band_load_kernel(int n, int bw, const double* __restrict__ A, do
 // inverse goes to dinv (CB x CB, row-major, lower triangle), and the block column's rows below it
 // (the A values band_update turns into the panel) to apanel ((bw + 1) x CB), so that band_update
 // can store finished panel rows in place while other tiles still read the originals.
+// Thread r < CB owns row r of the block (right-looking: two barriers per column); the inverse is
+// column-parallel (thread c runs the forward substitution of column c, no barrier); every thread
+// shares the copies.
 // Dynamic shared memory: D and X, CB x CBP each.
 __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int k0, double* __restrict__ lb,
                                                              double* __restrict__ dinv, double* __restrict__ apanel,
@@ -54,51 +58,48 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
     double (*X)[CBP] = reinterpret_cast<double (*)[CBP]>(psm + CB * CBP);
     const int w = min(CB, n - k0);
     const int base = k0 + w, rend = min(n, k0 + w + bw);
-    for (int t = threadIdx.x; t < (rend - base) * CB; t += POTRF_T) {
-        const int r = base + t / CB, c = t % CB, col = k0 + c;
-        apanel[t] = (c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
+    const int t = threadIdx.x;
+    for (int i = t; i < (rend - base) * CB; i += POTRF_T) {
+        const int r = base + i / CB, c = i % CB, col = k0 + c;
+        apanel[i] = (c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
     }
-    for (int t = threadIdx.x; t < CB * CB; t += POTRF_T) {
-        const int r = t / CB, c = t % CB;
+    for (int i = t; i < CB * CB; i += POTRF_T) {
+        const int r = i / CB, c = i % CB;
         D[r][c] = (r < w && c <= r && r - c <= bw) ? lb[bidx(k0 + r, k0 + c, bw)] : 0.0;
         X[r][c] = 0.0;
     }
     __syncthreads();
     for (int j = 0; j < w; ++j) {
-        if (threadIdx.x == 0) {
-            double d = D[j][j];
-            if (!(d > 0.0)) {                                 // not positive definite: flag, keep finite
-                atomicCAS(info, 0, k0 + j + 1);
-                d = 1.0;
-            }
-            D[j][j] = sqrt(d);
+        double d = D[j][j];
+        if (!(d > 0.0)) {                                     // not positive definite: flag, keep finite
+            if (t == j) atomicCAS(info, 0, k0 + j + 1);
+            d = 1.0;
         }
+        const double piv = sqrt(d);
+        if (t > j && t < w) D[t][j] = D[t][j] / piv;          // column j of L below the pivot
         __syncthreads();
-        const double piv = D[j][j];
-        for (int r = j + 1 + int(threadIdx.x); r < w; r += POTRF_T) D[r][j] = D[r][j] / piv;
-        __syncthreads();
-        const int m = w - j - 1;
-        for (int t = threadIdx.x; t < m * m; t += POTRF_T) {
-            const int r = j + 1 + t / m, c = j + 1 + t % m;
-            if (c <= r) D[r][c] -= D[r][j] * D[c][j];
+        if (t == j) D[j][j] = piv;
+        if (t > j && t < w) {
+            const double l = D[t][j];
+            for (int c = j + 1; c <= t; ++c) D[t][c] -= l * D[c][j];
         }
         __syncthreads();
     }
-    // inverse of the lower-triangular block, one row at a time: X[r][c] = -(sum_{c<=p<r} D[r][p] X[p][c]) / D[r][r]
-    for (int t = threadIdx.x; t < w; t += POTRF_T) X[t][t] = 1.0 / D[t][t];
-    __syncthreads();
-    for (int r = 1; r < w; ++r) {
-        for (int c = threadIdx.x; c < r; c += POTRF_T) {
+    // inverse of the lower-triangular block, column c by thread c:
+    // X[c][c] = 1 / D[c][c], X[r][c] = -(sum_{c<=p<r} D[r][p] X[p][c]) / D[r][r]
+    if (t < w) {
+        X[t][t] = 1.0 / D[t][t];
+        for (int r = t + 1; r < w; ++r) {
             double s = 0.0;
-            for (int p = c; p < r; ++p) s += D[r][p] * X[p][c];
-            X[r][c] = -s * X[r][r];
+            for (int p = t; p < r; ++p) s += D[r][p] * X[p][t];
+            X[r][t] = -s / D[r][r];
         }
-        __syncthreads();
     }
-    for (int t = threadIdx.x; t < CB * CB; t += POTRF_T) {
-        const int r = t / CB, c = t % CB;
+    __syncthreads();
+    for (int i = t; i < CB * CB; i += POTRF_T) {
+        const int r = i / CB, c = i % CB;
         if (r < w && c <= r && r - c <= bw) lb[bidx(k0 + r, k0 + c, bw)] = D[r][c];
-        dinv[t] = X[r][c];
+        dinv[i] = X[r][c];
     }
 }
 

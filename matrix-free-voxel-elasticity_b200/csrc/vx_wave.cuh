@@ -711,23 +711,22 @@ parity_wave(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args, const __gr
 }
 
 // Work decomposition for a grid: z tiles of 30 columns, y tiles of NW-1 rows, and the x chunk
-// length that balances the items over `ctas` persistent CTAs best (each item also computes the
-// element plane before its chunk, and pairs of planes want an even plane count per item).
+// length that keeps the `ctas` SMs busiest: useful node planes over the SMs' capacity for as many
+// rounds of items as the busiest CTA runs (each item also computes the element plane before its
+// chunk; pairs of planes want an even plane count per item).
 inline WaveSched wave_sched(const Grid& g, int nw, int pl, int ctas) {
     WaveSched s{};
     s.tz = (g.nz + 1 + WAVE_TZ - 1) / WAVE_TZ;
     s.ty = (g.ny + 1 + (nw - 1) - 1) / (nw - 1);
     const int cols = s.tz * s.ty;
     double best = -1.0;
-    for (int k = 1; k <= 64 && k <= g.nx + 1; ++k) {
+    for (int k = 1; k <= 128 && k <= g.nx + 1; ++k) {
         const int cx = (g.nx + 1 + k - 1) / k;
         const int chunks = (g.nx + 1 + cx - 1) / cx;
         const int64_t items = int64_t(chunks) * cols;
-        const int64_t G = std::min<int64_t>(ctas, items);
-        const int64_t rounds = (items + G - 1) / G;
-        const int steps = (cx + 1 + pl - 1) / pl;                // compute steps per full item
-        // work done / time taken by the busiest CTA (in element-plane steps)
-        const double eff = double(g.nx + 1) * cols / (double(rounds) * G * steps * pl);
+        const int64_t rounds = (items + ctas - 1) / ctas;
+        const int steps = (cx + 1 + pl - 1) / pl + 1;            // compute steps + the staging-only step
+        const double eff = double(g.nx + 1) * cols / (double(rounds) * ctas * steps * pl);
         if (eff > best + 1e-9) {
             best = eff;
             s.cx = cx;

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (read-only) and g++:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]    (default: $VOXEL_REF, else /root/reference)
 
 It imports the reference's own Python modules (src/voxel_mg.py, src/voxel_kernels.py,
 code/hex_modal/modal.py, experiments/session_a/dependencies/common.py, the donor
@@ -15,6 +15,7 @@ test suite reads the reference checkout; the fixtures are the only bridge.
 from __future__ import annotations
 
 import argparse
+import os
 import importlib.util
 import json
 import subprocess
@@ -63,7 +64,7 @@ def donor_problems(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--ref", type=Path, default=Path(os.environ.get("VOXEL_REF", "/root/reference")))
     ap.add_argument("--skip-slow", action="store_true", help="skip the 128x64x64 GMG solves (~1 min)")
     ap.add_argument("--only", choices=("donor_problems",), help="write one fixture file only")
     args = ap.parse_args()
