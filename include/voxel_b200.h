@@ -259,6 +259,32 @@ int vx_true_residual_planes(int prec, int nx, int ny, int nz, const double* bloc
  * in the reference (its kernels have no waits between threads). */
 int vx_device_status(int* status, int clear);
 
+/* Streaming operator kernel for FP64 / FP32 iterates (VX_F64, VX_F32), process-wide; the bf16
+ * iterate form always uses the element-plane-pair kernel.  All three compute the same arithmetic
+ * in the same order (FP32 results are bitwise equal; in FP64 the compiler contracts different
+ * multiply-add pairs, a difference of one rounding); they differ in how work is laid out:
+ *   VX_KERNEL_XP    a pair of element planes per thread, CTA barriers between rows (default)
+ *   VX_KERNEL_ZP    a pair of z node columns per thread, coalesced row spans, warps in a wavefront
+ *   VX_KERNEL_WAVE  one z column per lane, persistent CTAs, rows staged by bulk copies or cp.async
+ * vx_operator_partials follows the selection, so scratch sized before a change may be too small
+ * after it.  Returns the previous selection, or -1 for an unknown kind.  No counterpart in the
+ * reference. */
+enum { VX_KERNEL_ZP = 0, VX_KERNEL_WAVE = 1, VX_KERNEL_XP = 2 };
+int vx_set_stream_kernel(int kind);
+
+/* Tensor-core element-block operator, an experiment measured against the streaming kernels and not
+ * used by the solvers: the dense 24 x 24 element matrix applied to 128 elements at a time by
+ * tcgen05.mma (TF32 operands from FP32 storage, FP32 accumulation in tensor memory).
+ * ke: host 24 x 24 element matrix (row-major); E: element moduli (float); node_mask: optional,
+ * zeroes the constrained components of u; mode 0: y = K(E) u over the nodes (y overwritten, 3N
+ * floats); mode 1: the 24 scaled element results per element, y[24 e + i] (24 Ne floats).
+ * Results carry TF32 rounding (about 1e-3 relative).  The form the reference's donor ships is a
+ * BF16 WMMA element-block matvec (experiments/session_a/donor/src/gpu_fem/cuda_fused_matvec.py:147-281). */
+int vx_tc_element_product(int nx, int ny, int nz, const double* ke, const float* E, const uint8_t* node_mask,
+                          const float* u, float* y, int mode, cudaStream_t stream);
+/* Fault flag of vx_tc_element_product's bounded accumulator wait, as vx_device_status. */
+int vx_tc_status(int* status, int clear);
+
 /* The coarsest level's exact solve, set up without library calls (replaces the host Cholesky and the
  * two triangular solves of src/voxel_mg.py:152-159, experiments/session_i/run_gpu.py:281-286).
  * A: the dense n x n constrained matrix (vx_assemble_dense, row-major, symmetric positive definite),

@@ -53,6 +53,10 @@ SIGNATURES = {
     "vx_true_residual_planes": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, c_int, c_int, _P]),
     "vx_true_residual_noalloc": (c_int, [c_int, c_int, c_int, c_int, _D, _P, _P, _P, _P, _P, _P, _P]),
     "vx_device_status": (c_int, [POINTER(c_int), c_int]),
+    "vx_set_stream_kernel": (c_int, [c_int]),
+    "vx_tc_element_product": (c_int, [c_int, c_int, c_int, _D, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                      c_void_p]),
+    "vx_tc_status": (c_int, [POINTER(c_int), c_int]),
     "vx_coarse_factor_workspace": (c_int64, [c_int, c_int]),
     "vx_coarse_factor": (c_int, [c_int, c_int, _P, _P, _P, _P, _P]),
     # batches of independent systems
@@ -138,13 +142,14 @@ CAPTURE_STREAM = None
 
 # Kernel launches issued by each entry point (entry points not listed launch none or one:
 # host-only entry points are in HOST_ONLY).  Used to count this library's launches.
-KERNELS_PER_CALL = {"vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2, "vx_coarse_apply_factor": 2,
+KERNELS_PER_CALL = {"vx_tc_element_product": 1, "vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2, "vx_coarse_apply_factor": 2,
                     "vx_batch_coarse_apply_factor": 2}
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",
              "vx_graph_while_begin", "vx_graph_destroy", "vx_capture_status", "vx_graph_launch",
              "vx_oc_partials", "vx_graph_body_nodes", "vx_plane_fix_partials", "vx_device_status",
-             "vx_coarse_factor_workspace"}
+             "vx_coarse_factor_workspace", "vx_set_stream_kernel",
+             "vx_tc_status"}
 launches = 0          # kernels launched directly (graph launches are counted by the solvers)
 
 
@@ -170,6 +175,19 @@ def device_status(clear: bool = True) -> int:
     v = c_int(0)
     check(load().vx_device_status(ctypes.byref(v), int(bool(clear))), "vx_device_status")
     return int(v.value)
+
+
+STREAM_KERNELS = {"zp": 0, "wave": 1, "xp": 2}
+
+
+def set_stream_kernel(kind: str) -> str:
+    """Select the streaming operator kernel for FP64 / FP32 iterates ("zp", "wave" or "xp"); returns
+    the previous selection.  Operators size their partial sums at each call, so a change takes
+    effect at the next launch; captured graphs keep the kernel they were captured with."""
+    prev = int(load().vx_set_stream_kernel(STREAM_KERNELS[kind]))
+    if prev < 0:
+        raise ValueError(kind)
+    return {v: k for k, v in STREAM_KERNELS.items()}[prev]
 
 
 def dptr(a) -> _D:

@@ -22,6 +22,10 @@ int check_grid(int nx, int ny, int nz) {
         set_error("invalid grid (%d, %d, %d): every extent must be >= 1", nx, ny, nz);
         return VX_ERR_INVALID_ARGUMENT;
     }
+    if (ny + 1 > 6 * 65535) {      // the streaming kernels tile y over the launch grid's y extent
+        set_error("invalid grid (%d, %d, %d): ny must be below %d", nx, ny, nz, 6 * 65535);
+        return VX_ERR_INVALID_ARGUMENT;
+    }
     const double dofs = 3.0 * (nx + 1.0) * (ny + 1.0) * (nz + 1.0);
     if (dofs >= 2147483647.0) {
         set_error("grid (%d, %d, %d) has %.0f DOFs; the limit is 2^31 - 1", nx, ny, nz, dofs);

@@ -324,6 +324,7 @@ struct OpArgs2 {
 }  // namespace vx
 
 #include "vx_wave.cuh"
+#include "vx_zp.cuh"
 
 namespace vx {
 
@@ -717,6 +718,8 @@ inline int stream_cx(const Grid& g, Tiling t) {
     const int64_t yz = int64_t((g.nz + 1 + t.tz - 1) / t.tz) * ((g.ny + 1 + t.ty - 1) / t.ty);
     int cx = CX_MAX;
     while (cx > 4 && yz * ((g.nx + 1 + cx - 1) / cx) < 4 * 148) cx /= 2;
+    // at most 16384 CTAs (one partial sum each, the no-allocation residual's built-in scratch)
+    while (cx < g.nx + 1 && yz * ((g.nx + 1 + cx - 1) / cx) > 16384) cx *= 2;
     return cx;
 }
 
@@ -751,12 +754,26 @@ inline int64_t wave_ctas(const Grid& g) {
     const WaveSched w = wave_sched_for<TC>(g);
     return std::min<int64_t>(sm_count(), w.items);
 }
+template <typename TC>
+inline ZpGrid zp_grid_for(const Grid& g) {
+    return zp_grid(g, ZpCfg<TC>::NW, sm_count());
+}
 
-// CTAs (= partial sums) of a fused reducing launch of precision `prec` on grid g: the reducing
-// forms (VX_F64, VX_F32) run the persistent wavefront kernel, one CTA per SM at most
+// Streaming kernel for FP64 / FP32 iterates (process-wide; the other storage forms always run
+// parity_stream_xp): VX_KERNEL_XP (element-plane pairs, the default), VX_KERNEL_ZP (node-column
+// pairs) or VX_KERNEL_WAVE (persistent wavefront, one column per lane).
+static std::atomic<int> g_stream_kernel{VX_KERNEL_XP};
+
+// CTAs (= partial sums) of a fused reducing launch of precision `prec` on grid g
 int64_t stream_ctas(const Grid& g, int prec) {
-    if (prec == VX_F32) return wave_ctas<float>(g);
-    if (prec == VX_F64) return wave_ctas<double>(g);
+    const int kind = g_stream_kernel.load(std::memory_order_relaxed);
+    if (prec == VX_F32 || prec == VX_F64) {
+        if (kind == VX_KERNEL_ZP) {
+            const ZpGrid z = prec == VX_F32 ? zp_grid_for<float>(g) : zp_grid_for<double>(g);
+            return int64_t(z.tz) * z.ty * z.chunks;
+        }
+        if (kind == VX_KERNEL_WAVE) return prec == VX_F32 ? wave_ctas<float>(g) : wave_ctas<double>(g);
+    }
     const Tiling t = tiling(prec, true);
     dim3 d = stream_grid(g, t, stream_cx(g, t));
     return int64_t(d.x) * d.y * d.z;
@@ -783,7 +800,24 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
     OpArgs<TC, TU, TE, TY, TR> a = a_in;
     const bool cubic = a.cubic;
     static std::atomic<uint64_t> configured[2];            // per kernel of this instantiation: devices opted in
+    const int kind = wave ? g_stream_kernel.load(std::memory_order_relaxed) : VX_KERNEL_XP;
     if constexpr (wave) {
+        if (kind == VX_KERNEL_ZP) {
+            const ZpGrid z = zp_grid_for<TC>(a.g);
+            a.cx = z.cx;
+            const OpArgs2<TC, TU, TE, TY, TR> a2 = packed_args<TC, TU, TE, TY, TR, EPI, MASK>(a);
+            using Lz = ZpLayout<TC, TU, TE>;
+            static std::atomic<uint64_t> cfg_zp[2];
+            auto kz = cubic ? parity_zp<TC, TU, TE, TY, TR, EPI, MASK, true> : parity_zp<TC, TU, TE, TY, TR, EPI, MASK, false>;
+            int st = smem_opt_in(cfg_zp[cubic ? 1 : 0], (const void*)kz, Lz::BYTES, what);
+            if (st) return st;
+            vx::launch(kz, dim3(z.tz, z.ty, z.chunks), unsigned(Lz::NW * 32), Lz::BYTES, s, a2);
+            VX_CHECK_LAUNCH(what);
+            return VX_OK;
+        }
+    }
+    if constexpr (wave) {
+      if (kind == VX_KERNEL_WAVE) {
         const WaveSched ws = wave_sched_for<TC>(a.g);
         const unsigned G = unsigned(std::min<int64_t>(sm_count(), ws.items));
         const OpArgs2<TC, TU, TE, TY, TR> a2 = packed_args<TC, TU, TE, TY, TR, EPI, MASK>(a);
@@ -810,7 +844,9 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
         if (st) return st;
         VX_CHECK_LAUNCH(what);
         return VX_OK;
-    } else {
+      }
+    }
+    {
         const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
         a.cx = stream_cx(a.g, t);
         size_t smem, threads;
@@ -1284,6 +1320,14 @@ extern "C" int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const 
                                       nullptr, 0.0, res, scratch, stream);
     if (st) return st;
     return vx_reduce_partials(G, 1, scratch, norm2, stream);
+}
+
+extern "C" int vx_set_stream_kernel(int kind) {
+    if (kind != VX_KERNEL_ZP && kind != VX_KERNEL_WAVE && kind != VX_KERNEL_XP) {
+        set_error("vx_set_stream_kernel: unknown kernel %d", kind);
+        return -1;
+    }
+    return g_stream_kernel.exchange(kind);
 }
 
 // Fault flag of the streaming kernels' bounded waits (0 in every correct run): copied to *status;

@@ -249,3 +249,20 @@ def product(shape, rho, u, ke, mask, emin, emax=1.0, penal=3.0, want=("y", "ce",
               _ptr(y, "y", allow_none=True), _ptr(ce, "ce", allow_none=True), _ptr(d, "diag", allow_none=True),
               stream_ptr())
     return y, ce, d
+
+
+def tc_element_product(shape, ke, E, u, node_mask=None, per_element=False, out=None):
+    """The tensor-core element-block operator (an experiment, not used by the solvers): the dense
+    24 x 24 element matrix applied 128 elements at a time by tcgen05.mma with TF32 operands and FP32
+    accumulation.  E, u: float32 CUDA tensors (Ne, 3N); node_mask: optional uint8 node mask.
+    Returns y = K(E) (m . u) over the nodes (3N floats), or with per_element=True the 24 scaled
+    element results per element (Ne x 24).  Results carry TF32 rounding (~1e-3 relative)."""
+    shape = tuple(int(v) for v in shape)
+    ne, nn = n_elems(shape), n_nodes(shape)
+    k = np.ascontiguousarray(np.asarray(ke, dtype=np.float64).reshape(576))
+    n_out = 24 * ne if per_element else 3 * nn
+    y = torch.empty(n_out, dtype=torch.float32, device=u.device) if out is None else out
+    _lib.call("vx_tc_element_product", *shape, _lib.dptr(k), _ptr(E, "E", torch.float32, ne),
+              _ptr(node_mask, "node_mask", torch.uint8, nn, allow_none=True), _ptr(u, "u", torch.float32, 3 * nn),
+              _ptr(y, "y", torch.float32, n_out), int(bool(per_element)), stream_ptr())
+    return y.view(ne, 24) if per_element else y

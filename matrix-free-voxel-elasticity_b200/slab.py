@@ -507,6 +507,54 @@ class SlabHierarchy:
 
 
 # ---------------------------------------------------------------------------------------- outer loop
+def replay_until_done(replay, read, k, maxiter, it):
+    """Host loop of a solve whose body of k iterations (the last one a check) runs as one replay:
+    replay, read the device scalars, stop once they say converged or broken down, or before a body
+    would pass maxiter.  Every rank reads the same scalars -- they are computed from all-reduced
+    sums by the same kernels -- so every rank takes the same decisions and issues the same
+    collectives.  Returns (scalars, bodies replayed); the caller finishes the iterations that do not
+    fill a whole body one at a time."""
+    s = read()
+    bodies = 0
+    while not s[S_DONE] and not s[S_BREAK] and it + k <= maxiter:
+        replay()
+        bodies += 1
+        s = read()
+        it = int(s[S_IT])
+    return s, bodies
+
+
+class _ReplayBody:
+    """A body of solver iterations, NCCL exchanges included (neighbour swaps and all-reduces on this
+    process's current stream), captured once into a CUDA graph and replayed from the host -- the
+    form a slab solve spread over processes can take, since a device-side WHILE loop cannot wait
+    for the other ranks' decisions.  The body runs once un-captured first (module loading, NCCL
+    communicator set-up); callers re-initialise the solver state afterwards."""
+
+    def __init__(self, stream: torch.cuda.Stream, emit_body):
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            emit_body()
+        stream.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        before = _lib.launches
+        try:
+            with torch.cuda.graph(self.graph, stream=stream):
+                emit_body()
+        finally:
+            self.body_kernels = _lib.launches - before
+            _lib.launches = before
+
+    def launch(self):
+        self.graph.replay()
+        _lib.launches += self.body_kernels
+
+    def close(self):
+        if self.graph is not None:
+            self.graph.reset()
+            self.graph = None
+
+
 class SlabSolver:
     """K(E) u = f on a global (nx, ny, nz) voxel grid cut into `nparts` x-slabs: the flexible
     (Polak-Ribiere) PCG of src/voxel_mg.py:181-217 in FP64 with the slab V-cycle, the same
@@ -515,11 +563,14 @@ class SlabSolver:
 
     E (Ne) and mask (3N 0/1 DOF mask or N uint8 node mask) are the GLOBAL arrays; each process
     keeps its slabs' slices.  With torch.distributed initialised and world size > 1 this process
-    holds slab `rank` and exchanges with its neighbours over the process group."""
+    holds slab `rank` and exchanges with its neighbours over the process group; there
+    `dist_graph=True` (NCCL) captures check_every iterations, exchanges included, into a CUDA graph
+    that the host replays (replay_until_done) instead of launching every kernel of every iteration.
+    Release it with close() before destroy_process_group."""
 
     def __init__(self, shape, E, mask, nparts, ke=None, precision="mixed", pre=2, post=2, omega=0.6,
                  max_coarse_x=16, levels=None, tol=1e-8, maxiter=200, check_every=1, local=None, graph=True,
-                 spectral_seed=20260923):
+                 spectral_seed=20260923, dist_graph=False):
         from .api import _MG_STORAGE, _dev
         if precision not in _MG_STORAGE:
             raise ValueError(f"precision must be one of {tuple(_MG_STORAGE)} for the slab solver")
@@ -556,6 +607,17 @@ class SlabSolver:
         self.stream = torch.cuda.Stream()
         self.use_graph = bool(graph) and not self.comm.distributed
         self._graph = None
+        if dist_graph and not (self.comm.distributed and not self.comm.staged):
+            raise ValueError("dist_graph needs a process group with the NCCL backend and one slab per process")
+        self.dist_graph = bool(dist_graph)
+        self._replay = None
+
+    def close(self):
+        """Release the captured replay graph (it holds NCCL work; release it before the process
+        group is destroyed)."""
+        if self._replay is not None:
+            self._replay.close()
+            self._replay = None
 
     # -------------------------------------------------------------- distributed pieces
     def _levels(self):
@@ -658,6 +720,8 @@ class SlabSolver:
         st.wait_stream(caller)
         if use_graph and self._graph is None:
             self._graph = _GraphLoop(st, self.S, lambda: self._body(k))
+        if self.dist_graph and full > 0 and self._replay is None:
+            self._replay = _ReplayBody(st, lambda: self._body(k))
         with torch.cuda.stream(st):
             s = self._solve(f, x0, k, full, use_graph)
         caller.wait_stream(st)
@@ -692,6 +756,9 @@ class SlabSolver:
             s = self._read()
             self._graph.account(max(1, -(-int(s[S_IT]) // k)))
         it = int(s[S_IT])
+        if self._replay is not None and not s[S_DONE]:
+            s, _ = replay_until_done(self._replay.launch, self._read, k, self.maxiter, it)
+            it = int(s[S_IT])
         while not s[S_DONE] and not s[S_BREAK] and it < self.maxiter:
             check = (it + 1) % k == 0
             self._iteration(check)

@@ -10,6 +10,15 @@ from oracle import voxel_oracle as vo
 pytestmark = pytest.mark.gpu
 
 vx = pytest.importorskip("voxel_b200")
+from voxel_b200 import _lib  # noqa: E402
+
+
+@pytest.fixture(autouse=True)
+def wave_kernel():
+    prev = _lib.set_stream_kernel("wave")
+    yield
+    _lib.set_stream_kernel(prev)
+
 
 KE = vo.quadrature([1, 1, 1], 0.3)
 # (150, 40, 70): 3 x 3 tiles of (y, z) over 151 node planes -> more items than SMs

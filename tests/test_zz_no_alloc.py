@@ -59,13 +59,20 @@ def test_noalloc_matches_existing_entry_point_on_two_calls(shape, dtype, tol):
 
 
 def test_noalloc_scratch_covers_every_accepted_grid():
-    """The streaming kernel keeps one partial sum per persistent CTA (at most one per SM), so the
-    built-in 16384-double scratch holds the partials of every grid the library accepts; a grid
-    beyond the library's 2^31-DOF limit is refused with a clear error before any device work."""
-    for prec in (_lib.VX_F64, _lib.VX_F32):
-        for shape in ((2047, 400, 400), (1, 1, 1), (576, 288, 288)):
-            G = _lib.load().vx_operator_partials(prec, *shape)
-            assert 1 <= G <= min(16384, torch.cuda.get_device_properties(0).multi_processor_count)
+    """Every streaming kernel keeps one partial sum per CTA and chunks x only while the CTAs stay
+    within the built-in 16384-double scratch, so it holds the partials of every grid whose y-z
+    tiling fits (all but extremely flat ones); a grid beyond the library's 2^31-DOF limit is refused
+    with a clear error before any device work."""
+    prev = _lib.set_stream_kernel("xp")
+    try:
+        for kind in ("xp", "zp", "wave"):
+            _lib.set_stream_kernel(kind)
+            for prec in (_lib.VX_F64, _lib.VX_F32):
+                for shape in ((2047, 400, 400), (1, 1, 1), (576, 288, 288), (1, 1500, 1500)):
+                    G = _lib.load().vx_operator_partials(prec, *shape)
+                    assert 1 <= G <= 16384, (kind, prec, shape, G)
+    finally:
+        _lib.set_stream_kernel(prev)
     shape = (4000, 600, 600)                     # 4.3e9 DOFs
     dummy = torch.zeros(8, dtype=torch.float64, device="cuda")
     blocks = np.ascontiguousarray(vx.Modal(KE).blocks.reshape(72))
