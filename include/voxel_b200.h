@@ -260,16 +260,16 @@ int vx_true_residual_planes(int prec, int nx, int ny, int nz, const double* bloc
 int vx_device_status(int* status, int clear);
 
 /* Streaming operator kernel for FP64 / FP32 iterates (VX_F64, VX_F32), process-wide; the bf16
- * iterate form always uses the element-plane-pair kernel.  All three compute the same arithmetic
- * in the same order (FP32 results are bitwise equal; in FP64 the compiler contracts different
+ * iterate form always uses the element-plane-pair kernel.  Both compute the same arithmetic in the
+ * same order (FP32 results are bitwise equal; in FP64 the compiler contracts different
  * multiply-add pairs, a difference of one rounding); they differ in how work is laid out:
- *   VX_KERNEL_XP    a pair of element planes per thread, CTA barriers between rows (default)
- *   VX_KERNEL_ZP    a pair of z node columns per thread, coalesced row spans, warps in a wavefront
- *   VX_KERNEL_WAVE  one z column per lane, persistent CTAs, rows staged by bulk copies or cp.async
+ *   VX_KERNEL_XP  a pair of element planes per thread, CTA barriers between rows (default)
+ *   VX_KERNEL_ZP  a pair of z node columns per thread, coalesced row spans staged by cp.async,
+ *                 warps in a wavefront handing partial sums over mbarriers
  * vx_operator_partials follows the selection, so scratch sized before a change may be too small
  * after it.  Returns the previous selection, or -1 for an unknown kind.  No counterpart in the
  * reference. */
-enum { VX_KERNEL_ZP = 0, VX_KERNEL_WAVE = 1, VX_KERNEL_XP = 2 };
+enum { VX_KERNEL_XP = 0, VX_KERNEL_ZP = 1 };
 int vx_set_stream_kernel(int kind);
 
 /* Tensor-core element-block operator, an experiment measured against the streaming kernels and not

@@ -177,11 +177,11 @@ def device_status(clear: bool = True) -> int:
     return int(v.value)
 
 
-STREAM_KERNELS = {"zp": 0, "wave": 1, "xp": 2}
+STREAM_KERNELS = {"xp": 0, "zp": 1}
 
 
 def set_stream_kernel(kind: str) -> str:
-    """Select the streaming operator kernel for FP64 / FP32 iterates ("zp", "wave" or "xp"); returns
+    """Select the streaming operator kernel for FP64 / FP32 iterates ("xp" or "zp"); returns
     the previous selection.  Operators size their partial sums at each call, so a change takes
     effect at the next launch; captured graphs keep the kernel they were captured with."""
     prev = int(load().vx_set_stream_kernel(STREAM_KERNELS[kind]))

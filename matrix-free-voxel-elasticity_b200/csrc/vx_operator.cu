@@ -323,7 +323,6 @@ struct OpArgs2 {
 };
 }  // namespace vx
 
-#include "vx_wave.cuh"
 #include "vx_zp.cuh"
 
 namespace vx {
@@ -746,22 +745,13 @@ inline int sm_count() {
 }
 
 template <typename TC>
-inline WaveSched wave_sched_for(const Grid& g) {
-    return wave_sched(g, WaveCfg<TC>::NW, WaveCfg<TC>::PL, sm_count());
-}
-template <typename TC>
-inline int64_t wave_ctas(const Grid& g) {
-    const WaveSched w = wave_sched_for<TC>(g);
-    return std::min<int64_t>(sm_count(), w.items);
-}
-template <typename TC>
 inline ZpGrid zp_grid_for(const Grid& g) {
     return zp_grid(g, ZpCfg<TC>::NW, sm_count());
 }
 
 // Streaming kernel for FP64 / FP32 iterates (process-wide; the other storage forms always run
-// parity_stream_xp): VX_KERNEL_XP (element-plane pairs, the default), VX_KERNEL_ZP (node-column
-// pairs) or VX_KERNEL_WAVE (persistent wavefront, one column per lane).
+// parity_stream_xp): VX_KERNEL_XP (element-plane pairs, the default) or VX_KERNEL_ZP (node-column
+// pairs).
 static std::atomic<int> g_stream_kernel{VX_KERNEL_XP};
 
 // CTAs (= partial sums) of a fused reducing launch of precision `prec` on grid g
@@ -772,7 +762,6 @@ int64_t stream_ctas(const Grid& g, int prec) {
             const ZpGrid z = prec == VX_F32 ? zp_grid_for<float>(g) : zp_grid_for<double>(g);
             return int64_t(z.tz) * z.ty * z.chunks;
         }
-        if (kind == VX_KERNEL_WAVE) return prec == VX_F32 ? wave_ctas<float>(g) : wave_ctas<double>(g);
     }
     const Tiling t = tiling(prec, true);
     dim3 d = stream_grid(g, t, stream_cx(g, t));
@@ -795,13 +784,13 @@ template <typename TC, typename TU, typename TE, typename TY, int EPI, int MASK,
 int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const char* what) {
     constexpr bool v2 = !REV && !SIMP && MASK != MASK_DOF;
     static_assert(v2 || std::is_same<TR, TY>::value, "parity_stream takes r and invd of the output type");
-    // iterates in FP64 / FP32: the wavefront kernel (u staged by cp.async, 4- or 8-byte words)
-    constexpr bool wave = v2 && (std::is_same<TU, double>::value || std::is_same<TU, float>::value);
+    // iterates in FP64 / FP32: either streaming kernel (parity_zp stages 4- or 8-byte words)
+    constexpr bool zp_ok = v2 && (std::is_same<TU, double>::value || std::is_same<TU, float>::value);
     OpArgs<TC, TU, TE, TY, TR> a = a_in;
     const bool cubic = a.cubic;
     static std::atomic<uint64_t> configured[2];            // per kernel of this instantiation: devices opted in
-    const int kind = wave ? g_stream_kernel.load(std::memory_order_relaxed) : VX_KERNEL_XP;
-    if constexpr (wave) {
+    const int kind = zp_ok ? g_stream_kernel.load(std::memory_order_relaxed) : VX_KERNEL_XP;
+    if constexpr (zp_ok) {
         if (kind == VX_KERNEL_ZP) {
             const ZpGrid z = zp_grid_for<TC>(a.g);
             a.cx = z.cx;
@@ -815,36 +804,6 @@ int launch_stream(const OpArgs<TC, TU, TE, TY, TR>& a_in, cudaStream_t s, const 
             VX_CHECK_LAUNCH(what);
             return VX_OK;
         }
-    }
-    if constexpr (wave) {
-      if (kind == VX_KERNEL_WAVE) {
-        const WaveSched ws = wave_sched_for<TC>(a.g);
-        const unsigned G = unsigned(std::min<int64_t>(sm_count(), ws.items));
-        const OpArgs2<TC, TU, TE, TY, TR> a2 = packed_args<TC, TU, TE, TY, TR, EPI, MASK>(a);
-        const unsigned threads = WaveCfg<TC>::NW * 32;
-        // rows staged by bulk (TMA-engine) copies when the arrays are 16-byte aligned, else by cp.async
-        const bool bulk = aligned(a.u, 16) && aligned(a.E, 16) && (MASK == MASK_NONE || aligned(a.node_mask, 16));
-        auto go = [&](auto kern, size_t bytes, std::atomic<uint64_t>& flag) -> int {
-            int st = smem_opt_in(flag, (const void*)kern, bytes, what);
-            if (st) return st;
-            vx::launch(kern, G, threads, bytes, s, a2, ws);
-            return VX_OK;
-        };
-        static std::atomic<uint64_t> cfg_bulk[2];
-        int st;
-        if (bulk) {
-            using Lb = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, true, true>;
-            st = cubic ? go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, true, true>, Lb::BYTES, cfg_bulk[1])
-                       : go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, false, true>, Lb::BYTES, cfg_bulk[0]);
-        } else {
-            using La = WaveLayout<TC, TU, TE, TY, TR, EPI, MASK, true, false>;
-            st = cubic ? go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, true, false>, La::BYTES, configured[1])
-                       : go(parity_wave<TC, TU, TE, TY, TR, EPI, MASK, false, false>, La::BYTES, configured[0]);
-        }
-        if (st) return st;
-        VX_CHECK_LAUNCH(what);
-        return VX_OK;
-      }
     }
     {
         const Tiling t = tiling(std::is_same<TC, double>::value ? VX_F64 : VX_F32, v2);
@@ -1323,7 +1282,7 @@ extern "C" int vx_true_residual_noalloc(int prec, int nx, int ny, int nz, const 
 }
 
 extern "C" int vx_set_stream_kernel(int kind) {
-    if (kind != VX_KERNEL_ZP && kind != VX_KERNEL_WAVE && kind != VX_KERNEL_XP) {
+    if (kind != VX_KERNEL_ZP && kind != VX_KERNEL_XP) {
         set_error("vx_set_stream_kernel: unknown kernel %d", kind);
         return -1;
     }
@@ -1335,10 +1294,10 @@ extern "C" int vx_set_stream_kernel(int kind) {
 extern "C" int vx_device_status(int* status, int clear) {
     VX_CHECK_ARG(status, VX_ERR_NULL_POINTER, "vx_device_status: NULL status");
     int v = 0;
-    cudaError_t e = cudaMemcpyFromSymbol(&v, vx::g_wave_fault, sizeof(int));
+    cudaError_t e = cudaMemcpyFromSymbol(&v, vx::g_stream_fault, sizeof(int));
     if (e == cudaSuccess && clear && v) {
         const int zero = 0;
-        e = cudaMemcpyToSymbol(vx::g_wave_fault, &zero, sizeof(int));
+        e = cudaMemcpyToSymbol(vx::g_stream_fault, &zero, sizeof(int));
     }
     if (e != cudaSuccess) {
         set_error("vx_device_status: %s", cudaGetErrorString(e));

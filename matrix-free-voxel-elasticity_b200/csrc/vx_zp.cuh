@@ -1,7 +1,7 @@
 // parity_zp: the streaming Hex8 operator with a PAIR of z node columns per thread (FP64 and FP32
 // iterates).
 //
-// Same arithmetic as parity_stream_xp and parity_wave (parity form, separable X / Y / Z stages
+// Same arithmetic as parity_stream_xp (parity form, separable X / Y / Z stages
 // shared between neighbouring elements, E folded into the Z stage, cube-pattern block product,
 // node-owned tiles with recomputed halo elements, no atomics, bitwise deterministic), with the work
 // of a thread shaped to cut what is not arithmetic:
@@ -31,7 +31,10 @@
 //    is complete after element plane e and is written (or fused into the epilogue) at once.
 #pragma once
 
-#include "vx_wave.cuh"
+#include "vx_async.cuh"
+#include "vx_pair.cuh"
+
+#include <type_traits>
 
 namespace vx {
 
@@ -52,17 +55,23 @@ constexpr int ZP_TZ = 62;   // owned node columns per tile
 constexpr int ZP_W = 192;   // words of a row span: 64 node columns x 3 components
 
 // Shared memory of one CTA.  Per warp: the ring (D slots: own row span, upper row span, element
-// modulus span with E_ASYNC), the output span, the modulus span (without E_ASYNC) and three planes
-// of node-mask spans (own and upper row); then the exchange buffers (per row two buffers of six
-// pairs), the mbarriers (full / empty per row and buffer) and the abort flag.
+// modulus span with E_ASYNC; each copied in whole 16-byte chunks from the aligned chunk at or below
+// its first word, so it starts `shift` words into its buffer), the output span, the modulus span
+// (without E_ASYNC) and three planes of node-mask spans (own and upper row); then the exchange
+// buffers (per row two buffers of six pairs), the mbarriers (full / empty per row and buffer) and
+// the abort flag.
 template <typename TC, typename TU, typename TE>
 struct ZpLayout {
     using Cfg = ZpCfg<TC>;
     static constexpr int NW = Cfg::NW, D = Cfg::D, A = Cfg::A;
     static constexpr bool E_ASYNC = Cfg::E_ASYNC && sizeof(TE) >= 4;
     static constexpr size_t r16(size_t b) { return (b + 15) / 16 * 16; }
-    static constexpr size_t SLOT_E = E_ASYNC ? 64 * sizeof(TE) : 0;
-    static constexpr size_t SLOT_B = r16(2 * ZP_W * sizeof(TU) + SLOT_E);
+    static constexpr int CH = 16 / sizeof(TU);              // words per 16-byte chunk
+    static constexpr int ROW_W = ZP_W + CH;                 // a row span and its alignment shift
+    static constexpr int ECH = sizeof(TE) >= 4 ? 16 / int(sizeof(TE)) : 1;
+    static constexpr int E_W = 64 + ECH;
+    static constexpr size_t SLOT_E = E_ASYNC ? E_W * sizeof(TE) : 0;
+    static constexpr size_t SLOT_B = r16(2 * ROW_W * sizeof(TU) + SLOT_E);
     static constexpr size_t AX_OFF = D * SLOT_B;
     static constexpr size_t EX_OFF = AX_OFF + r16(ZP_W * sizeof(TC));
     static constexpr size_t MK_OFF = EX_OFF + (E_ASYNC ? 0 : r16(64 * sizeof(TE)));
@@ -105,8 +114,8 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + L::BAR_OFF);   // full[NWW][2], empty[NWW][2]
     volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 4 * NWW);
     auto own_span = [&](int s) { return reinterpret_cast<TU*>(wb + size_t(s) * L::SLOT_B); };
-    auto up_span = [&](int s) { return reinterpret_cast<TU*>(wb + size_t(s) * L::SLOT_B) + ZP_W; };
-    auto e_span = [&](int s) { return reinterpret_cast<TE*>(wb + size_t(s) * L::SLOT_B + 2 * ZP_W * sizeof(TU)); };
+    auto up_span = [&](int s) { return reinterpret_cast<TU*>(wb + size_t(s) * L::SLOT_B) + L::ROW_W; };
+    auto e_span = [&](int s) { return reinterpret_cast<TE*>(wb + size_t(s) * L::SLOT_B + 2 * L::ROW_W * sizeof(TU)); };
 #define HS_(r, b, k) hs[(((r) * 2 + (b)) * 6 + (k)) * 32 + lane]
     if (threadIdx.x < 4 * NWW) mbar_init(bars + threadIdx.x, 1);     // one arrival: lane 0 after a warp barrier
     if (threadIdx.x == 0) *abort_flag = 0;
@@ -147,24 +156,66 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
 
     auto nplane = [&](int q) { return min(max(q, 0), g.nx); };
     auto eplane = [&](int q) { return min(max(q, 0), g.nx - 1); };
-    // ring group gi: node plane x0 - 1 + gi (own and upper row spans) and the element plane before it
-    auto stage = [&](int gi) {
-        const int s = gi % D;
-        const int q = x0 - 1 + gi;
-        const TU* uo = a.u + (plane3 * nplane(q) + rowo);
-        const TU* uu = a.u + (plane3 * nplane(q) + rowu);
-        TU* so = own_span(s);
-        TU* su = up_span(s);
+    // Ring group gi: node plane x0 - 1 + gi (own and upper row spans) and the element plane before
+    // it.  A span is copied in 16-byte chunks from the 16-byte aligned chunk at or below its first
+    // word (lane c copies chunk c), so source and shared-memory addresses agree modulo 16 bytes and
+    // the span starts `shift` words into its buffer.  A chunk that reaches outside the array (only
+    // around the grid's first and last node) is copied word by word, zeros standing in for the words
+    // outside (they belong to columns beyond the grid, which only meet elements of modulus 0).
+    const int n_words = 3 * ((g.nx + 1) * nyz_nodes);
+    const int n_elems = g.nx * nyz_elems;
+    auto span_start = [&](int q, int rw) { return plane3 * nplane(q) + rw + 3 * Z0; };
+    auto e_start = [&](int q) { return nyz_elems * eplane(q - 1) + rowe + Z0; };
+    // words from `src` up to the first 16-byte boundary of the array (its word misalignment)
+    const int mis_u = int((reinterpret_cast<uintptr_t>(a.u) / sizeof(TU)) & (L::CH - 1));
+    const int mis_e = int((reinterpret_cast<uintptr_t>(a.E) / sizeof(TE)) & (L::ECH - 1));
+    auto stage_span = [&](auto* dst, const auto* src, int start, int mis, int total, auto chunk_words, int nchunks) {
+        constexpr int CW = decltype(chunk_words)::value;
+        using T = std::remove_cv_t<std::remove_pointer_t<decltype(src)>>;
+        const int base = start - ((start + mis) & (CW - 1));
         #pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            cp_async<sizeof(TU)>(so + lane + 32 * j, uo + zw[j]);
-            cp_async<sizeof(TU)>(su + lane + 32 * j, uu + zw[j]);
+        for (int c0 = 0; c0 < nchunks; c0 += 32) {
+            const int c = c0 + lane;
+            if (c < nchunks) {
+                const int w = base + c * CW;
+                T* d = dst + c * CW;
+                if (w >= 0 && w + CW <= total) {
+                    cp_async_cg16(d, src + w);
+                } else {
+                    #pragma unroll
+                    for (int t = 0; t < CW; ++t) {
+                        if (w + t >= 0 && w + t < total) cp_async<sizeof(T)>(d + t, src + w + t);
+                        else d[t] = T(0);
+                    }
+                }
+            }
         }
+    };
+    auto stage = [&](int gi) {
+        const int sl_ = gi % D;
+        const int q = x0 - 1 + gi;
+        stage_span(own_span(sl_), a.u, span_start(q, rowo), mis_u, n_words, std::integral_constant<int, L::CH>{},
+                   L::ROW_W / L::CH);
+        stage_span(up_span(sl_), a.u, span_start(q, rowu), mis_u, n_words, std::integral_constant<int, L::CH>{},
+                   L::ROW_W / L::CH);
         if constexpr (E_ASYNC) {
-            const TE* eb = a.E + (nyz_elems * eplane(q - 1) + rowe);
-            TE* se = e_span(s);
+            stage_span(e_span(sl_), a.E, e_start(q), mis_e, n_elems, std::integral_constant<int, L::ECH>{},
+                       L::E_W / L::ECH);
+        }
+    };
+    // the six words of this lane's pair in a staged row span starting `shift` words in
+    auto read_pair = [&](const TU* row_buf, int shift, TU w[6]) {
+        const TU* p = row_buf + shift + 6 * lane;
+        if ((shift & 1) == 0) {
             #pragma unroll
-            for (int j = 0; j < 2; ++j) cp_async<sizeof(TE)>(se + lane + 32 * j, eb + ze[j]);
+            for (int m = 0; m < 3; ++m) {
+                const V2U t = *reinterpret_cast<const V2U*>(p + 2 * m);
+                w[2 * m] = t.x;
+                w[2 * m + 1] = t.y;
+            }
+        } else {
+            #pragma unroll
+            for (int k = 0; k < 6; ++k) w[k] = p[k];
         }
     };
     // node-mask bytes of plane q, span columns lane and lane + 32 of the own and upper row
@@ -226,6 +277,27 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
     e_put(e_issue(x0 - 1));
     ELd e_pf = e_issue(x0);
 
+    auto msk = [](uint32_t m, int byte, int k_, TU v) -> TC {
+        return ((m >> (8 * byte + k_)) & 1u) ? TC(v) : TC(0);
+    };
+    // masked own and upper values of a node plane's pair, from its ring slot
+    auto plane_pair = [&](int slot, int q, uint32_t m, P own[3], P upper[3]) {
+        TU wo[6], wu[6];
+        read_pair(own_span(slot), (span_start(q, rowo) + mis_u) & (L::CH - 1), wo);
+        read_pair(up_span(slot), (span_start(q, rowu) + mis_u) & (L::CH - 1), wu);
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            own[k] = mk2(msk(m, 0, k, wo[k]), msk(m, 1, k, wo[3 + k]));
+            upper[k] = mk2(msk(m, 2, k, wu[k]), msk(m, 3, k, wu[3 + k]));
+        }
+    };
+    P lo[3], lon[3];                                            // node plane e, masked: own, upper row
+    uint32_t m_lo;
+    cp_async_wait<A>();                                          // group 0 (plane x0 - 1) has landed
+    __syncwarp();
+    m_lo = mask_pair(0);
+    plane_pair(0, x0 - 1, m_lo, lo, lon);
+
     P carry[3] = {mk2(TC(0), TC(0)), mk2(TC(0), TC(0)), mk2(TC(0), TC(0))};
     double acc = 0.0;
     for (int i = 0; i < steps; ++i) {
@@ -252,43 +324,25 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
         cp_async_wait<A>();                                      // groups 0 .. i + 1 have landed
         __syncwarp();                                            // ... for every lane of the warp
         const int sl = i % D, sh = (i + 1) % D;                  // slots of node planes e, e + 1
-        const uint32_t m_lo = mask_pair(i % 3), m_hi = mask_pair((i + 1) % 3);
+        const uint32_t m_hi = mask_pair((i + 1) % 3);
 
         // ---- X stage (own and upper rows), Y stage, on the node pair
+        P hi[3], hin[3];
+        plane_pair(sh, e + 1, m_hi, hi, hin);
         P Y[3][2][2];
-        {
-            TU w[4][6];                                          // own e, own e+1, upper e, upper e+1
-            const TU* src[4] = {own_span(sl), own_span(sh), up_span(sl), up_span(sh)};
-            #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                #pragma unroll
-                for (int m = 0; m < 3; ++m) {
-                    const V2U t = *reinterpret_cast<const V2U*>(src[r] + 6 * lane + 2 * m);
-                    w[r][2 * m] = t.x;
-                    w[r][2 * m + 1] = t.y;
-                }
-            }
-            auto msk = [](uint32_t m, int byte, int k_, TU v) -> TC {
-                return ((m >> (8 * byte + k_)) & 1u) ? TC(v) : TC(0);
-            };
-            #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const P lo = mk2(msk(m_lo, 0, k, w[0][k]), msk(m_lo, 1, k, w[0][3 + k]));
-                const P hi = mk2(msk(m_hi, 0, k, w[1][k]), msk(m_hi, 1, k, w[1][3 + k]));
-                const P lon = mk2(msk(m_lo, 2, k, w[2][k]), msk(m_lo, 3, k, w[2][3 + k]));
-                const P hin = mk2(msk(m_hi, 2, k, w[3][k]), msk(m_hi, 3, k, w[3][3 + k]));
-                const P X0 = add2(lo, hi), X1 = sub2(lo, hi);
-                const P B0 = add2(lon, hin), B1 = sub2(lon, hin);
-                Y[k][0][0] = add2(X0, B0); Y[k][0][1] = sub2(X0, B0);
-                Y[k][1][0] = add2(X1, B1); Y[k][1][1] = sub2(X1, B1);
-            }
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const P X0 = add2(lo[k], hi[k]), X1 = sub2(lo[k], hi[k]);
+            const P B0 = add2(lon[k], hin[k]), B1 = sub2(lon[k], hin[k]);
+            Y[k][0][0] = add2(X0, B0); Y[k][0][1] = sub2(X0, B0);
+            Y[k][1][0] = add2(X1, B1); Y[k][1][1] = sub2(X1, B1);
         }
         // ---- element moduli of the pair (A, B)
         TC eA, eB;
         if constexpr (E_ASYNC) {
-            const TE* es = e_span(sh);
-            eA = TC(Storage<TE>::cvt(es[2 * lane]));
-            eB = TC(Storage<TE>::cvt(es[2 * lane + 1]));
+            const TE* es = e_span(sh) + ((e_start(e + 1) + mis_e) & (L::ECH - 1)) + 2 * lane;
+            eA = TC(Storage<TE>::cvt(es[0]));
+            eB = TC(Storage<TE>::cvt(es[1]));
         } else {
             eA = TC(Storage<TE>::cvt(exs[2 * lane]));
             eB = TC(Storage<TE>::cvt(exs[2 * lane + 1]));
@@ -415,8 +469,10 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
         }
         // the operator's value on the pair's words (constrained components take the raw iterate),
         // into the output span
+        const int sh_lo = (span_start(e, rowo) + mis_u) & (L::CH - 1);
         if (out) {
-            const TU* xo = own_span(sl);
+            TU xw[6];
+            if constexpr (MASK != MASK_NONE) read_pair(own_span(sl), sh_lo, xw);
             #pragma unroll
             for (int m = 0; m < 3; ++m) {
                 TC v2[2];
@@ -425,7 +481,8 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
                     const int w = 2 * m + t, h = w / 3, k = w % 3;
                     const bool fr = (m_lo >> (8 * h + k)) & 1u;
                     const TC yv = h == 0 ? yo[k].lo() : yo[k].hi();
-                    v2[t] = (MASK == MASK_NONE || fr) ? yv : TC(xo[6 * lane + w]);
+                    if constexpr (MASK == MASK_NONE) v2[t] = yv;
+                    else v2[t] = fr ? yv : TC(xw[w]);
                 }
                 typename Vec2T<TC>::type t2;
                 t2.x = v2[0];
@@ -436,7 +493,7 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
         __syncwarp();
         // ---- span epilogue: coalesced outputs of node plane e
         if (out) {
-            const TU* xo = own_span(sl);
+            const TU* xo = own_span(sl) + sh_lo;
             const uint8_t* mo = mks + (i % 3) * 128;
             TY* yp = a.y + (plane3 * e + rowo);
             #pragma unroll
@@ -465,6 +522,9 @@ parity_zp(const __grid_constant__ OpArgs2<TC, TU, TE, TY, TR> args) {
         }
         // ---- the next planes: masks of plane e + 2 and moduli of element plane e + 1 land in their
         // spans, the next prefetches are issued
+        #pragma unroll
+        for (int k = 0; k < 3; ++k) { lo[k] = hi[k]; lon[k] = hin[k]; }
+        m_lo = m_hi;
         mask_put(m_pf, (i + 2) % 3);
         m_pf = mask_issue(e + 3);
         e_put(e_pf);

@@ -1,6 +1,6 @@
 """The node-column-pair operator kernel (parity_zp, the default for FP64 / FP32 iterates): every
 fused form against the oracle on ragged grids (tiles cut in y, z and x), and bitwise agreement with
-the two other streaming kernels, which compute the same operations in the same order.
+the element-plane-pair kernel, which computes the same operations in the same order.
 Tolerances: 1e-13 relative (FP64), 1e-5 (FP32) against the FP64 oracle; the kernels among
 themselves: bitwise."""
 import numpy as np
@@ -88,8 +88,8 @@ def test_every_form_matches_the_oracle(kernel, shape, dtype, tol):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-def test_three_kernels_agree(dtype):
-    """zp, wave and xp: FP32 outputs agree to the bit (packed f32x2 intrinsics, never contracted);
+def test_both_kernels_agree(dtype):
+    """zp and xp: FP32 outputs agree to the bit (packed f32x2 intrinsics, never contracted);
     FP64 outputs to 1e-15 of the largest entry (the compiler fuses different multiply-add pairs of
     the block product and the inverse Z stage into FMAs in each kernel).  The partial sums are
     grouped per CTA, so their totals agree to rounding only."""
@@ -102,12 +102,12 @@ def test_three_kernels_agree(dtype):
     outs = {}
     prev = _lib.set_stream_kernel("zp")
     try:
-        for kind in ("zp", "wave", "xp"):
+        for kind in ("zp", "xp"):
             _lib.set_stream_kernel(kind)
             outs[kind] = forms(op, ut, Et, nm, rt, invd)
     finally:
         _lib.set_stream_kernel(prev)
-    for kind in ("wave", "xp"):
+    for kind in ("xp",):
         for key in ("raw", "dirichlet", "jacobi", "residual", "apply_dot", "true_residual"):
             a_, b_ = outs["zp"][key], outs[kind][key]
             if dtype == torch.float32:
