@@ -364,11 +364,14 @@ def run_b200(args, rank, world, local_rank):
     uh = torch.empty(fh.numel(), dtype=torch.float64, pin_memory=True)       # the caller's result buffer
     for i in range(args.warmup + args.steps):
         torch.cuda.synchronize()
+        if i >= args.warmup:
+            torch.cuda.nvtx.range_push("e2e")             # ncu --nvtx --nvtx-include e2e/
         t0 = time.perf_counter()
         u, info = vx.solve(shape, Eh, fh, mh, precision=precision, levels=levels, out=uh, **api_kw)
         torch.cuda.synchronize()
         if i >= args.warmup:
             e2e.append(time.perf_counter() - t0)
+            torch.cuda.nvtx.range_pop()
     out["e2e"] = {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(Eh.numel() * 8 + fh.numel() * 8 + mh.numel() * 8),
                   "d2h_bytes_per_step": int(fh.numel() * 8),
                   "includes": "H2D of E/force/0-1 DOF mask from pinned memory, hierarchy refresh (moduli, masks, "

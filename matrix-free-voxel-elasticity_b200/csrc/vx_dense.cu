@@ -13,7 +13,9 @@
 //                     bw below it) forms the panel rows L_I = A_I L_kk^-T and L_J the same way (a
 //                     64 x 64 product with the block's inverse), writes L_I (diagonal tiles only),
 //                     and subtracts L_I L_J^T from the band;
-//   * band_inverse:   X = L^-1 column by column: a CTA owns 32 consecutive columns (one warp each),
+//   * band_inverse_blocked: X = L^-1 by blocks of 32 rows x 32 columns, a band GEMM per block and
+//                     the diagonal block inverses band_potrf kept (bands up to about 600 wide);
+//   * band_inverse:   (wider bands) X = L^-1 column by column: a CTA owns 32 consecutive columns (one warp each),
 //                     streams the band rows of L through shared memory by cp.async, and each warp
 //                     runs the forward substitution x_i = -(sum_p L[i][p] x_p) / L[i][i] over the
 //                     window of its last bw + 1 values; every x_i goes to M[i][j] and M[j][i].
@@ -45,69 +47,109 @@ __global__ void band_load_kernel(int n, int bw, const double* __restrict__ A, do
 // inverse goes to dinv (CB x CB, row-major, lower triangle), and the block column's rows below it
 // (the A values band_update turns into the panel) to apanel ((bw + 1) x CB), so that band_update
 // can store finished panel rows in place while other tiles still read the originals.
-// Thread r < CB owns row r of the block (right-looking: two barriers per column); the inverse is
-// column-parallel (thread c runs the forward substitution of column c, no barrier); every thread
-// shares the copies.
-// Dynamic shared memory: D and X, CB x CBP each.
+// The block's CB pivots are a chain of dependent steps, so it is factored by CB threads with the
+// rows in registers (right-looking; thread i holds row i; per pivot: the pivot thread's square root
+// and reciprocal, a named barrier of the two warps, the column through shared memory, a rank-1
+// update of the row in registers); a block smaller than CB (the last) is padded with the identity.
+// The inverse then needs no barrier: thread c runs the forward substitution of column c of X =
+// L^-1 in registers, reading the rows of L from shared memory.  Every loop is unrolled, so the
+// row and column registers are addressed at compile time (a variant with the pivot loop rolled and
+// predicated register selects spilled).
+__device__ __forceinline__ void potrf_bar() { asm volatile("bar.sync 1, %0;" ::"n"(CB) : "memory"); }
+
 __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int k0, double* __restrict__ lb,
                                                              double* __restrict__ dinv, double* __restrict__ apanel,
                                                              int* __restrict__ info) {
+    static_assert(CB == 64 && POTRF_T >= CB, "two factoring warps");
     vx::pdl_begin();
     extern __shared__ __align__(16) double psm[];
+    __shared__ double colj[CB], rinv[CB];
     double (*D)[CBP] = reinterpret_cast<double (*)[CBP]>(psm);
     double (*X)[CBP] = reinterpret_cast<double (*)[CBP]>(psm + CB * CBP);
     const int w = min(CB, n - k0);
     const int base = k0 + w, rend = min(n, k0 + w + bw);
     const int t = threadIdx.x;
+    #pragma unroll 8
     for (int i = t; i < (rend - base) * CB; i += POTRF_T) {
         const int r = base + i / CB, c = i % CB, col = k0 + c;
         apanel[i] = (c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
     }
+    #pragma unroll
     for (int i = t; i < CB * CB; i += POTRF_T) {
         const int r = i / CB, c = i % CB;
-        D[r][c] = (r < w && c <= r && r - c <= bw) ? lb[bidx(k0 + r, k0 + c, bw)] : 0.0;
-        X[r][c] = 0.0;
+        double v = 0.0;
+        if (r < w) v = (c <= r && r - c <= bw) ? lb[bidx(k0 + r, k0 + c, bw)] : 0.0;
+        else if (r == c) v = 1.0;                      // identity padding of a short block
+        D[r][c] = v;
     }
     __syncthreads();
-    for (int j = 0; j < w; ++j) {
-        double d = D[j][j];
-        if (!(d > 0.0)) {                                     // not positive definite: flag, keep finite
-            if (t == j) atomicCAS(info, 0, k0 + j + 1);
-            d = 1.0;
+    if (t < CB) {
+        double a[CB];
+        #pragma unroll
+        for (int c = 0; c < CB; ++c) a[c] = D[t][c];
+        #pragma unroll
+        for (int j = 0; j < CB; ++j) {
+            if (t == j) {
+                double d = a[j];
+                if (!(d > 0.0)) {                      // not positive definite: flag, keep finite
+                    if (j < w) atomicCAS(info, 0, k0 + j + 1);
+                    d = 1.0;
+                }
+                const double piv = sqrt(d);
+                a[j] = piv;
+                rinv[j] = 1.0 / piv;
+            }
+            potrf_bar();
+            if (t > j) {
+                a[j] *= rinv[j];                       // L[t][j]
+                colj[t] = a[j];
+            }
+            potrf_bar();
+            if (t > j) {
+                const double l = a[j];
+                #pragma unroll
+                for (int c = j + 1; c < CB; ++c) a[c] -= l * colj[c];   // c > t: never read (upper part)
+            }
+            potrf_bar();                               // colj is rewritten by the next pivot
         }
-        const double piv = sqrt(d);
-        if (t > j && t < w) D[t][j] = D[t][j] / piv;          // column j of L below the pivot
-        __syncthreads();
-        if (t == j) D[j][j] = piv;
-        if (t > j && t < w) {
-            const double l = D[t][j];
-            for (int c = j + 1; c <= t; ++c) D[t][c] -= l * D[c][j];
-        }
-        __syncthreads();
-    }
-    // inverse of the lower-triangular block, column c by thread c:
-    // X[c][c] = 1 / D[c][c], X[r][c] = -(sum_{c<=p<r} D[r][p] X[p][c]) / D[r][r]
-    if (t < w) {
-        X[t][t] = 1.0 / D[t][t];
-        for (int r = t + 1; r < w; ++r) {
-            double s = 0.0;
-            for (int p = t; p < r; ++p) s += D[r][p] * X[p][t];
-            X[r][t] = -s / D[r][r];
-        }
+        #pragma unroll
+        for (int c = 0; c < CB; ++c) D[t][c] = c <= t ? a[c] : 0.0;
     }
     __syncthreads();
+    if (t < CB) {                                       // column t of X = L^-1
+        double x[CB];
+        #pragma unroll
+        for (int r = 0; r < CB; ++r) {
+            double s0 = 0.0, s1 = 0.0;
+            #pragma unroll
+            for (int p = 0; p + 1 < r; p += 2) {
+                s0 += D[r][p] * x[p];
+                s1 += D[r][p + 1] * x[p + 1];
+            }
+            if (r & 1) s0 += D[r][r - 1] * x[r - 1];
+            x[r] = ((r == t ? 1.0 : 0.0) - (s0 + s1)) * rinv[r];
+        }
+        #pragma unroll
+        for (int r = 0; r < CB; ++r) X[r][t] = x[r];
+    }
+    __syncthreads();
+    #pragma unroll
     for (int i = t; i < CB * CB; i += POTRF_T) {
         const int r = i / CB, c = i % CB;
         if (r < w && c <= r && r - c <= bw) lb[bidx(k0 + r, k0 + c, bw)] = D[r][c];
-        dinv[i] = X[r][c];
+        dinv[i] = (r < w && c < w) ? X[r][c] : 0.0;
     }
 }
 
 // One lower tile (I, J) of the rows below block column k0: rows ri = base + I*CB + r, rj = base +
 // J*CB + c, base = k0 + w.  Dynamic shared memory: the block inverse and the two panels (3 CB x CBP).
+// Thread t computes a 4 x 4 register block of every product: rows t / 16 + 16 a, columns t % 16 +
+// 16 b (a, b < 4), so each step of a sum loads 8 values for 16 (or 32) multiply-adds and the
+// accumulations run as independent chains.
 __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, int k0, int tiles,
                                                                double* __restrict__ lb, const double* __restrict__ dinv,
                                                                const double* __restrict__ apanel) {
+    static_assert(UPDATE_T == 256 && CB == 64, "16 x 16 threads, 4 x 4 outputs each");
     vx::pdl_begin();
     extern __shared__ __align__(16) double sm[];
     double (*Xi)[CBP] = reinterpret_cast<double (*)[CBP]>(sm);
@@ -122,6 +164,7 @@ __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, in
     const int rend = min(n, k0 + w + bw);              // rows the block column reaches
     const int ri0 = base + I * CB, rj0 = base + J * CB;
     if (ri0 >= rend) return;                           // (never: the grid covers the window exactly)
+    #pragma unroll
     for (int t = threadIdx.x; t < CB * CB; t += UPDATE_T) {
         const int r = t / CB, c = t % CB;
         Xi[r][c] = dinv[t];
@@ -130,26 +173,38 @@ __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, in
         PJ[r][c] = rj < rend ? apanel[int64_t(rj - base) * CB + c] : 0.0;
     }
     __syncthreads();
-    // panels: P <- P X^T (P[r][m] = sum_{p<=m} A[r][p] X[m][p]); 16 outputs per thread, then written back
-    constexpr int PER = CB * CB / UPDATE_T;
-    double oi[PER], oj[PER];
+    const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
+    // panels: P <- P X^T, P[r][m] = sum_p A[r][p] X[m][p] (X lower triangular: the full sum is exact)
+    double oi[4][4], oj[4][4];
     #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int t = threadIdx.x + q * UPDATE_T, r = t / CB, m = t % CB;
-        double si = 0.0, sj = 0.0;
-        for (int p = 0; p <= m; ++p) {
-            si += PI[r][p] * Xi[m][p];
-            sj += PJ[r][p] * Xi[m][p];
+    for (int a = 0; a < 4; ++a) {
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) { oi[a][b] = 0.0; oj[a][b] = 0.0; }
+    }
+    #pragma unroll 4
+    for (int p = 0; p < CB; ++p) {
+        double ai[4], aj[4], x[4];
+        #pragma unroll
+        for (int a = 0; a < 4; ++a) { ai[a] = PI[tr + 16 * a][p]; aj[a] = PJ[tr + 16 * a][p]; }
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) x[b] = Xi[tc + 16 * b][p];
+        #pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            #pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                oi[a][b] = fma(ai[a], x[b], oi[a][b]);
+                oj[a][b] = fma(aj[a], x[b], oj[a][b]);
+            }
         }
-        oi[q] = si;
-        oj[q] = sj;
     }
     __syncthreads();
     #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int t = threadIdx.x + q * UPDATE_T, r = t / CB, m = t % CB;
-        PI[r][m] = oi[q];
-        PJ[r][m] = oj[q];
+    for (int a = 0; a < 4; ++a) {
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            PI[tr + 16 * a][tc + 16 * b] = oi[a][b];
+            PJ[tr + 16 * a][tc + 16 * b] = oj[a][b];
+        }
     }
     __syncthreads();
     if (I == J) {                                      // the panel rows of tile I are final: store them
@@ -159,12 +214,33 @@ __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, in
         }
     }
     // trailing update of the tile: A[ri][rj] -= sum_m L[ri][m] L[rj][m] (lower triangle, in the band)
-    for (int t = threadIdx.x; t < CB * CB; t += UPDATE_T) {
-        const int r = t / CB, c = t % CB, ri = ri0 + r, rj = rj0 + c;
-        if (ri >= rend || rj >= rend || rj > ri || ri - rj > bw) continue;
-        double s = 0.0;
-        for (int m = 0; m < w; ++m) s += PI[r][m] * PJ[c][m];
-        lb[bidx(ri, rj, bw)] -= s;
+    double o[4][4];
+    #pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) o[a][b] = 0.0;
+    }
+    #pragma unroll 4
+    for (int m = 0; m < CB; ++m) {
+        double pi[4], pj[4];
+        #pragma unroll
+        for (int a = 0; a < 4; ++a) pi[a] = PI[tr + 16 * a][m];
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) pj[b] = PJ[tc + 16 * b][m];
+        #pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            #pragma unroll
+            for (int b = 0; b < 4; ++b) o[a][b] = fma(pi[a], pj[b], o[a][b]);
+        }
+    }
+    #pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int ri = ri0 + tr + 16 * a, rj = rj0 + tc + 16 * b;
+            if (ri >= rend || rj >= rend || rj > ri || ri - rj > bw) continue;
+            lb[bidx(ri, rj, bw)] -= o[a][b];
+        }
     }
 }
 
@@ -240,6 +316,110 @@ __global__ void band_inverse_kernel(int n, int bw, const double* __restrict__ lb
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// X = L^-1 by blocks of IRB rows for ITC columns per CTA (columns c0 .. c0 + ITC - 1).  Walking down
+// the row blocks i0 = c0, c0 + IRB, ...:
+//     S   = L[i0 .. i0 + IRB)[i0 - bw .. i0) X[i0 - bw .. i0)[cols]     (the band left of the block)
+//     X_I = Dinv_I (E_I - S)                                          (E_I: the identity's rows)
+// with Dinv_I the inverse of L's IRB x IRB diagonal block (the diagonal sub-blocks of the CB-block
+// inverses band_potrf kept, dinv_all).  The last WR >= bw + IRB rows of X for these columns live in a
+// shared-memory ring (rows above c0 are zero and never written); the band rows of L are staged per
+// block; each finished block goes to M[i][j] (rows, coalesced over columns) and, through shared memory,
+// to M[j][i] (coalesced over rows).  Thread t: column t % 32, rows t / 32 + 8 m (m < 4).
+constexpr int IRB = 32, ITC = 32, INVB_T = 256;
+
+struct InvbLayout {
+    int bw, WR;
+    size_t ls, ring, dv, st, bytes;
+    __host__ __device__ explicit InvbLayout(int bw_) : bw(bw_) {
+        WR = (bw + IRB + IRB - 1) / IRB * IRB;
+        ls = size_t(IRB) * (bw + 1);                 // staged band rows, padded
+        ring = size_t(WR) * ITC;
+        dv = size_t(IRB) * (IRB + 1);
+        st = size_t(IRB) * (ITC + 1);
+        bytes = (ls + ring + dv + st) * sizeof(double);
+    }
+};
+
+__global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int bw, const double* __restrict__ lb,
+                                                                      const double* __restrict__ dinv_all,
+                                                                      double* __restrict__ packed) {
+    vx::pdl_begin();
+    extern __shared__ __align__(16) double sm[];
+    const InvbLayout Lo(bw);
+    const int LSW = bw + 1;
+    double* Ls = sm;                                   // [IRB][bw + 1]: Ls[r][q] = L[i0 + r][i0 - bw + q], q < bw
+    double* Wr = Ls + Lo.ls;                           // [WR][ITC] ring of X rows
+    double* Dv = Wr + Lo.ring;                         // [IRB][IRB + 1]
+    double* St = Dv + Lo.dv;                           // [IRB][ITC + 1]
+    const int t = threadIdx.x, c = t & 31, rg = t >> 5;
+    const int c0 = blockIdx.x * ITC;
+    const int WR = Lo.WR;
+    for (int i = t; i < WR * ITC; i += INVB_T) Wr[i] = 0.0;
+    for (int i0 = c0; i0 < n; i0 += IRB) {
+        __syncthreads();                               // the previous block's reads of Ls, Dv, St are done
+        // stage the band rows (zero outside row i's band and beyond n) and the diagonal block inverse
+        for (int i = t; i < IRB * bw; i += INVB_T) {
+            const int r = i / bw, q = i % bw, row = i0 + r;
+            Ls[r * LSW + q] = (q >= r && row < n) ? lb[int64_t(row) * (bw + 1) + (q - r)] : 0.0;
+        }
+        const double* dsrc = dinv_all + int64_t(i0 / CB) * CB * CB + (i0 % CB) * CB + (i0 % CB);
+        for (int i = t; i < IRB * IRB; i += INVB_T) {
+            const int r = i / IRB, k = i % IRB;
+            Dv[r * (IRB + 1) + k] = (k <= r) ? dsrc[r * CB + k] : 0.0;
+        }
+        __syncthreads();
+        // S = Ls X_window over the band columns that can be non-zero (rows >= c0)
+        const int q0 = max(0, c0 - (i0 - bw));
+        double s[4] = {0.0, 0.0, 0.0, 0.0};
+        int slot = (i0 - bw + q0) % WR;
+        if (slot < 0) slot += WR;
+        for (int q = q0; q < bw; ++q) {
+            const double x = Wr[slot * ITC + c];
+            #pragma unroll
+            for (int m = 0; m < 4; ++m) s[m] += Ls[(rg + 8 * m) * LSW + q] * x;
+            if (++slot == WR) slot = 0;
+        }
+        #pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int r = rg + 8 * m;
+            St[r * (ITC + 1) + c] = ((i0 + r == c0 + c) ? 1.0 : 0.0) - s[m];
+        }
+        __syncthreads();
+        // X_I = Dinv_I (E_I - S)
+        double x[4];
+        #pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int r = rg + 8 * m;
+            double a0 = 0.0, a1 = 0.0;
+            int k = 0;
+            for (; k + 1 <= r; k += 2) {
+                a0 += Dv[r * (IRB + 1) + k] * St[k * (ITC + 1) + c];
+                a1 += Dv[r * (IRB + 1) + k + 1] * St[(k + 1) * (ITC + 1) + c];
+            }
+            if (k == r) a0 += Dv[r * (IRB + 1) + k] * St[k * (ITC + 1) + c];
+            x[m] = a0 + a1;
+        }
+        __syncthreads();                               // every read of St done before it holds X_I
+        #pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int r = rg + 8 * m, i = i0 + r, j = c0 + c;
+            const bool ok = i < n && j < n && i >= j;
+            const double v = ok ? x[m] : 0.0;
+            int ws = i % WR;
+            Wr[ws * ITC + c] = v;
+            St[r * (ITC + 1) + c] = v;
+            if (ok) packed[int64_t(i) * n + j] = v;    // lower part, coalesced over columns
+        }
+        __syncthreads();
+        // upper part M[j][i] = X[i][j], coalesced over rows: lane = row of the block
+        #pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int cc = rg + 8 * m, r = c, i = i0 + r, j = c0 + cc;
+            if (i < n && j < n && i > j) packed[int64_t(j) * n + i] = St[r * (ITC + 1) + cc];
+        }
+    }
+}
+
 int inverse_warps(int bw) {
     const size_t budget = 227 * 1024;
     const size_t row = size_t(bw + 1) * sizeof(double);
@@ -256,7 +436,8 @@ using namespace vx;
 extern "C" int64_t vx_coarse_factor_workspace(int n, int bw) {
     if (n <= 0 || bw < 0) return -1;
     bw = std::min(bw, n - 1);
-    return int64_t(n) * (bw + 1) + int64_t(CB) * CB + int64_t(bw + 1) * CB;
+    const int64_t nblk = (n + CB - 1) / CB;
+    return int64_t(n) * (bw + 1) + nblk * CB * CB + int64_t(bw + 1) * CB;
 }
 
 extern "C" int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* work, int* info,
@@ -268,8 +449,8 @@ extern "C" int vx_coarse_factor(int n, int bw, const double* A, double* packed, 
     const int nw = inverse_warps(bw);
     VX_CHECK_ARG(nw > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_factor: bandwidth %d is too wide", bw);
     double* lb = work;
-    double* dinv = work + int64_t(n) * (bw + 1);
-    double* apanel = dinv + int64_t(CB) * CB;
+    double* dinv_all = work + int64_t(n) * (bw + 1);                  // every diagonal block's inverse
+    double* apanel = dinv_all + int64_t((n + CB - 1) / CB) * CB * CB;
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), stream);
     if (e != cudaSuccess) {
         set_error("vx_coarse_factor: memset: %s", cudaGetErrorString(e));
@@ -286,6 +467,7 @@ extern "C" int vx_coarse_factor(int n, int bw, const double* A, double* packed, 
     const int64_t band = int64_t(n) * (bw + 1);
     vx::launch(band_load_kernel, unsigned((band + 255) / 256), 256, 0, stream, n, bw, A, lb);
     for (int k0 = 0; k0 < n; k0 += CB) {
+        double* dinv = dinv_all + int64_t(k0 / CB) * CB * CB;
         vx::launch(band_potrf_kernel, 1, POTRF_T, psm, stream, n, bw, k0, lb, dinv, apanel, info);
         const int w = std::min(CB, n - k0);
         const int rows = std::min(n, k0 + w + bw) - (k0 + w);
@@ -294,8 +476,17 @@ extern "C" int vx_coarse_factor(int n, int bw, const double* A, double* packed, 
         vx::launch(band_update_kernel, unsigned(T * (T + 1) / 2), UPDATE_T, usm, stream, n, bw, k0, T, lb,
                    (const double*)dinv, (const double*)apanel);
     }
-    vx::launch(band_inverse_kernel, unsigned((n + nw - 1) / nw), unsigned(nw * 32), ism, stream, n, bw,
-               (const double*)lb, packed);
+    const InvbLayout il(bw);
+    if (il.bytes <= 227 * 1024) {
+        static std::atomic<uint64_t> opt_b;
+        st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, "vx_coarse_factor");
+        if (st) return st;
+        vx::launch(band_inverse_blocked_kernel, unsigned((n + ITC - 1) / ITC), INVB_T, il.bytes, stream, n, bw,
+                   (const double*)lb, (const double*)dinv_all, packed);
+    } else {
+        vx::launch(band_inverse_kernel, unsigned((n + nw - 1) / nw), unsigned(nw * 32), ism, stream, n, bw,
+                   (const double*)lb, packed);
+    }
     VX_CHECK_LAUNCH("vx_coarse_factor");
     return VX_OK;
 }

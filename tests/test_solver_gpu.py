@@ -336,11 +336,13 @@ def test_voxel_mg_fast_route_speed_128x64x64():
     assert t_mirror <= 1.2 * t_solver + 2e-4, (t_mirror, t_solver)
 
 
-@pytest.mark.parametrize("n,bw", [(1, 0), (5, 4), (70, 9), (200, 63), (517, 64), (1000, 130), (1911, 275)])
+@pytest.mark.parametrize("n,bw", [(1, 0), (5, 4), (70, 9), (200, 63), (517, 64), (1000, 130), (1911, 275),
+                                  (5700, 335), (1500, 700)])
 def test_banded_coarse_factor_matches_the_dense_inverse_factor(n, bw):
     """vx_coarse_factor (banded Cholesky + banded forward substitution, no library call) gives the
     packed tril(L^-1) + triu(L^-T, 1) of a banded SPD matrix to FP64 rounding, for sizes that are
-    not multiples of the 64-column block and bands narrower and wider than a block."""
+    not multiples of the 64-column block and bands narrower and wider than a block (the coarsest
+    matrix of 576x288x288 is n 5700, bw 335; a band of 700 takes the column-by-column inverse)."""
     rng = np.random.default_rng(n + bw)
     B = np.zeros((n, n))
     for k in range(bw + 1):
