@@ -295,6 +295,13 @@ int vx_tc_status(int* status, int clear);
  * (about 5800) are rejected with VX_ERR_INVALID_ARGUMENT ("too wide"). */
 int64_t vx_coarse_factor_workspace(int n, int bw);
 int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* work, int* info, cudaStream_t stream);
+/* Several coarsest systems of one size at once (a serving batch's per-job coarse solves), every
+ * launch of the factorisation covering all of them: slots (host, `count` entries) index the n x n
+ * matrix stacks A and packed (slot k at k n^2) and info (slot k at k); work holds `count` workspaces
+ * of vx_coarse_factor_workspace(n, bw) doubles.  Results equal vx_coarse_factor's on each matrix.
+ * No counterpart in the reference. */
+int vx_batch_coarse_factor(int n, int bw, int count, const int* slots, const double* A, double* packed,
+                           double* work, int* info, cudaStream_t stream);
 
 /* ---------------------------------------------------------------------------- batches
  * `slots` independent systems of one size solved in lockstep (the serving loop's batches): slot k's

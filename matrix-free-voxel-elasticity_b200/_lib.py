@@ -59,6 +59,7 @@ SIGNATURES = {
     "vx_tc_status": (c_int, [POINTER(c_int), c_int]),
     "vx_coarse_factor_workspace": (c_int64, [c_int, c_int]),
     "vx_coarse_factor": (c_int, [c_int, c_int, _P, _P, _P, _P, _P]),
+    "vx_batch_coarse_factor": (c_int, [c_int, c_int, c_int, POINTER(c_int), _P, _P, _P, _P, _P]),
     # batches of independent systems
     "vx_batch_finalize": (c_int, [c_int, c_int64, c_int, _P, c_int64, _P, _P]),
     "vx_batch_cg_update": (c_int, [c_int, c_int64, c_int, c_int64, _P, _P, _P, _P, _P, c_int, _P]),
@@ -162,7 +163,7 @@ def call(name: str, *args) -> None:
     if fn is None:
         fn = _FNS[name] = getattr(load(), name)
     check(fn(*args), name)
-    if name == "vx_coarse_factor":          # band load, a factor and an update per 64-column block, inverse
+    if name in ("vx_coarse_factor", "vx_batch_coarse_factor"):   # load, a factor and an update per block, inverse
         launches += 2 * ((int(args[0]) + 63) // 64) + 1
     elif name not in HOST_ONLY:
         launches += KERNELS_PER_CALL.get(name, 1)

@@ -121,7 +121,6 @@ class BatchedSolver:
         self.stream = torch.cuda.Stream()
         self._graph = None
         self._event = None
-        self._job_ops = [VoxelOperator(s_, self.ke * 2 ** l, torch.float64) for l, s_ in enumerate(geo.job_shapes)]
 
     def footprint_bytes(self) -> int:
         n = self.op.ndof
@@ -178,7 +177,11 @@ class BatchedSolver:
             for k, E, f, tol in jobs:
                 self.modulus(k).copy_(torch.as_tensor(E).to(device="cuda", dtype=torch.float64).reshape(-1))
                 self.seg(self.b, k).copy_(torch.as_tensor(f).to(device="cuda", dtype=torch.float64).reshape(-1))
-                self._refresh_slot(k)
+            # every level's moduli and diagonals in one launch per level (the other slots' values come
+            # out unchanged), then the new slots' coarsest systems factored side by side
+            self.M.refresh_levels()
+            self.M.refresh_blocks([k for k, *_ in jobs])
+            for k, E, f, tol in jobs:
                 self.seg(self.x, k).zero_()
                 self.seg(self.p, k).zero_()
                 self.seg(self.z_old, k).zero_()
@@ -198,26 +201,6 @@ class BatchedSolver:
                 _lib.call("vx_solver_finalize", FIN_RZ, self.G, part, S_k, _s())
                 _lib.call("vx_cg_direction", _lib.VX_F64, self.zprec, self.n_job, S_k, self.seg(z, k).data_ptr(),
                           self.seg(self.p, k).data_ptr(), self.seg(self.z_old, k).data_ptr(), _s())   # beta = 0
-
-    def _refresh_slot(self, k):
-        """Slot k's moduli and inverse diagonals on every level, and its coarsest factor."""
-        M = self.M
-        for l, (L, js) in enumerate(zip(M.levels, self.geo.job_shapes)):
-            jx, jy, jz = js
-            pitch_l = self.pitch >> l
-            e_off = k * pitch_l * jy * jz
-            n_off = k * pitch_l * (jy + 1) * (jz + 1)
-            ne, nn = jx * jy * jz, (jx + 1) * (jy + 1) * (jz + 1)
-            if l:
-                P, (px, py, pz) = M.levels[l - 1], self.geo.job_shapes[l - 1]
-                pe = k * (self.pitch >> (l - 1)) * py * pz
-                _lib.call("vx_coarsen_modulus", _lib.VX_F64, px, py, pz, P.E64.data_ptr() + 8 * pe,
-                          L.E64.data_ptr() + 8 * e_off, _s())
-            if L.E.data_ptr() != L.E64.data_ptr():
-                L.E[e_off:e_off + ne].copy_(L.E64[e_off:e_off + ne])
-            inv = self._job_ops[l].diagonal(L.E64[e_off:e_off + ne], L.mask[n_off:n_off + nn], inverse=True)
-            L.invd[3 * n_off:3 * (n_off + nn)].copy_(inv)
-        M.refresh_block(k)
 
     def run(self, iterations=None):
         """Enqueue `iterations` (default: the captured chunk) fcg iterations for every slot on the
@@ -261,12 +244,16 @@ class BatchedSolver:
 
     def result(self, k):
         """(x_k copy, iterations, converged, rel, compliance f_k . x_k) of slot k, after poll()."""
-        s = self.S_host.numpy()[k]
+        return self.results([k])[0]
+
+    def results(self, ks):
+        """result() of several slots with one synchronisation."""
+        S = self.S_host.numpy()
         with torch.cuda.stream(self.stream):
-            x = self.seg(self.x, k).clone()
-            comp = torch.dot(self.seg(self.b, k), x)
-        self.stream.synchronize()
-        return x, int(s[S_IT]), bool(s[S_REL] <= s[S_TOL]), float(s[S_REL]), float(comp)
+            xs = [self.seg(self.x, k).clone() for k in ks]
+            comps = torch.stack([torch.dot(self.seg(self.b, k), x) for k, x in zip(ks, xs)]).cpu() if ks else []
+        return [(x, int(S[k, S_IT]), bool(S[k, S_REL] <= S[k, S_TOL]), float(S[k, S_REL]), float(c))
+                for k, x, c in zip(ks, xs, comps)]
 
     def retire(self, k):
         """Slot k becomes free (its work stays a no-op until a new job is admitted)."""

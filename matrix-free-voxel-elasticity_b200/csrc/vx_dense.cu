@@ -35,8 +35,45 @@ constexpr int INV_STAGES = 4;     // L rows in flight in band_inverse
 
 __device__ __forceinline__ int64_t bidx(int i, int j, int bw) { return int64_t(i) * (bw + 1) + (j - i + bw); }
 
-__global__ void band_load_kernel(int n, int bw, const double* __restrict__ A, double* __restrict__ lb) {
+// Several factorisations of one size run side by side, factorisation m = blockIdx.y of every launch:
+// matrix slot[m] of A (and packed, info), workspace m of `work` (the band, the diagonal block
+// inverses, the panel copy).
+constexpr int FB_MAX = 64;
+struct FactorBatch {
+    const double* A;
+    double* packed;
+    double* work;
+    int* info;
+    int64_t mat;             // doubles from one matrix slot to the next (n * n)
+    int64_t ws;              // doubles of one workspace
+    int nblk;                // CB-column blocks
+    int slot[FB_MAX];
+};
+struct FactorPtrs {
+    const double* A;
+    double* packed;
+    double* lb;
+    double* dinv_all;
+    double* apanel;
+    int* info;
+};
+__device__ __forceinline__ FactorPtrs fptrs(const FactorBatch& fb, int n, int bw) {
+    const int m = blockIdx.y, s = fb.slot[m];
+    FactorPtrs p;
+    p.A = fb.A + s * fb.mat;
+    p.packed = fb.packed + s * fb.mat;
+    p.lb = fb.work + m * fb.ws;
+    p.dinv_all = p.lb + int64_t(n) * (bw + 1);
+    p.apanel = p.dinv_all + int64_t(fb.nblk) * CB * CB;
+    p.info = fb.info + s;
+    return p;
+}
+
+__global__ void band_load_kernel(int n, int bw, const __grid_constant__ FactorBatch fb) {
     vx::pdl_begin();
+    const FactorPtrs P = fptrs(fb, n, bw);
+    const double* __restrict__ A = P.A;
+    double* __restrict__ lb = P.lb;
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= int64_t(n) * (bw + 1)) return;
     const int i = int(t / (bw + 1)), c = int(t % (bw + 1)), j = i - bw + c;
@@ -57,11 +94,14 @@ __global__ void band_load_kernel(int n, int bw, const double* __restrict__ A, do
 // predicated register selects spilled).
 __device__ __forceinline__ void potrf_bar() { asm volatile("bar.sync 1, %0;" ::"n"(CB) : "memory"); }
 
-__global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int k0, double* __restrict__ lb,
-                                                             double* __restrict__ dinv, double* __restrict__ apanel,
-                                                             int* __restrict__ info) {
+__global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int k0, const __grid_constant__ FactorBatch fb) {
     static_assert(CB == 64 && POTRF_T >= CB, "two factoring warps");
     vx::pdl_begin();
+    const FactorPtrs P = fptrs(fb, n, bw);
+    double* __restrict__ lb = P.lb;
+    double* __restrict__ dinv = P.dinv_all + int64_t(k0 / CB) * CB * CB;
+    double* __restrict__ apanel = P.apanel;
+    int* __restrict__ info = P.info;
     extern __shared__ __align__(16) double psm[];
     __shared__ double colj[CB], rinv[CB];
     double (*D)[CBP] = reinterpret_cast<double (*)[CBP]>(psm);
@@ -147,10 +187,13 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
 // 16 b (a, b < 4), so each step of a sum loads 8 values for 16 (or 32) multiply-adds and the
 // accumulations run as independent chains.
 __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, int k0, int tiles,
-                                                               double* __restrict__ lb, const double* __restrict__ dinv,
-                                                               const double* __restrict__ apanel) {
+                                                               const __grid_constant__ FactorBatch fb) {
     static_assert(UPDATE_T == 256 && CB == 64, "16 x 16 threads, 4 x 4 outputs each");
     vx::pdl_begin();
+    const FactorPtrs P = fptrs(fb, n, bw);
+    double* __restrict__ lb = P.lb;
+    const double* __restrict__ dinv = P.dinv_all + int64_t(k0 / CB) * CB * CB;
+    const double* __restrict__ apanel = P.apanel;
     extern __shared__ __align__(16) double sm[];
     double (*Xi)[CBP] = reinterpret_cast<double (*)[CBP]>(sm);
     double (*PI)[CBP] = reinterpret_cast<double (*)[CBP]>(sm + CB * CBP);
@@ -258,8 +301,11 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 // X = L^-1 into the packed matrix (lower part X, upper part X^T).  CTA = nw warps, columns
 // j0 .. j0+nw-1 (warp w: column j0 + w); shared memory: INV_STAGES staged band rows of L, then one
 // window of bw + 1 values per warp (x_p of its column at slot p mod (bw + 1)).
-__global__ void band_inverse_kernel(int n, int bw, const double* __restrict__ lb, double* __restrict__ packed) {
+__global__ void band_inverse_kernel(int n, int bw, const __grid_constant__ FactorBatch fb) {
     vx::pdl_begin();
+    const FactorPtrs P = fptrs(fb, n, bw);
+    const double* __restrict__ lb = P.lb;
+    double* __restrict__ packed = P.packed;
     extern __shared__ __align__(16) double sm[];
     const int W = bw + 1;
     const int nw = blockDim.x >> 5;
@@ -340,10 +386,12 @@ struct InvbLayout {
     }
 };
 
-__global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int bw, const double* __restrict__ lb,
-                                                                      const double* __restrict__ dinv_all,
-                                                                      double* __restrict__ packed) {
+__global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int bw, const __grid_constant__ FactorBatch fb) {
     vx::pdl_begin();
+    const FactorPtrs P = fptrs(fb, n, bw);
+    const double* __restrict__ lb = P.lb;
+    const double* __restrict__ dinv_all = P.dinv_all;
+    double* __restrict__ packed = P.packed;
     extern __shared__ __align__(16) double sm[];
     const InvbLayout Lo(bw);
     const int LSW = bw + 1;
@@ -440,53 +488,84 @@ extern "C" int64_t vx_coarse_factor_workspace(int n, int bw) {
     return int64_t(n) * (bw + 1) + nblk * CB * CB + int64_t(bw + 1) * CB;
 }
 
-extern "C" int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* work, int* info,
-                                cudaStream_t stream) {
-    VX_CHECK_ARG(n > 0 && bw >= 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_factor: bad size n=%d bw=%d", n, bw);
-    VX_CHECK_ARG(A && packed && work && info, VX_ERR_NULL_POINTER, "vx_coarse_factor: NULL pointer");
-    VX_CHECK_ARG(A != packed, VX_ERR_INVALID_ARGUMENT, "vx_coarse_factor: packed may not alias A");
+// count factorisations of one size (matrix slots slots[0..count) of A, packed and info; workspace m
+// of work for the m-th), every launch covering all of them (blockIdx.y).
+static int coarse_factor_batch(const char* what, int n, int bw, int count, const int* slots, const double* A,
+                               double* packed, double* work, int* info, cudaStream_t stream) {
+    VX_CHECK_ARG(n > 0 && bw >= 0, VX_ERR_INVALID_ARGUMENT, "%s: bad size n=%d bw=%d", what, n, bw);
+    VX_CHECK_ARG(A && packed && work && info, VX_ERR_NULL_POINTER, "%s: NULL pointer", what);
+    VX_CHECK_ARG(A != packed, VX_ERR_INVALID_ARGUMENT, "%s: packed may not alias A", what);
+    VX_CHECK_ARG(count >= 1 && count <= FB_MAX, VX_ERR_INVALID_ARGUMENT, "%s: count %d outside 1..%d", what, count,
+                 FB_MAX);
     bw = std::min(bw, n - 1);
     const int nw = inverse_warps(bw);
-    VX_CHECK_ARG(nw > 0, VX_ERR_INVALID_ARGUMENT, "vx_coarse_factor: bandwidth %d is too wide", bw);
-    double* lb = work;
-    double* dinv_all = work + int64_t(n) * (bw + 1);                  // every diagonal block's inverse
-    double* apanel = dinv_all + int64_t((n + CB - 1) / CB) * CB * CB;
-    cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), stream);
-    if (e != cudaSuccess) {
-        set_error("vx_coarse_factor: memset: %s", cudaGetErrorString(e));
-        return VX_ERR_CUDA;
+    VX_CHECK_ARG(nw > 0, VX_ERR_INVALID_ARGUMENT, "%s: bandwidth %d is too wide", what, bw);
+    FactorBatch fb{};
+    fb.A = A;
+    fb.packed = packed;
+    fb.work = work;
+    fb.info = info;
+    fb.mat = int64_t(n) * n;
+    fb.ws = vx_coarse_factor_workspace(n, bw);
+    fb.nblk = (n + CB - 1) / CB;
+    for (int m = 0; m < count; ++m) {
+        VX_CHECK_ARG(slots[m] >= 0, VX_ERR_INVALID_ARGUMENT, "%s: negative slot", what);
+        fb.slot[m] = slots[m];
+        cudaError_t e = cudaMemsetAsync(info + slots[m], 0, sizeof(int), stream);
+        if (e != cudaSuccess) {
+            set_error("%s: memset: %s", what, cudaGetErrorString(e));
+            return VX_ERR_CUDA;
+        }
     }
     const size_t psm = size_t(2) * CB * CBP * sizeof(double);
     const size_t usm = size_t(3) * CB * CBP * sizeof(double);
     const size_t ism = size_t(INV_STAGES + nw) * (bw + 1) * sizeof(double);
-    static std::atomic<uint64_t> opt_p, opt_u, opt_i;
-    int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel, psm, "vx_coarse_factor");
-    if (!st) st = smem_opt_in(opt_u, (const void*)band_update_kernel, usm, "vx_coarse_factor");
-    if (!st) st = smem_opt_in(opt_i, (const void*)band_inverse_kernel, 227 * 1024, "vx_coarse_factor");
+    static std::atomic<uint64_t> opt_p, opt_u, opt_i, opt_b;
+    int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel, psm, what);
+    if (!st) st = smem_opt_in(opt_u, (const void*)band_update_kernel, usm, what);
+    if (!st) st = smem_opt_in(opt_i, (const void*)band_inverse_kernel, 227 * 1024, what);
+    if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, what);
     if (st) return st;
+    const unsigned B = unsigned(count);
     const int64_t band = int64_t(n) * (bw + 1);
-    vx::launch(band_load_kernel, unsigned((band + 255) / 256), 256, 0, stream, n, bw, A, lb);
+    vx::launch(band_load_kernel, dim3(unsigned((band + 255) / 256), B), 256, 0, stream, n, bw, fb);
     for (int k0 = 0; k0 < n; k0 += CB) {
-        double* dinv = dinv_all + int64_t(k0 / CB) * CB * CB;
-        vx::launch(band_potrf_kernel, 1, POTRF_T, psm, stream, n, bw, k0, lb, dinv, apanel, info);
+        vx::launch(band_potrf_kernel, dim3(1, B), POTRF_T, psm, stream, n, bw, k0, fb);
         const int w = std::min(CB, n - k0);
         const int rows = std::min(n, k0 + w + bw) - (k0 + w);
         if (rows <= 0) continue;
         const int T = (rows + CB - 1) / CB;
-        vx::launch(band_update_kernel, unsigned(T * (T + 1) / 2), UPDATE_T, usm, stream, n, bw, k0, T, lb,
-                   (const double*)dinv, (const double*)apanel);
+        vx::launch(band_update_kernel, dim3(unsigned(T * (T + 1) / 2), B), UPDATE_T, usm, stream, n, bw, k0, T, fb);
     }
     const InvbLayout il(bw);
     if (il.bytes <= 227 * 1024) {
-        static std::atomic<uint64_t> opt_b;
-        st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, "vx_coarse_factor");
-        if (st) return st;
-        vx::launch(band_inverse_blocked_kernel, unsigned((n + ITC - 1) / ITC), INVB_T, il.bytes, stream, n, bw,
-                   (const double*)lb, (const double*)dinv_all, packed);
+        vx::launch(band_inverse_blocked_kernel, dim3(unsigned((n + ITC - 1) / ITC), B), INVB_T, il.bytes, stream, n,
+                   bw, fb);
     } else {
-        vx::launch(band_inverse_kernel, unsigned((n + nw - 1) / nw), unsigned(nw * 32), ism, stream, n, bw,
-                   (const double*)lb, packed);
+        vx::launch(band_inverse_kernel, dim3(unsigned((n + nw - 1) / nw), B), unsigned(nw * 32), ism, stream, n, bw,
+                   fb);
     }
-    VX_CHECK_LAUNCH("vx_coarse_factor");
+    VX_CHECK_LAUNCH(what);
+    return VX_OK;
+}
+
+extern "C" int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* work, int* info,
+                                cudaStream_t stream) {
+    const int slot0 = 0;
+    return coarse_factor_batch("vx_coarse_factor", n, bw, 1, &slot0, A, packed, work, info, stream);
+}
+
+// Several coarsest systems of one size at once (the serving batches' per-job coarse solves): slots
+// are host indices into the matrix stacks A / packed (n x n each) and info; work holds count
+// workspaces of vx_coarse_factor_workspace(n, bw) doubles.
+extern "C" int vx_batch_coarse_factor(int n, int bw, int count, const int* slots, const double* A, double* packed,
+                                      double* work, int* info, cudaStream_t stream) {
+    VX_CHECK_ARG(slots, VX_ERR_NULL_POINTER, "vx_batch_coarse_factor: NULL slots");
+    VX_CHECK_ARG(count >= 1, VX_ERR_INVALID_ARGUMENT, "vx_batch_coarse_factor: count %d", count);
+    for (int c0 = 0; c0 < count; c0 += FB_MAX) {      // chunks reuse the workspaces, in stream order
+        const int st = coarse_factor_batch("vx_batch_coarse_factor", n, bw, std::min(FB_MAX, count - c0), slots + c0, A,
+                                           packed, work, info, stream);
+        if (st) return st;
+    }
     return VX_OK;
 }

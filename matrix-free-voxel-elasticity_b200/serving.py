@@ -318,15 +318,28 @@ def default_slots(shape, max_slots=16, dofs_per_batch=32e6):
     return int(max(1, min(max_slots, dofs_per_batch // per)))
 
 
+def batch_ladder(max_slots):
+    """Capacities of a shape's batches: 1, 2, 4, ... up to max_slots (the last one max_slots)."""
+    caps, c = [], 1
+    while c < max_slots:
+        caps.append(c)
+        c *= 2
+    caps.append(int(max_slots))
+    return caps
+
+
 def serve_batched(requests, shapes=None, slots=None, precision="mixed", chunk=4, maxiter=200, budget_bytes=150e9,
                   prewarm=None, keep_solution=False, clock=time.perf_counter, poll_s=50e-6):
-    """Continuous batching with fused launches: one batch.BatchedSolver per grid shape (its own stream
-    and captured chunk graph) holds up to slots[shape] jobs; every kernel of a chunk serves all the
-    shape's jobs at once.  Requests are admitted FIFO per shape into free slots between chunks,
-    finished jobs leave their slot at once, and the shapes' batches run concurrently.  A shape's
-    batch is built on its first request unless listed in `prewarm` (default: every shape), so a
-    cold shape pays its set-up inside the stream.  The batches' footprint must fit the budget.
-    Returns (completions sorted by request id, summary)."""
+    """Continuous batching with fused launches.  Each grid shape has a ladder of batch.BatchedSolvers
+    of capacities 1, 2, 4, ... up to slots[shape] (batch_ladder), each with its own stream and
+    captured chunk graph; every kernel of a chunk serves all the jobs of its batch at once.  A batch
+    costs what its capacity costs, whatever its occupancy, so arrivals go where they waste least:
+    between chunks, requests that have arrived fill the free slots of batches already running their
+    shape's jobs (continuous batching), and the rest start the smallest idle empty batch that holds
+    them all (else the largest idle one).  Finished jobs leave their slot at once; every batch of
+    every shape runs concurrently.  A shape's batches are built when first needed unless the shape
+    is listed in `prewarm` (default: every shape), so a cold shape pays its set-up inside the stream.
+    The batches' footprint must fit the budget.  Returns (completions sorted by request id, summary)."""
     import torch
     from .batch import BatchedSolver
     from .problems import cantilever_equal_split, simp_modulus
@@ -334,87 +347,105 @@ def serve_batched(requests, shapes=None, slots=None, precision="mixed", chunk=4,
     slots = {s: (slots or {}).get(s, default_slots(s)) for s in shapes}
     prewarm = set(shapes) if prewarm is None else {tuple(s) for s in prewarm}
     forces = {s: cantilever_equal_split(s)[1] for s in shapes}
-    solvers, used = {}, 0.0
+    ladders = {s: batch_ladder(slots[s]) for s in shapes}
+    batches = {s: [None] * len(ladders[s]) for s in shapes}     # built lazily
+    used = 0.0
 
-    def build(shape):
+    def build(s, i):
         nonlocal used
-        bs = BatchedSolver(shape, slots[shape], precision=precision, chunk=chunk, maxiter=maxiter)
+        bs = BatchedSolver(s, ladders[s][i], precision=precision, chunk=chunk, maxiter=maxiter)
         used += bs.footprint_bytes()
         if used > budget_bytes:
             raise ValueError(f"batches need {used / 1e9:.1f} GB, over the {budget_bytes / 1e9:.0f} GB budget")
         # one throw-away job captures the chunk graph before any request is timed on it
-        E1 = torch.ones(shape[0] * shape[1] * shape[2], dtype=torch.float64, device="cuda")
-        bs.solve([(E1, forces[shape], 1e-2)])
+        E1 = torch.ones(s[0] * s[1] * s[2], dtype=torch.float64, device="cuda")
+        bs.solve([(E1, forces[s], 1e-2)])
         bs.retire(0)
-        solvers[shape] = bs
+        bs.active, bs.inflight = {}, False          # slot -> (request, admitted time)
+        batches[s][i] = bs
         return bs
 
     for s in shapes:
         if s in prewarm:
-            build(s)
+            for i in range(len(ladders[s])):
+                build(s, i)
     torch.cuda.synchronize()
-    pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
-    active = {s: {} for s in shapes}             # shape -> slot -> (request, admitted time)
-    inflight = {s: False for s in shapes}
+    pending = {s: deque() for s in shapes}
+    arrivals = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
     done = []
     peak = 0
+    cold = [s for s in shapes if s not in prewarm]
     t0 = clock()
-    while pending or any(active.values()):
+
+    def live():
+        return [b for s in shapes for b in batches[s] if b is not None]
+
+    def admit(bs, s, rs):
+        free = [k for k in range(bs.B) if k not in bs.active]
+        jobs = []
+        for k, r in zip(free, rs):
+            rho = r.density if isinstance(r.density, torch.Tensor) else torch.as_tensor(r.density)
+            E = simp_modulus(rho.to("cuda", torch.float64), 1e-9)
+            jobs.append((k, E, forces[s], r.tol))
+            bs.active[k] = (r, clock() - t0)
+        bs.admit(jobs)
+
+    while arrivals or any(pending.values()) or any(b.active for b in live()):
         now = clock() - t0
         progressed = False
-        # admission: arrived requests into free slots of their shape (FIFO per shape)
-        joins = {}
-        still = deque()
-        while pending and pending[0].arrival <= now:
-            r = pending.popleft()
-            s = tuple(r.shape)
-            free = slots[s] - len(active[s]) - len(joins.get(s, []))
-            if free > 0 and not inflight[s]:
-                joins.setdefault(s, []).append(r)
-            else:
-                still.append(r)
-        pending.extendleft(reversed(still))
-        for s, rs in joins.items():
-            bs = solvers.get(s) or build(s)
-            free_slots = [k for k in range(slots[s]) if k not in active[s]]
-            jobs = []
-            for k, r in zip(free_slots, rs):
-                rho = r.density if isinstance(r.density, torch.Tensor) else torch.as_tensor(r.density)
-                E = simp_modulus(rho.to("cuda", torch.float64), 1e-9)
-                jobs.append((k, E, forces[s], r.tol))
-                active[s][k] = (r, clock() - t0)
-            bs.admit(jobs)
-            progressed = True
-        peak = max(peak, sum(len(a) for a in active.values()))
-        # launch a chunk for every shape with jobs and nothing in flight
+        while arrivals and arrivals[0].arrival <= now:
+            r = arrivals.popleft()
+            pending[tuple(r.shape)].append(r)
+        # admission between chunks
         for s in shapes:
-            if active[s] and not inflight[s]:
-                solvers[s].run()
-                inflight[s] = True
+            q = pending[s]
+            if not q:
+                continue
+            for bs in batches[s]:                   # running batches with free slots first
+                if q and bs is not None and bs.active and not bs.inflight and len(bs.active) < bs.B:
+                    take = [q.popleft() for _ in range(min(len(q), bs.B - len(bs.active)))]
+                    admit(bs, s, take)
+                    progressed = True
+            while q:
+                idle = [i for i, b in enumerate(batches[s]) if b is None or (not b.active and not b.inflight)]
+                if not idle:
+                    break
+                fit = [i for i in idle if ladders[s][i] >= len(q)]
+                i = fit[0] if fit else idle[-1]
+                bs = batches[s][i] or build(s, i)
+                take = [q.popleft() for _ in range(min(len(q), bs.B))]
+                admit(bs, s, take)
+                progressed = True
+        peak = max(peak, sum(len(b.active) for b in live()))
+        # launch a chunk on every batch with jobs and nothing in flight
+        for bs in live():
+            if bs.active and not bs.inflight:
+                bs.run()
+                bs.inflight = True
                 progressed = True
         # completion
         for s in shapes:
-            if inflight[s] and solvers[s].ready():
-                inflight[s] = False
-                bs = solvers[s]
+            for bs in batches[s]:
+                if bs is None or not bs.inflight or not bs.ready():
+                    continue
+                bs.inflight = False
                 fin, *_ = bs.poll()
-                for k in list(active[s]):
-                    if fin[k]:
-                        r, adm = active[s].pop(k)
-                        x, it, ok, rel, comp = bs.result(k)
-                        bs.retire(k)
-                        done.append(Completion(r.rid, s, r.tol, r.arrival, adm, clock() - t0, it, ok, rel, comp,
-                                               x if keep_solution else None))
+                ks = [k for k in list(bs.active) if fin[k]]
+                for k, (x, it, ok, rel, comp) in zip(ks, bs.results(ks)):
+                    r, adm = bs.active.pop(k)
+                    bs.retire(k)
+                    done.append(Completion(r.rid, s, r.tol, r.arrival, adm, clock() - t0, it, ok, rel, comp,
+                                           x if keep_solution else None))
                 progressed = True
         if not progressed:
-            if not any(active.values()) and pending:
-                wait = pending[0].arrival - (clock() - t0)
+            if not any(b.active for b in live()) and not any(pending.values()) and arrivals:
+                wait = arrivals[0].arrival - (clock() - t0)
                 if wait > 0:
                     time.sleep(min(wait, 0.01))
             else:
                 time.sleep(poll_s)
     makespan = clock() - t0
     out = summarize(done, makespan)
-    out.update(peak_inflight=peak, slots={"x".join(map(str, s)): slots[s] for s in shapes},
-               batches_gb=used / 1e9, cold_shapes=["x".join(map(str, s)) for s in shapes if s not in prewarm])
+    out.update(peak_inflight=peak, slots={"x".join(map(str, s)): ladders[s] for s in shapes},
+               batches_gb=used / 1e9, cold_shapes=["x".join(map(str, s)) for s in cold])
     return sorted(done, key=lambda c: c.rid), out

@@ -182,14 +182,7 @@ class MGHierarchy:
         L0 = self.levels[0]
         if E.data_ptr() != L0.E64.data_ptr():
             L0.E64.copy_(E)
-        for i, L in enumerate(self.levels):
-            if i:
-                prev = self.levels[i - 1]
-                _lib.call("vx_coarsen_modulus", _lib.VX_F64, *prev.shape, prev.E64.data_ptr(), L.E64.data_ptr(), _s())
-            if L.E.data_ptr() != L.E64.data_ptr():
-                L.E.copy_(L.E64)
-            inv64 = L.op64.diagonal(L.E64, L.mask, inverse=True)
-            L.invd.copy_(inv64)
+        self.refresh_levels()
         c = self.levels[-1]
         if self.blocks:
             for k in range(self.blocks):
@@ -200,6 +193,18 @@ class MGHierarchy:
         # no error check here (it would synchronise the stream); a non-SPD coarse matrix shows up as a
         # non-finite residual and a non-converged solve
         self._coarse_inverse()
+
+    def refresh_levels(self):
+        """Every level's moduli (coarsened from the finest), their narrow copies and the inverse
+        diagonals, one launch each per level (in place)."""
+        for i, L in enumerate(self.levels):
+            if i:
+                prev = self.levels[i - 1]
+                _lib.call("vx_coarsen_modulus", _lib.VX_F64, *prev.shape, prev.E64.data_ptr(), L.E64.data_ptr(), _s())
+            if L.E.data_ptr() != L.E64.data_ptr():
+                L.E.copy_(L.E64)
+            inv64 = L.op64.diagonal(L.E64, L.mask, inverse=True)
+            L.invd.copy_(inv64)
 
     def _assemble_block(self, k):
         """Coarsest dense matrix of stacked job k (from its own segment of the coarsest moduli and mask)."""
@@ -213,8 +218,26 @@ class MGHierarchy:
 
     def refresh_block(self, k):
         """Re-assemble and re-factor stacked job k's coarsest system (after its moduli changed)."""
-        self._assemble_block(k)
-        self._factor_block(k)
+        self.refresh_blocks([k])
+
+    def refresh_blocks(self, ks, assemble=True):
+        """Re-assemble (optionally) and re-factor the coarsest systems of stacked jobs ks, the
+        factorisations side by side in the same launches (vx_batch_coarse_factor)."""
+        ks = [int(k) for k in ks]
+        if not ks:
+            return
+        if assemble:
+            for k in ks:
+                self._assemble_block(k)
+        n = self.A_coarse.shape[1]
+        nx, ny, nz = self.job_coarse
+        bw = min(n - 1, 3 * ((ny + 1) * (nz + 1) + (nz + 1) + 1) + 2)
+        ws = int(_lib.load().vx_coarse_factor_workspace(n, bw))
+        if getattr(self, "_factor_work", None) is None or self._factor_work.numel() < ws * min(len(ks), 64):
+            self._factor_work = torch.empty(ws * min(self.blocks, 64), dtype=torch.float64, device="cuda")
+        slots = (ctypes.c_int * len(ks))(*ks)
+        _lib.call("vx_batch_coarse_factor", n, bw, len(ks), slots, self.A_coarse.data_ptr(),
+                  self.coarse_packed.data_ptr(), self._factor_work.data_ptr(), self._factor_info.data_ptr(), _s())
 
     def _coarse_inverse(self):
         """Factor the coarsest matrix A = L L^T (FP64 Cholesky) and pack L^-1 with its transpose for
@@ -225,8 +248,7 @@ class MGHierarchy:
         stream without a host synchronisation.  Returns the factorisation's device-side info tensor
         (0 when A is positive definite)."""
         if self.blocks:
-            for k in range(self.blocks):
-                self._factor_block(k)
+            self.refresh_blocks(range(self.blocks), assemble=False)
             return self._factor_info
         n = self.A_coarse.shape[0]
         nx, ny, nz = self.levels[-1].shape
@@ -246,16 +268,6 @@ class MGHierarchy:
         linv = _lower_inverse(factor).contiguous()                  # the kernel reads it row-major
         _lib.call("vx_coarse_pack", linv.shape[0], linv.data_ptr(), self.coarse_packed.data_ptr(), _s())
         return info
-
-    def _factor_block(self, k):
-        n = self.A_coarse.shape[1]
-        nx, ny, nz = self.job_coarse
-        bw = min(n - 1, 3 * ((ny + 1) * (nz + 1) + (nz + 1) + 1) + 2)
-        if getattr(self, "_factor_work", None) is None:
-            self._factor_work = torch.empty(int(_lib.load().vx_coarse_factor_workspace(n, bw)), dtype=torch.float64,
-                                            device="cuda")
-        _lib.call("vx_coarse_factor", n, bw, self.A_coarse[k].data_ptr(), self.coarse_packed[k].data_ptr(),
-                  self._factor_work.data_ptr(), self._factor_info[k:k + 1].data_ptr(), _s())
 
     def footprint_bytes(self) -> int:
         b = 0

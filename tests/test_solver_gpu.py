@@ -378,3 +378,41 @@ def test_banded_coarse_factor_flags_a_matrix_that_is_not_positive_definite():
                  torch.cuda.current_stream().cuda_stream)
     assert int(info) == 98                                  # 1-based column of the first bad pivot
     assert torch.isfinite(packed).all()
+
+
+def test_batched_coarse_factor_equals_one_at_a_time():
+    """vx_batch_coarse_factor on a subset of matrix slots gives each slot exactly what
+    vx_coarse_factor gives alone, and leaves the other slots untouched."""
+    import ctypes
+    n, bw, B = 700, 90, 5
+    rng = np.random.default_rng(11)
+    mats = []
+    for _ in range(B):
+        Bm = np.zeros((n, n))
+        for k in range(bw + 1):
+            Bm += np.diag(rng.standard_normal(n - k), -k)
+        A = np.triu(np.tril(Bm @ Bm.T, bw), -bw)
+        A += np.eye(n) * (np.abs(A).sum(1).max() + 1)
+        mats.append(A)
+    A = cu(np.stack(mats))
+    lib = vx._lib.load()
+    ws = int(lib.vx_coarse_factor_workspace(n, bw))
+    s = torch.cuda.current_stream().cuda_stream
+    one = torch.full_like(A, float("nan"))
+    info1 = torch.zeros(B, dtype=torch.int32, device="cuda")
+    work1 = torch.empty(ws, dtype=torch.float64, device="cuda")
+    for k in range(B):
+        vx._lib.call("vx_coarse_factor", n, bw, A[k].data_ptr(), one[k].data_ptr(), work1.data_ptr(),
+                     info1[k:k + 1].data_ptr(), s)
+    ks = [4, 1, 3]
+    many = torch.full_like(A, 7.0)
+    info = torch.full((B,), -1, dtype=torch.int32, device="cuda")
+    work = torch.empty(ws * len(ks), dtype=torch.float64, device="cuda")
+    slots = (ctypes.c_int * len(ks))(*ks)
+    vx._lib.call("vx_batch_coarse_factor", n, bw, len(ks), slots, A.data_ptr(), many.data_ptr(), work.data_ptr(),
+                 info.data_ptr(), s)
+    for k in range(B):
+        if k in ks:
+            assert torch.equal(many[k], one[k]) and int(info[k]) == 0
+        else:
+            assert bool((many[k] == 7.0).all()) and int(info[k]) == -1
