@@ -810,24 +810,26 @@ def serving_section(n=256, repeats=1, clocks_index=0, per_stream_slots=16):
         out["batched"] = runs[0] if repeats == 1 else {"runs": runs, "p99_ms": [r["p99_ms"] for r in runs],
                                                        "p50_ms": [r["p50_ms"] for r in runs]}
         slots = per_stream_slots
-        backend = serving.CudaBackend(precision="mixed")
-        backend.prewarm(shapes, slots, 150e9)
-        warm = serving.request_stream(n=8, shapes=shapes, rate=1e6, seed=99)
-        for r in warm:
-            r.arrival = 0.0
-        sched = serving.Scheduler(serving._PoolCharge(backend), budget_bytes=150e9, max_slots=slots)
-        sched.run(warm)
+        warm_shapes = [s_ for s_ in shapes if s_ != cold]
         pruns = []
-        for rep in range(repeats):
+        for rep in range(repeats):                 # a fresh pool per run: the cold shape is cold every time
+            backend = serving.CudaBackend(precision="mixed")
+            backend.prewarm(warm_shapes, slots, 150e9)
+            warm = serving.request_stream(n=8, shapes=warm_shapes, rate=1e6, seed=99)
+            for r in warm:
+                r.arrival = 0.0
+            sched = serving.Scheduler(serving._PoolCharge(backend), budget_bytes=150e9, max_slots=slots)
+            sched.run(warm)
             sched.peak_inflight = 0
             done, makespan = sched.run(reqs)
             ps = serving.summarize(done, makespan)
-            ps.update(peak_inflight=sched.peak_inflight, prewarmed_solvers_per_shape=slots)
+            ps.update(peak_inflight=sched.peak_inflight, prewarmed_solvers_per_shape=slots,
+                      cold_shapes=["x".join(map(str, cold))])
             pruns.append(ps)
+            del backend, sched
+            torch.cuda.empty_cache()
         out["per_stream"] = pruns[0] if repeats == 1 else {"runs": pruns, "p99_ms": [r["p99_ms"] for r in pruns],
                                                             "p50_ms": [r["p50_ms"] for r in pruns]}
-        del backend, sched
-        torch.cuda.empty_cache()
         serial_done, serial_summary = serving.serve(reqs, precision="fp64", max_slots=1, prewarm=True)
         out["serial_fp64"] = serial_summary
         torch.cuda.empty_cache()
