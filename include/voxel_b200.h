@@ -329,9 +329,10 @@ int vx_batch_graph_while_end(void* handle, const double* S, int slots, cudaStrea
  * allocate device memory (a request loop that must never call cudaMalloc mid-flight, a plugin
  * inside another framework's memory arena, a process under a hard memory cap).  The partial sums
  * live in a fixed array compiled into the library: 16384 doubles (128 KiB) on every device that
- * loads it, kept until the process exits.  The streaming kernel keeps one partial per persistent CTA
- * (vx_operator_partials(prec, ...), at most one per SM), so every grid the library accepts fits;
- * a launch that would need more than 16384 partials is rejected with VX_ERR_INVALID_ARGUMENT.  The
+ * loads it, kept until the process exits.  The streaming kernels keep one partial per CTA
+ * (vx_operator_partials(prec, ...)) and chunk x only while the CTAs stay within 16384, so every grid
+ * fits whose y-z tiling does (all but extremely flat ones); a launch that would need more than 16384
+ * partials is rejected with VX_ERR_INVALID_ARGUMENT.  The
  * first call on each device looks up the array's device address (cudaGetSymbolAddress) and keeps
  * it for the process: make that first call before any stream capture, and do not use the entry
  * point across a reset of the device's primary context (cudaDeviceReset), which would leave the

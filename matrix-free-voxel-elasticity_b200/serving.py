@@ -310,6 +310,16 @@ def request_stream(n=256, shapes=((48, 24, 24), (96, 48, 48), (160, 80, 80), (25
     return reqs
 
 
+def reserve_device_memory(nbytes):
+    """Grow the caching allocator by `nbytes` (one block allocated and freed), so that solvers and
+    batches built while a stream is being served take their memory from the cache: a cudaMalloc
+    there would synchronise the device and stall every job in flight."""
+    import torch
+    if nbytes and nbytes > 0:
+        t = torch.empty(int(nbytes), dtype=torch.uint8, device="cuda")
+        del t
+
+
 # ------------------------------------------------------------------------------ batched serving
 def default_slots(shape, max_slots=16, dofs_per_batch=32e6):
     """Slots of a shape's batch: as many jobs as fit about `dofs_per_batch` stacked DOFs, at most max_slots."""
@@ -329,7 +339,7 @@ def batch_ladder(max_slots):
 
 
 def serve_batched(requests, shapes=None, slots=None, precision="mixed", chunk=4, maxiter=200, budget_bytes=150e9,
-                  prewarm=None, keep_solution=False, clock=time.perf_counter, poll_s=50e-6):
+                  prewarm=None, keep_solution=False, clock=time.perf_counter, poll_s=50e-6, reserve_bytes=0):
     """Continuous batching with fused launches.  Each grid shape has a ladder of batch.BatchedSolvers
     of capacities 1, 2, 4, ... up to slots[shape] (batch_ladder), each with its own stream and
     captured chunk graph; every kernel of a chunk serves all the jobs of its batch at once.  A batch
@@ -338,8 +348,9 @@ def serve_batched(requests, shapes=None, slots=None, precision="mixed", chunk=4,
     shape's jobs (continuous batching), and the rest start the smallest idle empty batch that holds
     them all (else the largest idle one).  Finished jobs leave their slot at once; every batch of
     every shape runs concurrently.  A shape's batches are built when first needed unless the shape
-    is listed in `prewarm` (default: every shape), so a cold shape pays its set-up inside the stream.
-    The batches' footprint must fit the budget.  Returns (completions sorted by request id, summary)."""
+    is listed in `prewarm` (default: every shape), so a cold shape pays its set-up inside the stream
+    (`reserve_bytes` of cached memory make that set-up allocation-free).  The batches' footprint must
+    fit the budget.  Returns (completions sorted by request id, summary)."""
     import torch
     from .batch import BatchedSolver
     from .problems import cantilever_equal_split, simp_modulus
@@ -369,6 +380,7 @@ def serve_batched(requests, shapes=None, slots=None, precision="mixed", chunk=4,
         if s in prewarm:
             for i in range(len(ladders[s])):
                 build(s, i)
+    reserve_device_memory(reserve_bytes)            # for the cold shapes' batches
     torch.cuda.synchronize()
     pending = {s: deque() for s in shapes}
     arrivals = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
