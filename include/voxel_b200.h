@@ -302,6 +302,11 @@ int vx_coarse_factor(int n, int bw, const double* A, double* packed, double* wor
  * No counterpart in the reference. */
 int vx_batch_coarse_factor(int n, int bw, int count, const int* slots, const double* A, double* packed,
                            double* work, int* info, cudaStream_t stream);
+/* The packed inverse factor tril(L^-1) + triu(L^-T, 1) from a Cholesky factor L the caller already
+ * has (dense row-major n x n, lower triangle read, half-bandwidth bw): what the reference's
+ * Multigrid(..., coarse_factor, ...) receives (src/voxel_mg.py:120-160).  work: as vx_coarse_factor.
+ * No factorisation: the diagonal blocks are inverted side by side, then the blocked band inverse. */
+int vx_coarse_pack_factor(int n, int bw, const double* L, double* packed, double* work, cudaStream_t stream);
 
 /* ---------------------------------------------------------------------------- batches
  * `slots` independent systems of one size solved in lockstep (the serving loop's batches): slot k's

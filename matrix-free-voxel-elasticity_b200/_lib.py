@@ -60,6 +60,7 @@ SIGNATURES = {
     "vx_coarse_factor_workspace": (c_int64, [c_int, c_int]),
     "vx_coarse_factor": (c_int, [c_int, c_int, _P, _P, _P, _P, _P]),
     "vx_batch_coarse_factor": (c_int, [c_int, c_int, c_int, POINTER(c_int), _P, _P, _P, _P, _P]),
+    "vx_coarse_pack_factor": (c_int, [c_int, c_int, _P, _P, _P, _P]),
     # batches of independent systems
     "vx_batch_finalize": (c_int, [c_int, c_int64, c_int, _P, c_int64, _P, _P]),
     "vx_batch_cg_update": (c_int, [c_int, c_int64, c_int, c_int64, _P, _P, _P, _P, _P, c_int, _P]),
@@ -143,7 +144,7 @@ CAPTURE_STREAM = None
 
 # Kernel launches issued by each entry point (entry points not listed launch none or one:
 # host-only entry points are in HOST_ONLY).  Used to count this library's launches.
-KERNELS_PER_CALL = {"vx_tc_element_product": 1, "vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2, "vx_coarse_apply_factor": 2,
+KERNELS_PER_CALL = {"vx_tc_element_product": 1, "vx_coarse_pack_factor": 3, "vx_dots": 2, "vx_assemble_dense": 1, "vx_true_residual_noalloc": 2, "vx_coarse_apply_factor": 2,
                     "vx_batch_coarse_apply_factor": 2}
 HOST_ONLY = {"vx_last_error", "vx_version", "vx_element_matrix", "vx_element", "vx_parity_blocks",
              "vx_operator_partials", "vx_partials_size", "vx_solver_slots", "vx_solver_partials",

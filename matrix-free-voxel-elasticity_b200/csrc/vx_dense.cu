@@ -94,9 +94,13 @@ __global__ void band_load_kernel(int n, int bw, const __grid_constant__ FactorBa
 // predicated register selects spilled).
 __device__ __forceinline__ void potrf_bar() { asm volatile("bar.sync 1, %0;" ::"n"(CB) : "memory"); }
 
+// FACTOR = false: the band already holds a Cholesky factor; only the diagonal block's inverse is
+// formed (block k0 = blockIdx.x CB, every block in one launch; no panel copy, nothing written back).
+template <bool FACTOR>
 __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int k0, const __grid_constant__ FactorBatch fb) {
     static_assert(CB == 64 && POTRF_T >= CB, "two factoring warps");
     vx::pdl_begin();
+    if constexpr (!FACTOR) k0 = blockIdx.x * CB;
     const FactorPtrs P = fptrs(fb, n, bw);
     double* __restrict__ lb = P.lb;
     double* __restrict__ dinv = P.dinv_all + int64_t(k0 / CB) * CB * CB;
@@ -109,10 +113,12 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
     const int w = min(CB, n - k0);
     const int base = k0 + w, rend = min(n, k0 + w + bw);
     const int t = threadIdx.x;
-    #pragma unroll 8
-    for (int i = t; i < (rend - base) * CB; i += POTRF_T) {
-        const int r = base + i / CB, c = i % CB, col = k0 + c;
-        apanel[i] = (c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
+    if constexpr (FACTOR) {
+        #pragma unroll 8
+        for (int i = t; i < (rend - base) * CB; i += POTRF_T) {
+            const int r = base + i / CB, c = i % CB, col = k0 + c;
+            apanel[i] = (c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
+        }
     }
     #pragma unroll
     for (int i = t; i < CB * CB; i += POTRF_T) {
@@ -123,7 +129,8 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
         D[r][c] = v;
     }
     __syncthreads();
-    if (t < CB) {
+    if (!FACTOR && t < CB) rinv[t] = 1.0 / D[t][t];
+    if (FACTOR && t < CB) {
         double a[CB];
         #pragma unroll
         for (int c = 0; c < CB; ++c) a[c] = D[t][c];
@@ -176,7 +183,7 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
     #pragma unroll
     for (int i = t; i < CB * CB; i += POTRF_T) {
         const int r = i / CB, c = i % CB;
-        if (r < w && c <= r && r - c <= bw) lb[bidx(k0 + r, k0 + c, bw)] = D[r][c];
+        if (FACTOR && r < w && c <= r && r - c <= bw) lb[bidx(k0 + r, k0 + c, bw)] = D[r][c];
         dinv[i] = (r < w && c < w) ? X[r][c] : 0.0;
     }
 }
@@ -521,7 +528,7 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
     const size_t usm = size_t(3) * CB * CBP * sizeof(double);
     const size_t ism = size_t(INV_STAGES + nw) * (bw + 1) * sizeof(double);
     static std::atomic<uint64_t> opt_p, opt_u, opt_i, opt_b;
-    int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel, psm, what);
+    int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel<true>, psm, what);
     if (!st) st = smem_opt_in(opt_u, (const void*)band_update_kernel, usm, what);
     if (!st) st = smem_opt_in(opt_i, (const void*)band_inverse_kernel, 227 * 1024, what);
     if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, what);
@@ -530,7 +537,7 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
     const int64_t band = int64_t(n) * (bw + 1);
     vx::launch(band_load_kernel, dim3(unsigned((band + 255) / 256), B), 256, 0, stream, n, bw, fb);
     for (int k0 = 0; k0 < n; k0 += CB) {
-        vx::launch(band_potrf_kernel, dim3(1, B), POTRF_T, psm, stream, n, bw, k0, fb);
+        vx::launch(band_potrf_kernel<true>, dim3(1, B), POTRF_T, psm, stream, n, bw, k0, fb);
         const int w = std::min(CB, n - k0);
         const int rows = std::min(n, k0 + w + bw) - (k0 + w);
         if (rows <= 0) continue;
@@ -567,5 +574,48 @@ extern "C" int vx_batch_coarse_factor(int n, int bw, int count, const int* slots
                                            packed, work, info, stream);
         if (st) return st;
     }
+    return VX_OK;
+}
+
+// The packed inverse factor from a Cholesky factor the caller already has (dense row-major lower
+// triangle, half-bandwidth bw): the band is loaded from L, every diagonal block inverted in one
+// launch, then the blocked band inverse.  work: vx_coarse_factor_workspace(n, bw) doubles.
+extern "C" int vx_coarse_pack_factor(int n, int bw, const double* L, double* packed, double* work,
+                                     cudaStream_t stream) {
+    const char* what = "vx_coarse_pack_factor";
+    VX_CHECK_ARG(n > 0 && bw >= 0, VX_ERR_INVALID_ARGUMENT, "%s: bad size n=%d bw=%d", what, n, bw);
+    VX_CHECK_ARG(L && packed && work, VX_ERR_NULL_POINTER, "%s: NULL pointer", what);
+    VX_CHECK_ARG(L != packed, VX_ERR_INVALID_ARGUMENT, "%s: packed may not alias L", what);
+    bw = std::min(bw, n - 1);
+    const int nw = inverse_warps(bw);
+    VX_CHECK_ARG(nw > 0, VX_ERR_INVALID_ARGUMENT, "%s: bandwidth %d is too wide", what, bw);
+    FactorBatch fb{};
+    fb.A = L;
+    fb.packed = packed;
+    fb.work = work;
+    fb.info = nullptr;
+    fb.mat = int64_t(n) * n;
+    fb.ws = vx_coarse_factor_workspace(n, bw);
+    fb.nblk = (n + CB - 1) / CB;
+    fb.slot[0] = 0;
+    const size_t psm = size_t(2) * CB * CBP * sizeof(double);
+    const size_t ism = size_t(INV_STAGES + nw) * (bw + 1) * sizeof(double);
+    static std::atomic<uint64_t> opt_p, opt_i, opt_b;
+    int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel<false>, psm, what);
+    if (!st) st = smem_opt_in(opt_i, (const void*)band_inverse_kernel, 227 * 1024, what);
+    if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, what);
+    if (st) return st;
+    const int64_t band = int64_t(n) * (bw + 1);
+    vx::launch(band_load_kernel, dim3(unsigned((band + 255) / 256), 1), 256, 0, stream, n, bw, fb);
+    vx::launch(band_potrf_kernel<false>, dim3(unsigned(fb.nblk), 1), POTRF_T, psm, stream, n, bw, 0, fb);
+    const InvbLayout il(bw);
+    if (il.bytes <= 227 * 1024) {
+        vx::launch(band_inverse_blocked_kernel, dim3(unsigned((n + ITC - 1) / ITC), 1), INVB_T, il.bytes, stream, n,
+                   bw, fb);
+    } else {
+        vx::launch(band_inverse_kernel, dim3(unsigned((n + nw - 1) / nw), 1), unsigned(nw * 32), ism, stream, n, bw,
+                   fb);
+    }
+    VX_CHECK_LAUNCH(what);
     return VX_OK;
 }

@@ -32,7 +32,7 @@ from . import _lib
 from .element import quadrature
 from .operators import PREC, STORAGE, VoxelOperator, node_mask_from_dofs, stream_ptr
 from .solver import (FIN_BETA_PR, FIN_NB, FIN_PQ, FIN_RZ, FIN_TRUE, S_BREAK, S_CHECK, S_DONE, S_IT, S_MAXIT,
-                     S_MV, S_REL, S_TOL, SolveResult, _GraphLoop, _lower_inverse, hierarchy_shapes)
+                     S_MV, S_REL, S_TOL, SolveResult, _GraphLoop, hierarchy_shapes)
 
 PLANE_APPLY, PLANE_JACOBI, PLANE_RESIDUAL, PLANE_TRUE_RES = range(4)
 _ARITH = {torch.float64: torch.float64, torch.float32: torch.float32, torch.bfloat16: torch.float32}
@@ -352,13 +352,16 @@ class SlabHierarchy:
         kc = np.ascontiguousarray(self.ke * 2 ** l)
         A = torch.empty(self.nc, self.nc, dtype=torch.float64, device="cuda")
         _lib.call("vx_assemble_dense", *cs, _lib.dptr(kc), Eg.data_ptr(), mg.data_ptr(), A.data_ptr(), _s())
-        L, info = torch.linalg.cholesky_ex(A)
-        if int(info) != 0:
-            raise ValueError(f"coarsest-level matrix is not positive definite (cholesky info {int(info)})")
-        linv = _lower_inverse(L).contiguous()
+        # banded Cholesky and the packed inverse factor in the library's own kernels (as MGHierarchy)
+        bw = min(self.nc - 1, 3 * ((cs[1] + 1) * (cs[2] + 1) + (cs[2] + 1) + 1) + 2)
+        work = torch.empty(int(_lib.load().vx_coarse_factor_workspace(self.nc, bw)), dtype=torch.float64, device="cuda")
+        info = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.coarse_packed = torch.empty_like(A)
-        _lib.call("vx_coarse_pack", self.nc, linv.data_ptr(), self.coarse_packed.data_ptr(), _s())
-        del A, L, linv
+        _lib.call("vx_coarse_factor", self.nc, bw, A.data_ptr(), self.coarse_packed.data_ptr(), work.data_ptr(),
+                  info.data_ptr(), _s())
+        if int(info) != 0:
+            raise ValueError(f"coarsest-level matrix is not positive definite (pivot {int(info)})")
+        del A, work
         self._rc = torch.zeros(self.nc, dtype=self.aux_dtype, device="cuda")
         self._zc = torch.zeros(self.nc, dtype=self.dtype, device="cuda")
         self._yc = torch.zeros(self.nc, dtype=torch.float64, device="cuda")

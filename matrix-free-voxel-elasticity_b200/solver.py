@@ -281,20 +281,21 @@ class MGHierarchy:
     def spectral_omegas(self, iterations=30, seed=20260923):
         """omega_l = 4 / (3 lambda_l), lambda_l from a seeded FP64 power iteration on D^-1 A over the
         free DOFs (src/voxel_mg.py:228-244).  Returns (omegas, lambdas)."""
-        omegas, lambdas = [], []
+        omegas, lams = [], []
         for L in self.levels[:-1]:
             rng = np.random.default_rng(seed)
             m = ((L.mask.to(torch.int32)[:, None] >> torch.arange(3, device="cuda")) & 1).reshape(-1).double()
             v = torch.as_tensor(rng.standard_normal(L.n), device="cuda") * m
             v = v / torch.linalg.vector_norm(v)
             inv64 = L.op64.diagonal(L.E64, L.mask, inverse=True)
-            lam = 0.0
-            for _ in range(iterations):
+            lam = None
+            for _ in range(iterations):                 # the norms stay on the device: no host round trip
                 w = inv64 * L.op64.matvec(v, L.E64, L.mask) * m
-                lam = float(torch.linalg.vector_norm(w))
+                lam = torch.linalg.vector_norm(w)
                 v = w / lam
-            lambdas.append(lam)
-            omegas.append(4.0 / (3.0 * lam))
+            lams.append(lam)
+        lambdas = [float(x) for x in lams]              # one synchronisation for all levels
+        omegas = [4.0 / (3.0 * x) for x in lambdas]
         return omegas, lambdas
 
     # ------------------------------------------------------------------ kernel emission

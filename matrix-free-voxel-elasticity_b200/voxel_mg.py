@@ -156,12 +156,16 @@ class Multigrid:
         n_smooth = len(self.levels) - 1
         self.omegas = list(omegas) if omegas is not None else [0.6] * n_smooth
         assert len(self.omegas) == n_smooth
-        # the coarse solve: L^-1 of the FP64 factor packed with its transpose (two triangular passes)
-        f64 = _t(coarse_factor, torch.float64)
+        # the coarse solve: L^-1 of the FP64 factor packed with its transpose (two triangular passes),
+        # formed by the library from the caller's banded factor
+        f64 = _t(coarse_factor, torch.float64).contiguous()
         n = f64.shape[0]
-        linv = _lower_inverse(f64).contiguous()
-        self._packed = torch.empty_like(linv)
-        _lib.call("vx_coarse_pack", n, linv.data_ptr(), self._packed.data_ptr(), stream_ptr())
+        cs = [int(v) for v in shapes[-1]]
+        bw = min(n - 1, 3 * ((cs[1] + 1) * (cs[2] + 1) + (cs[2] + 1) + 1) + 2)
+        self._packed = torch.empty_like(f64)
+        work = torch.empty(int(_lib.load().vx_coarse_factor_workspace(n, bw)), dtype=torch.float64, device="cuda")
+        _lib.call("vx_coarse_pack_factor", n, bw, f64.data_ptr(), self._packed.data_ptr(), work.data_ptr(),
+                  stream_ptr())
         self._coarse_y = torch.empty(n, dtype=torch.float64, device="cuda")
         # what the device route needs: FP64 finest modulus, products of one element matrix ke * 2^l
         self._shapes = [tuple(int(v) for v in sh) for sh in shapes]

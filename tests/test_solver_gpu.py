@@ -416,3 +416,26 @@ def test_batched_coarse_factor_equals_one_at_a_time():
             assert torch.equal(many[k], one[k]) and int(info[k]) == 0
         else:
             assert bool((many[k] == 7.0).all()) and int(info[k]) == -1
+
+
+@pytest.mark.parametrize("n,bw", [(70, 9), (1000, 130), (4131, 275)])
+def test_packed_inverse_from_a_given_factor(n, bw):
+    """vx_coarse_pack_factor turns a Cholesky factor the caller computed (the reference Multigrid's
+    coarse_factor argument) into the packed tril(L^-1) + triu(L^-T, 1), to FP64 rounding."""
+    rng = np.random.default_rng(n)
+    B = np.zeros((n, n))
+    for k in range(bw + 1):
+        B += np.diag(rng.standard_normal(n - k), -k)
+    A = np.triu(np.tril(B @ B.T, bw), -bw)
+    A += np.eye(n) * (np.abs(A).sum(1).max() + 1)
+    L = np.linalg.cholesky(A)
+    X = np.linalg.inv(L)
+    ref = np.tril(X) + np.triu(X.T, 1)
+    Ld = cu(L)
+    packed = torch.full_like(Ld, float("nan"))
+    work = torch.empty(int(vx._lib.load().vx_coarse_factor_workspace(n, bw)), dtype=torch.float64, device="cuda")
+    vx._lib.call("vx_coarse_pack_factor", n, bw, Ld.data_ptr(), packed.data_ptr(), work.data_ptr(),
+                 torch.cuda.current_stream().cuda_stream)
+    P = packed.cpu().numpy()
+    assert np.isfinite(P).all()
+    assert np.max(np.abs(P - ref)) <= 1e-12 * np.max(np.abs(ref))
