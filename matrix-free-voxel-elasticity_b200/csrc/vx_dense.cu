@@ -85,13 +85,19 @@ __global__ void band_load_kernel(int n, int bw, const __grid_constant__ FactorBa
 // (the A values band_update turns into the panel) to apanel ((bw + 1) x CB), so that band_update
 // can store finished panel rows in place while other tiles still read the originals.
 // The block's CB pivots are a chain of dependent steps, so it is factored by CB threads with the
-// rows in registers (right-looking; thread i holds row i; per pivot: the pivot thread's square root
-// and reciprocal, a named barrier of the two warps, the column through shared memory, a rank-1
-// update of the row in registers); a block smaller than CB (the last) is padded with the identity.
-// The inverse then needs no barrier: thread c runs the forward substitution of column c of X =
-// L^-1 in registers, reading the rows of L from shared memory.  Every loop is unrolled, so the
-// row and column registers are addressed at compile time (a variant with the pivot loop rolled and
-// predicated register selects spilled).
+// rows in registers (right-looking; thread i holds row i; per pivot: the pivot thread's reciprocal
+// square root (the pivot is d rsqrt(d)), a named barrier of the two warps, the column through
+// shared memory, a rank-1 update of the row in registers).  Two variants measured no faster: one
+// barrier per pivot with every row forming the reciprocal square root from a double-buffered
+// column (+8%), and a look-ahead in which row j + 1 forms the next pivot before finishing its
+// update (+2%).  Meanwhile warps 2-7 copy the panel rows; a block smaller than CB (the last) is
+// padded with the identity.
+// The inverse X = L^-1 goes by 32 x 32 blocks: warps 0 and 1 run the forward substitutions of
+// X11 and X22 (lane = column, in registers, four partial sums per row), then all eight warps form
+// X21 = -X22 (L21 X11).  Every loop is unrolled, so the row and column registers are addressed at
+// compile time (a variant with the pivot loop rolled and the row shifted through the registers ran
+// slower).
+constexpr int HB = CB / 2, HBP = HB + 1;   // half blocks of the block inverse
 __device__ __forceinline__ void potrf_bar() { asm volatile("bar.sync 1, %0;" ::"n"(CB) : "memory"); }
 
 // FACTOR = false: the band already holds a Cholesky factor; only the diagonal block's inverse is
@@ -110,23 +116,23 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
     __shared__ double colj[CB], rinv[CB];
     double (*D)[CBP] = reinterpret_cast<double (*)[CBP]>(psm);
     double (*X)[CBP] = reinterpret_cast<double (*)[CBP]>(psm + CB * CBP);
+    double (*Tm)[HBP] = reinterpret_cast<double (*)[HBP]>(psm + 2 * CB * CBP);   // L21 X11
     const int w = min(CB, n - k0);
     const int base = k0 + w, rend = min(n, k0 + w + bw);
     const int t = threadIdx.x;
-    if constexpr (FACTOR) {
-        #pragma unroll 8
-        for (int i = t; i < (rend - base) * CB; i += POTRF_T) {
-            const int r = base + i / CB, c = i % CB, col = k0 + c;
-            apanel[i] = (c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
+    {                                                  // the block: every load issued, then stored
+        constexpr int NL = CB * CB / POTRF_T;
+        double v[NL];
+        #pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int i = t + u * POTRF_T, r = i / CB, c = i % CB;
+            v[u] = (r < w && c <= r && r - c <= bw) ? lb[bidx(k0 + r, k0 + c, bw)] : (r >= w && r == c ? 1.0 : 0.0);
+        }                                              // (identity padding of a short block)
+        #pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int i = t + u * POTRF_T;
+            D[i / CB][i % CB] = v[u];
         }
-    }
-    #pragma unroll
-    for (int i = t; i < CB * CB; i += POTRF_T) {
-        const int r = i / CB, c = i % CB;
-        double v = 0.0;
-        if (r < w) v = (c <= r && r - c <= bw) ? lb[bidx(k0 + r, k0 + c, bw)] : 0.0;
-        else if (r == c) v = 1.0;                      // identity padding of a short block
-        D[r][c] = v;
     }
     __syncthreads();
     if (!FACTOR && t < CB) rinv[t] = 1.0 / D[t][t];
@@ -142,9 +148,9 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
                     if (j < w) atomicCAS(info, 0, k0 + j + 1);
                     d = 1.0;
                 }
-                const double piv = sqrt(d);
-                a[j] = piv;
-                rinv[j] = 1.0 / piv;
+                const double ri = rsqrt(d);
+                a[j] = d * ri;
+                rinv[j] = ri;
             }
             potrf_bar();
             if (t > j) {
@@ -161,23 +167,71 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
         }
         #pragma unroll
         for (int c = 0; c < CB; ++c) D[t][c] = c <= t ? a[c] : 0.0;
+    } else if (FACTOR) {                               // meanwhile warps 2-7 copy the panel rows
+        // in batches whose loads are all issued before their stores: the band and the panel share
+        // one workspace, so the compiler may not move a load above an earlier store by itself
+        constexpr int CPB = 16, CPT = POTRF_T - CB;
+        const int total = (rend - base) * CB;
+        for (int i0 = t - CB; i0 < total; i0 += CPB * CPT) {
+            double v[CPB];
+            #pragma unroll
+            for (int u = 0; u < CPB; ++u) {
+                const int i = i0 + u * CPT, r = base + i / CB, c = i % CB, col = k0 + c;
+                v[u] = (i < total && c < w && r - col <= bw) ? lb[bidx(r, col, bw)] : 0.0;
+            }
+            #pragma unroll
+            for (int u = 0; u < CPB; ++u)
+                if (i0 + u * CPT < total) apanel[i0 + u * CPT] = v[u];
+        }
     }
     __syncthreads();
-    if (t < CB) {                                       // column t of X = L^-1
-        double x[CB];
+    // X = L^-1 by 32 x 32 blocks: X11 (warp 0) and X22 (warp 1) by forward substitution, lane = column,
+    // in registers; then X21 = -X22 (L21 X11) by all threads
+    if (t < 2 * HB) {
+        const int o = (t / HB) * HB, c = t % HB;
+        double x[HB];
         #pragma unroll
-        for (int r = 0; r < CB; ++r) {
-            double s0 = 0.0, s1 = 0.0;
+        for (int r = 0; r < HB; ++r) {
+            double s[4] = {0.0, 0.0, 0.0, 0.0};
             #pragma unroll
-            for (int p = 0; p + 1 < r; p += 2) {
-                s0 += D[r][p] * x[p];
-                s1 += D[r][p + 1] * x[p + 1];
-            }
-            if (r & 1) s0 += D[r][r - 1] * x[r - 1];
-            x[r] = ((r == t ? 1.0 : 0.0) - (s0 + s1)) * rinv[r];
+            for (int p = 0; p < r; ++p) s[p & 3] += D[o + r][o + p] * x[p];
+            x[r] = ((r == c ? 1.0 : 0.0) - ((s[0] + s[1]) + (s[2] + s[3]))) * rinv[o + r];
         }
         #pragma unroll
-        for (int r = 0; r < CB; ++r) X[r][t] = x[r];
+        for (int r = 0; r < HB; ++r) X[o + r][o + c] = x[r];
+    } else {
+        for (int i = t - 2 * HB; i < HB * HB; i += POTRF_T - 2 * HB) X[i / HB][HB + i % HB] = 0.0;
+    }
+    __syncthreads();
+    const int tc = t % HB, tr = t / HB;                // column and first row of this thread's outputs
+    constexpr int NR = HB * HB / POTRF_T;              // outputs per thread, rows tr + RS m
+    constexpr int RS = POTRF_T / HB;
+    {
+        double s[NR];
+        #pragma unroll
+        for (int m = 0; m < NR; ++m) s[m] = 0.0;
+        #pragma unroll
+        for (int p = 0; p < HB; ++p) {                 // Tm = L21 X11
+            const double xv = X[p][tc];
+            #pragma unroll
+            for (int m = 0; m < NR; ++m) s[m] += D[HB + tr + RS * m][p] * xv;
+        }
+        #pragma unroll
+        for (int m = 0; m < NR; ++m) Tm[tr + RS * m][tc] = s[m];
+    }
+    __syncthreads();
+    {
+        double s[NR];
+        #pragma unroll
+        for (int m = 0; m < NR; ++m) s[m] = 0.0;
+        #pragma unroll
+        for (int p = 0; p < HB; ++p) {                 // X21 = -X22 Tm (X22 lower triangular, zeros above)
+            const double tv = Tm[p][tc];
+            #pragma unroll
+            for (int m = 0; m < NR; ++m) s[m] += X[HB + tr + RS * m][HB + p] * tv;
+        }
+        #pragma unroll
+        for (int m = 0; m < NR; ++m) X[HB + tr + RS * m][tc] = -s[m];
     }
     __syncthreads();
     #pragma unroll
@@ -283,13 +337,23 @@ __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, in
             for (int b = 0; b < 4; ++b) o[a][b] = fma(pi[a], pj[b], o[a][b]);
         }
     }
+    double cur[4][4];                                  // every old value read before any write
+    #pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int ri = ri0 + tr + 16 * a, rj = rj0 + tc + 16 * b;
+            const bool in = ri < rend && rj < rend && rj <= ri && ri - rj <= bw;
+            cur[a][b] = in ? lb[bidx(ri, rj, bw)] : 0.0;
+        }
+    }
     #pragma unroll
     for (int a = 0; a < 4; ++a) {
         #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const int ri = ri0 + tr + 16 * a, rj = rj0 + tc + 16 * b;
             if (ri >= rend || rj >= rend || rj > ri || ri - rj > bw) continue;
-            lb[bidx(ri, rj, bw)] -= o[a][b];
+            lb[bidx(ri, rj, bw)] = cur[a][b] - o[a][b];
         }
     }
 }
@@ -412,10 +476,25 @@ __global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int
     for (int i = t; i < WR * ITC; i += INVB_T) Wr[i] = 0.0;
     for (int i0 = c0; i0 < n; i0 += IRB) {
         __syncthreads();                               // the previous block's reads of Ls, Dv, St are done
-        // stage the band rows (zero outside row i's band and beyond n) and the diagonal block inverse
-        for (int i = t; i < IRB * bw; i += INVB_T) {
-            const int r = i / bw, q = i % bw, row = i0 + r;
-            Ls[r * LSW + q] = (q >= r && row < n) ? lb[int64_t(row) * (bw + 1) + (q - r)] : 0.0;
+        // stage the band rows (zero outside row i's band and beyond n) and the diagonal block inverse:
+        // warp rg copies rows rg, rg + 8, ..., lanes along the row, every load of a batch issued
+        // before its stores (the staging is on the chain of every block step)
+        #pragma unroll
+        for (int rr = rg; rr < IRB; rr += INVB_T / 32) {
+            const int row = i0 + rr;
+            const double* src = lb + int64_t(row) * (bw + 1) - rr;   // src[q] = L[row][i0 - bw + q]
+            double* dst = Ls + rr * LSW;
+            for (int q0 = c; q0 < bw; q0 += 4 * 32) {
+                double v[4];
+                #pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int q = q0 + 32 * u;
+                    v[u] = (q < bw && q >= rr && row < n) ? src[q] : 0.0;
+                }
+                #pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (q0 + 32 * u < bw) dst[q0 + 32 * u] = v[u];
+            }
         }
         const double* dsrc = dinv_all + int64_t(i0 / CB) * CB * CB + (i0 % CB) * CB + (i0 % CB);
         for (int i = t; i < IRB * IRB; i += INVB_T) {
@@ -524,7 +603,7 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
             return VX_ERR_CUDA;
         }
     }
-    const size_t psm = size_t(2) * CB * CBP * sizeof(double);
+    const size_t psm = size_t(2 * CB * CBP + HB * HBP) * sizeof(double);
     const size_t usm = size_t(3) * CB * CBP * sizeof(double);
     const size_t ism = size_t(INV_STAGES + nw) * (bw + 1) * sizeof(double);
     static std::atomic<uint64_t> opt_p, opt_u, opt_i, opt_b;
@@ -598,7 +677,7 @@ extern "C" int vx_coarse_pack_factor(int n, int bw, const double* L, double* pac
     fb.ws = vx_coarse_factor_workspace(n, bw);
     fb.nblk = (n + CB - 1) / CB;
     fb.slot[0] = 0;
-    const size_t psm = size_t(2) * CB * CBP * sizeof(double);
+    const size_t psm = size_t(2 * CB * CBP + HB * HBP) * sizeof(double);
     const size_t ism = size_t(INV_STAGES + nw) * (bw + 1) * sizeof(double);
     static std::atomic<uint64_t> opt_p, opt_i, opt_b;
     int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel<false>, psm, what);
