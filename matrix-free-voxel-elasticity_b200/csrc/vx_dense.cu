@@ -13,8 +13,8 @@
 //                     bw below it) forms the panel rows L_I = A_I L_kk^-T and L_J the same way (a
 //                     64 x 64 product with the block's inverse), writes L_I (diagonal tiles only),
 //                     and subtracts L_I L_J^T from the band;
-//   * band_inverse_blocked: X = L^-1 by blocks of 32 rows x 32 columns, a band GEMM per block and
-//                     the diagonal block inverses band_potrf kept (bands up to about 600 wide);
+//   * band_inverse_blocked: X = L^-1 by blocks of 32 rows x 16 columns, a band GEMM per block and
+//                     the diagonal block inverses band_potrf kept (bands up to about 550 wide);
 //   * band_inverse:   (wider bands) X = L^-1 column by column: a CTA owns 32 consecutive columns (one warp each),
 //                     streams the band rows of L through shared memory by cp.async, and each warp
 //                     runs the forward substitution x_i = -(sum_p L[i][p] x_p) / L[i][i] over the
@@ -433,58 +433,69 @@ __global__ void band_inverse_kernel(int n, int bw, const __grid_constant__ Facto
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-// X = L^-1 by blocks of IRB rows for ITC columns per CTA (columns c0 .. c0 + ITC - 1).  Walking down
-// the row blocks i0 = c0, c0 + IRB, ...:
+// X = L^-1 by blocks of IRB rows for TC columns per CTA (columns c0 .. c0 + TC - 1).  Walking down
+// the row blocks i0 = IRB floor(c0 / IRB), + IRB, ...:
 //     S   = L[i0 .. i0 + IRB)[i0 - bw .. i0) X[i0 - bw .. i0)[cols]     (the band left of the block)
 //     X_I = Dinv_I (E_I - S)                                          (E_I: the identity's rows)
 // with Dinv_I the inverse of L's IRB x IRB diagonal block (the diagonal sub-blocks of the CB-block
 // inverses band_potrf kept, dinv_all).  The last WR >= bw + IRB rows of X for these columns live in a
 // shared-memory ring (rows above c0 are zero and never written); the band rows of L are staged per
 // block; each finished block goes to M[i][j] (rows, coalesced over columns) and, through shared memory,
-// to M[j][i] (coalesced over rows).  Thread t: column t % 32, rows t / 32 + 8 m (m < 4).
-constexpr int IRB = 32, ITC = 32, INVB_T = 256;
+// to M[j][i] (coalesced over rows).  Thread t: column t % TC, rows t / TC + (INVB_T / TC) m.
+// The first CTA's walk over all n / IRB row blocks is the critical path, and each step's band product
+// (IRB x bw x TC multiply-adds on one SM) sets its length: INV_TC = 16 columns per CTA halves the step
+// of 32 columns for twice the CTAs (the band rows are staged by each CTA, from L2).
+constexpr int IRB = 32, INVB_T = 256, INV_TC = 16;
 
+template <int TC>
 struct InvbLayout {
     int bw, WR;
     size_t ls, ring, dv, st, bytes;
     __host__ __device__ explicit InvbLayout(int bw_) : bw(bw_) {
         WR = (bw + IRB + IRB - 1) / IRB * IRB;
         ls = size_t(IRB) * (bw + 1);                 // staged band rows, padded
-        ring = size_t(WR) * ITC;
+        ring = size_t(WR) * TC;
         dv = size_t(IRB) * (IRB + 1);
-        st = size_t(IRB) * (ITC + 1);
+        st = size_t(IRB) * (TC + 1);
         bytes = (ls + ring + dv + st) * sizeof(double);
     }
 };
 
+template <int TC>
 __global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int bw, const __grid_constant__ FactorBatch fb) {
+    static_assert(TC >= 8 && TC <= 32 && INVB_T % TC == 0 && IRB * TC % INVB_T == 0, "thread layout");
+    constexpr int RG = INVB_T / TC;                    // row groups
+    constexpr int MR = IRB / RG;                       // rows per thread
+    constexpr int KQ = MR >= 4 ? 1 : 4 / MR;           // partial sums per row over the band
     vx::pdl_begin();
     const FactorPtrs P = fptrs(fb, n, bw);
     const double* __restrict__ lb = P.lb;
     const double* __restrict__ dinv_all = P.dinv_all;
     double* __restrict__ packed = P.packed;
     extern __shared__ __align__(16) double sm[];
-    const InvbLayout Lo(bw);
+    const InvbLayout<TC> Lo(bw);
     const int LSW = bw + 1;
     double* Ls = sm;                                   // [IRB][bw + 1]: Ls[r][q] = L[i0 + r][i0 - bw + q], q < bw
-    double* Wr = Ls + Lo.ls;                           // [WR][ITC] ring of X rows
+    double* Wr = Ls + Lo.ls;                           // [WR][TC] ring of X rows
     double* Dv = Wr + Lo.ring;                         // [IRB][IRB + 1]
-    double* St = Dv + Lo.dv;                           // [IRB][ITC + 1]
-    const int t = threadIdx.x, c = t & 31, rg = t >> 5;
-    const int c0 = blockIdx.x * ITC;
+    double* St = Dv + Lo.dv;                           // [IRB][TC + 1]
+    const int t = threadIdx.x, c = t % TC, rg = t / TC, lane = t & 31, wid = t >> 5;
+    const int c0 = blockIdx.x * TC;
     const int WR = Lo.WR;
-    for (int i = t; i < WR * ITC; i += INVB_T) Wr[i] = 0.0;
-    for (int i0 = c0; i0 < n; i0 += IRB) {
+    for (int i = t; i < WR * TC; i += INVB_T) Wr[i] = 0.0;
+    // row blocks aligned to IRB (the diagonal block inverses are IRB-aligned sub-blocks of the CB-block
+    // inverses); rows above c0 come out zero for these columns
+    for (int i0 = c0 / IRB * IRB; i0 < n; i0 += IRB) {
         __syncthreads();                               // the previous block's reads of Ls, Dv, St are done
         // stage the band rows (zero outside row i's band and beyond n) and the diagonal block inverse:
-        // warp rg copies rows rg, rg + 8, ..., lanes along the row, every load of a batch issued
-        // before its stores (the staging is on the chain of every block step)
+        // warp w copies rows w, w + 8, ..., lanes along the row, every load of a batch issued before
+        // its stores (the staging is on the chain of every block step)
         #pragma unroll
-        for (int rr = rg; rr < IRB; rr += INVB_T / 32) {
+        for (int rr = wid; rr < IRB; rr += INVB_T / 32) {
             const int row = i0 + rr;
             const double* src = lb + int64_t(row) * (bw + 1) - rr;   // src[q] = L[row][i0 - bw + q]
             double* dst = Ls + rr * LSW;
-            for (int q0 = c; q0 < bw; q0 += 4 * 32) {
+            for (int q0 = lane; q0 < bw; q0 += 4 * 32) {
                 double v[4];
                 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
@@ -504,52 +515,69 @@ __global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int
         __syncthreads();
         // S = Ls X_window over the band columns that can be non-zero (rows >= c0)
         const int q0 = max(0, c0 - (i0 - bw));
-        double s[4] = {0.0, 0.0, 0.0, 0.0};
+        double s[MR][KQ];
+        #pragma unroll
+        for (int m = 0; m < MR; ++m)
+            #pragma unroll
+            for (int k = 0; k < KQ; ++k) s[m][k] = 0.0;
         int slot = (i0 - bw + q0) % WR;
         if (slot < 0) slot += WR;
-        for (int q = q0; q < bw; ++q) {
-            const double x = Wr[slot * ITC + c];
+        int q = q0;
+        for (; q + KQ <= bw; q += KQ) {
             #pragma unroll
-            for (int m = 0; m < 4; ++m) s[m] += Ls[(rg + 8 * m) * LSW + q] * x;
+            for (int k = 0; k < KQ; ++k) {
+                const double x = Wr[slot * TC + c];
+                #pragma unroll
+                for (int m = 0; m < MR; ++m) s[m][k] += Ls[(rg + RG * m) * LSW + q + k] * x;
+                if (++slot == WR) slot = 0;
+            }
+        }
+        for (; q < bw; ++q) {
+            const double x = Wr[slot * TC + c];
+            #pragma unroll
+            for (int m = 0; m < MR; ++m) s[m][0] += Ls[(rg + RG * m) * LSW + q] * x;
             if (++slot == WR) slot = 0;
         }
         #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const int r = rg + 8 * m;
-            St[r * (ITC + 1) + c] = ((i0 + r == c0 + c) ? 1.0 : 0.0) - s[m];
+        for (int m = 0; m < MR; ++m) {
+            const int r = rg + RG * m;
+            double sum = s[m][0];
+            #pragma unroll
+            for (int k = 1; k < KQ; ++k) sum += s[m][k];
+            St[r * (TC + 1) + c] = ((i0 + r == c0 + c) ? 1.0 : 0.0) - sum;
         }
         __syncthreads();
         // X_I = Dinv_I (E_I - S)
-        double x[4];
+        double x[MR];
         #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const int r = rg + 8 * m;
+        for (int m = 0; m < MR; ++m) {
+            const int r = rg + RG * m;
             double a0 = 0.0, a1 = 0.0;
             int k = 0;
             for (; k + 1 <= r; k += 2) {
-                a0 += Dv[r * (IRB + 1) + k] * St[k * (ITC + 1) + c];
-                a1 += Dv[r * (IRB + 1) + k + 1] * St[(k + 1) * (ITC + 1) + c];
+                a0 += Dv[r * (IRB + 1) + k] * St[k * (TC + 1) + c];
+                a1 += Dv[r * (IRB + 1) + k + 1] * St[(k + 1) * (TC + 1) + c];
             }
-            if (k == r) a0 += Dv[r * (IRB + 1) + k] * St[k * (ITC + 1) + c];
+            if (k == r) a0 += Dv[r * (IRB + 1) + k] * St[k * (TC + 1) + c];
             x[m] = a0 + a1;
         }
         __syncthreads();                               // every read of St done before it holds X_I
         #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const int r = rg + 8 * m, i = i0 + r, j = c0 + c;
+        for (int m = 0; m < MR; ++m) {
+            const int r = rg + RG * m, i = i0 + r, j = c0 + c;
             const bool ok = i < n && j < n && i >= j;
             const double v = ok ? x[m] : 0.0;
             int ws = i % WR;
-            Wr[ws * ITC + c] = v;
-            St[r * (ITC + 1) + c] = v;
+            Wr[ws * TC + c] = v;
+            St[r * (TC + 1) + c] = v;
             if (ok) packed[int64_t(i) * n + j] = v;    // lower part, coalesced over columns
         }
         __syncthreads();
         // upper part M[j][i] = X[i][j], coalesced over rows: lane = row of the block
         #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const int cc = rg + 8 * m, r = c, i = i0 + r, j = c0 + cc;
-            if (i < n && j < n && i > j) packed[int64_t(j) * n + i] = St[r * (ITC + 1) + cc];
+        for (int m = 0; m < TC / 8; ++m) {
+            const int cc = wid + 8 * m, r = lane, i = i0 + r, j = c0 + cc;
+            if (i < n && j < n && i > j) packed[int64_t(j) * n + i] = St[r * (TC + 1) + cc];
         }
     }
 }
@@ -610,7 +638,7 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
     int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel<true>, psm, what);
     if (!st) st = smem_opt_in(opt_u, (const void*)band_update_kernel, usm, what);
     if (!st) st = smem_opt_in(opt_i, (const void*)band_inverse_kernel, 227 * 1024, what);
-    if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, what);
+    if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel<INV_TC>, 227 * 1024, what);
     if (st) return st;
     const unsigned B = unsigned(count);
     const int64_t band = int64_t(n) * (bw + 1);
@@ -623,9 +651,9 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
         const int T = (rows + CB - 1) / CB;
         vx::launch(band_update_kernel, dim3(unsigned(T * (T + 1) / 2), B), UPDATE_T, usm, stream, n, bw, k0, T, fb);
     }
-    const InvbLayout il(bw);
+    const InvbLayout<INV_TC> il(bw);
     if (il.bytes <= 227 * 1024) {
-        vx::launch(band_inverse_blocked_kernel, dim3(unsigned((n + ITC - 1) / ITC), B), INVB_T, il.bytes, stream, n,
+        vx::launch(band_inverse_blocked_kernel<INV_TC>, dim3(unsigned((n + INV_TC - 1) / INV_TC), B), INVB_T, il.bytes, stream, n,
                    bw, fb);
     } else {
         vx::launch(band_inverse_kernel, dim3(unsigned((n + nw - 1) / nw), B), unsigned(nw * 32), ism, stream, n, bw,
@@ -682,14 +710,14 @@ extern "C" int vx_coarse_pack_factor(int n, int bw, const double* L, double* pac
     static std::atomic<uint64_t> opt_p, opt_i, opt_b;
     int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel<false>, psm, what);
     if (!st) st = smem_opt_in(opt_i, (const void*)band_inverse_kernel, 227 * 1024, what);
-    if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel, 227 * 1024, what);
+    if (!st) st = smem_opt_in(opt_b, (const void*)band_inverse_blocked_kernel<INV_TC>, 227 * 1024, what);
     if (st) return st;
     const int64_t band = int64_t(n) * (bw + 1);
     vx::launch(band_load_kernel, dim3(unsigned((band + 255) / 256), 1), 256, 0, stream, n, bw, fb);
     vx::launch(band_potrf_kernel<false>, dim3(unsigned(fb.nblk), 1), POTRF_T, psm, stream, n, bw, 0, fb);
-    const InvbLayout il(bw);
+    const InvbLayout<INV_TC> il(bw);
     if (il.bytes <= 227 * 1024) {
-        vx::launch(band_inverse_blocked_kernel, dim3(unsigned((n + ITC - 1) / ITC), 1), INVB_T, il.bytes, stream, n,
+        vx::launch(band_inverse_blocked_kernel<INV_TC>, dim3(unsigned((n + INV_TC - 1) / INV_TC), 1), INVB_T, il.bytes, stream, n,
                    bw, fb);
     } else {
         vx::launch(band_inverse_kernel, dim3(unsigned((n + nw - 1) / nw), 1), unsigned(nw * 32), ism, stream, n, bw,
