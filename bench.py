@@ -264,6 +264,19 @@ def kernel_table(solver, vx, torch, flush, reps=10):
     return rows
 
 
+def coarse_factor_time(solver, flush, reps=3):
+    """Device time of the coarsest level's factorisation (banded Cholesky and packed inverse factor,
+    vx_coarse_factor) on the solver's own coarse matrix.  Every hierarchy refresh runs it, so it is
+    part of each e2e call."""
+    M = solver.M
+    if getattr(M, "A_coarse", None) is None or M.A_coarse.dim() != 2:
+        return None
+    n = int(M.A_coarse.shape[0])
+    nx, ny, nz = M.levels[-1].shape
+    bw = min(n - 1, 3 * ((ny + 1) * (nz + 1) + (nz + 1) + 1) + 2)
+    return {"ms": kernel_time(M._coarse_inverse, reps, flush) * 1e3, "n": n, "bw": bw}
+
+
 # ----------------------------------------------------------------------------------- arms
 def solve_arm(shape, E, mask, force, precision, kw, args, flush, rank_sync):
     """Build a solver of `precision`, time it (CUDA events, L2 flushed), return (solver, times, result)."""
@@ -351,6 +364,7 @@ def run_b200(args, rank, world, local_rank):
                        "kernels": {k: {"launch_us": v[0] * 1e6, "GB/s": v[1] / v[0] / 1e9, "frac_hbm": v[1] / v[0] / 1e9 / hbm,
                                        "per_solve": counts.get(k, 0)} for k, v in table.items()}}
     out["matvec"] = {"GDOF/s_f64_apply": 3 * solver.op64.nodes / table["apply_dot_f64"][0] / 1e9}
+    out["coarse_factor"] = coarse_factor_time(solver, flush)
     out["clocks"] = clocks.summary()
     products = products_per_solve(res, levels, 2, 2, kw["check_every"])
     del solver
@@ -473,6 +487,8 @@ def small_section(args, flush, rank_sync):
         s, times, res = solve_arm(shape, E, mask, force, prec, kw, args, flush, rank_sync)
         out[prec] = {"s": float(np.mean(times)), "iterations": res.iterations, "rel": res.rel,
                      "compliance": float(force @ res.x)}
+        if prec == "mixed":
+            out["coarse_factor"] = coarse_factor_time(s, flush)
         del s
     torch.cuda.empty_cache()
     cpu = cpu_baseline(name)
