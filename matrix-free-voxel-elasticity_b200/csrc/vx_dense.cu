@@ -440,24 +440,27 @@ __global__ void band_inverse_kernel(int n, int bw, const __grid_constant__ Facto
 // with Dinv_I the inverse of L's IRB x IRB diagonal block (the diagonal sub-blocks of the CB-block
 // inverses band_potrf kept, dinv_all).  The last WR >= bw + IRB rows of X for these columns live in a
 // shared-memory ring (rows above c0 are zero and never written); the band rows of L are staged per
-// block; each finished block goes to M[i][j] (rows, coalesced over columns) and, through shared memory,
-// to M[j][i] (coalesced over rows).  Thread t: column t % TC, rows t / TC + (INVB_T / TC) m.
+// block, transposed; S is a band GEMM split over the warps along the band (a 4 x 4 register tile per
+// lane); each finished block goes to M[i][j] (rows, coalesced over columns) and, through shared
+// memory, to M[j][i] (coalesced over rows).  Thread t: column t % TC, rows t / TC + (INVB_T / TC) m.
 // The first CTA's walk over all n / IRB row blocks is the critical path, and each step's band product
 // (IRB x bw x TC multiply-adds on one SM) sets its length: INV_TC = 16 columns per CTA halves the step
 // of 32 columns for twice the CTAs (the band rows are staged by each CTA, from L2).
 constexpr int IRB = 32, INVB_T = 256, INV_TC = 16;
+constexpr int LTP = IRB + 2;   // row of the transposed band stage: 16-byte aligned, stores 4-way at most
 
 template <int TC>
 struct InvbLayout {
     int bw, WR;
-    size_t ls, ring, dv, st, bytes;
+    size_t ls, ring, dv, st, red, bytes;
     __host__ __device__ explicit InvbLayout(int bw_) : bw(bw_) {
         WR = (bw + IRB + IRB - 1) / IRB * IRB;
-        ls = size_t(IRB) * (bw + 1);                 // staged band rows, padded
+        ls = size_t(bw) * LTP;                       // staged band rows, transposed: [q][row]
         ring = size_t(WR) * TC;
         dv = size_t(IRB) * (IRB + 1);
         st = size_t(IRB) * (TC + 1);
-        bytes = (ls + ring + dv + st) * sizeof(double);
+        red = size_t(INVB_T / 32) * IRB * TC;        // per-warp partial products
+        bytes = (ls + ring + dv + st + red) * sizeof(double);
     }
 };
 
@@ -466,7 +469,6 @@ __global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int
     static_assert(TC >= 8 && TC <= 32 && INVB_T % TC == 0 && IRB * TC % INVB_T == 0, "thread layout");
     constexpr int RG = INVB_T / TC;                    // row groups
     constexpr int MR = IRB / RG;                       // rows per thread
-    constexpr int KQ = MR >= 4 ? 1 : 4 / MR;           // partial sums per row over the band
     vx::pdl_begin();
     const FactorPtrs P = fptrs(fb, n, bw);
     const double* __restrict__ lb = P.lb;
@@ -474,11 +476,11 @@ __global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int
     double* __restrict__ packed = P.packed;
     extern __shared__ __align__(16) double sm[];
     const InvbLayout<TC> Lo(bw);
-    const int LSW = bw + 1;
-    double* Ls = sm;                                   // [IRB][bw + 1]: Ls[r][q] = L[i0 + r][i0 - bw + q], q < bw
+    double* Ls = sm;                                   // [bw][LTP]: Ls[q][r] = L[i0 + r][i0 - bw + q], q < bw
     double* Wr = Ls + Lo.ls;                           // [WR][TC] ring of X rows
     double* Dv = Wr + Lo.ring;                         // [IRB][IRB + 1]
     double* St = Dv + Lo.dv;                           // [IRB][TC + 1]
+    double* Red = St + Lo.st;                          // [warps][IRB x TC] partial band products
     const int t = threadIdx.x, c = t % TC, rg = t / TC, lane = t & 31, wid = t >> 5;
     const int c0 = blockIdx.x * TC;
     const int WR = Lo.WR;
@@ -487,63 +489,87 @@ __global__ void __launch_bounds__(INVB_T) band_inverse_blocked_kernel(int n, int
     // inverses); rows above c0 come out zero for these columns
     for (int i0 = c0 / IRB * IRB; i0 < n; i0 += IRB) {
         __syncthreads();                               // the previous block's reads of Ls, Dv, St are done
-        // stage the band rows (zero outside row i's band and beyond n) and the diagonal block inverse:
-        // warp w copies rows w, w + 8, ..., lanes along the row, every load of a batch issued before
-        // its stores (the staging is on the chain of every block step)
-        #pragma unroll
-        for (int rr = wid; rr < IRB; rr += INVB_T / 32) {
-            const int row = i0 + rr;
-            const double* src = lb + int64_t(row) * (bw + 1) - rr;   // src[q] = L[row][i0 - bw + q]
-            double* dst = Ls + rr * LSW;
-            for (int q0 = lane; q0 < bw; q0 += 4 * 32) {
-                double v[4];
-                #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int q = q0 + 32 * u;
-                    v[u] = (q < bw && q >= rr && row < n) ? src[q] : 0.0;
-                }
-                #pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    if (q0 + 32 * u < bw) dst[q0 + 32 * u] = v[u];
-            }
-        }
+        // stage the band rows (zero outside row i's band and beyond n), transposed, and the diagonal
+        // block inverse: warp w copies rows w, w + 8, ..., lanes along the row.  The staging is on the
+        // chain of every block step, so each thread issues all of its loads (up to SQ 32-column
+        // chunks of its four rows, one round trip for bands up to 32 SQ wide) before any store.
+        constexpr int SQ = 9;
         const double* dsrc = dinv_all + int64_t(i0 / CB) * CB * CB + (i0 % CB) * CB + (i0 % CB);
-        for (int i = t; i < IRB * IRB; i += INVB_T) {
-            const int r = i / IRB, k = i % IRB;
-            Dv[r * (IRB + 1) + k] = (k <= r) ? dsrc[r * CB + k] : 0.0;
+        double dv[IRB * IRB / INVB_T];
+        #pragma unroll
+        for (int u = 0; u < IRB * IRB / INVB_T; ++u) {
+            const int i = t + u * INVB_T, r = i / IRB, k = i % IRB;
+            dv[u] = (k <= r) ? dsrc[r * CB + k] : 0.0;
+        }
+        for (int qb = 0; qb < bw; qb += 32 * SQ) {
+            double v[4][SQ];
+            #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int rr = wid + 8 * j, row = i0 + rr;
+                const double* src = lb + int64_t(row) * (bw + 1) - rr;   // src[q] = L[row][i0 - bw + q]
+                #pragma unroll
+                for (int u = 0; u < SQ; ++u) {
+                    const int q = qb + lane + 32 * u;
+                    v[j][u] = (q < bw && q >= rr && row < n) ? src[q] : 0.0;
+                }
+            }
+            #pragma unroll
+            for (int j = 0; j < 4; ++j)
+                #pragma unroll
+                for (int u = 0; u < SQ; ++u) {
+                    const int q = qb + lane + 32 * u;
+                    if (q < bw) Ls[q * LTP + wid + 8 * j] = v[j][u];
+                }
+        }
+        #pragma unroll
+        for (int u = 0; u < IRB * IRB / INVB_T; ++u) {
+            const int i = t + u * INVB_T;
+            Dv[(i / IRB) * (IRB + 1) + i % IRB] = dv[u];
         }
         __syncthreads();
-        // S = Ls X_window over the band columns that can be non-zero (rows >= c0)
-        const int q0 = max(0, c0 - (i0 - bw));
-        double s[MR][KQ];
-        #pragma unroll
-        for (int m = 0; m < MR; ++m)
+        // S = Ls X_window over the band columns that can be non-zero (rows >= c0): warp w takes the
+        // w-th eighth of those columns for the whole IRB x TC block, lane = a 4 x 4 register tile
+        // (rows 4 (lane / 4) .., columns 4 (lane % 4) ..) read as 16-byte pairs from the transposed
+        // band stage and the ring; the warps' partial tiles are then summed through shared memory.
+        static_assert(IRB == 32 && TC == 16 && INVB_T == 256, "8 warps x 32 lanes x 4 x 4 tiles cover 32 x 16");
+        {
+            const int q0 = max(0, c0 - (i0 - bw));
+            const int len = bw - q0, chunk = (len + 7) / 8;
+            const int qs = q0 + wid * max(chunk, 0), qe = min(bw, qs + max(chunk, 0));
+            const int tr = 4 * (lane >> 2), tcol = 4 * (lane & 3);
+            double acc[4][4];
             #pragma unroll
-            for (int k = 0; k < KQ; ++k) s[m][k] = 0.0;
-        int slot = (i0 - bw + q0) % WR;
-        if (slot < 0) slot += WR;
-        int q = q0;
-        for (; q + KQ <= bw; q += KQ) {
-            #pragma unroll
-            for (int k = 0; k < KQ; ++k) {
-                const double x = Wr[slot * TC + c];
+            for (int i = 0; i < 4; ++i)
                 #pragma unroll
-                for (int m = 0; m < MR; ++m) s[m][k] += Ls[(rg + RG * m) * LSW + q + k] * x;
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            int slot = (i0 - bw + qs) % WR;
+            if (slot < 0) slot += WR;
+            #pragma unroll 2
+            for (int q = qs; q < qe; ++q) {
+                const double2 l01 = *reinterpret_cast<const double2*>(Ls + q * LTP + tr);
+                const double2 l23 = *reinterpret_cast<const double2*>(Ls + q * LTP + tr + 2);
+                const double2 w01 = *reinterpret_cast<const double2*>(Wr + slot * TC + tcol);
+                const double2 w23 = *reinterpret_cast<const double2*>(Wr + slot * TC + tcol + 2);
+                const double l[4] = {l01.x, l01.y, l23.x, l23.y}, x[4] = {w01.x, w01.y, w23.x, w23.y};
+                #pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    #pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] += l[i] * x[j];
                 if (++slot == WR) slot = 0;
             }
-        }
-        for (; q < bw; ++q) {
-            const double x = Wr[slot * TC + c];
+            double* rw = Red + wid * (IRB * TC);
             #pragma unroll
-            for (int m = 0; m < MR; ++m) s[m][0] += Ls[(rg + RG * m) * LSW + q] * x;
-            if (++slot == WR) slot = 0;
+            for (int i = 0; i < 4; ++i)
+                #pragma unroll
+                for (int j = 0; j < 4; ++j) rw[(tr + i) * TC + tcol + j] = acc[i][j];
         }
+        __syncthreads();
         #pragma unroll
         for (int m = 0; m < MR; ++m) {
             const int r = rg + RG * m;
-            double sum = s[m][0];
+            double sum = 0.0;
             #pragma unroll
-            for (int k = 1; k < KQ; ++k) sum += s[m][k];
+            for (int w = 0; w < INVB_T / 32; ++w) sum += Red[w * (IRB * TC) + r * TC + c];
             St[r * (TC + 1) + c] = ((i0 + r == c0 + c) ? 1.0 : 0.0) - sum;
         }
         __syncthreads();
