@@ -24,6 +24,7 @@
 #include "vx_common.cuh"
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 
 namespace vx {
 
@@ -84,27 +85,29 @@ __global__ void band_load_kernel(int n, int bw, const __grid_constant__ FactorBa
 // inverse goes to dinv (CB x CB, row-major, lower triangle), and the block column's rows below it
 // (the A values band_update turns into the panel) to apanel ((bw + 1) x CB), so that band_update
 // can store finished panel rows in place while other tiles still read the originals.
-// The block's CB pivots are a chain of dependent steps, so it is factored by CB threads with the
-// rows in registers (right-looking; thread i holds row i; per pivot: the pivot thread's reciprocal
-// square root (the pivot is d rsqrt(d)), a named barrier of the two warps, the column through
-// shared memory, a rank-1 update of the row in registers).  Two variants measured no faster: one
-// barrier per pivot with every row forming the reciprocal square root from a double-buffered
-// column (+8%), and a look-ahead in which row j + 1 forms the next pivot before finishing its
-// update (+2%).  Meanwhile warps 2-7 copy the panel rows; a block smaller than CB (the last) is
-// padded with the identity.
+// The block's CB pivots are a chain of dependent steps, so it is factored by four warps with the
+// rows in registers (right-looking; threads i and CB + i hold the even and the odd columns of row i;
+// per pivot: the pivot thread's reciprocal square root (the pivot is d rsqrt(d)), a named barrier of
+// the four warps, the column through shared memory, a rank-1 update of the row in registers, split
+// between the two threads of the row).  Three variants measured no faster: one barrier per pivot
+// with every row forming the reciprocal square root from a double-buffered column (+8%), a
+// look-ahead in which row j + 1 forms the next pivot before finishing its update (+2%), and (with
+// two factoring warps) the update of a whole row by one thread.  Meanwhile warps 4-7 copy the
+// panel rows; a block smaller than CB (the last) is padded with the identity.
 // The inverse X = L^-1 goes by 32 x 32 blocks: warps 0 and 1 run the forward substitutions of
 // X11 and X22 (lane = column, in registers, four partial sums per row), then all eight warps form
 // X21 = -X22 (L21 X11).  Every loop is unrolled, so the row and column registers are addressed at
 // compile time (a variant with the pivot loop rolled and the row shifted through the registers ran
 // slower).
 constexpr int HB = CB / 2, HBP = HB + 1;   // half blocks of the block inverse
-__device__ __forceinline__ void potrf_bar() { asm volatile("bar.sync 1, %0;" ::"n"(CB) : "memory"); }
+constexpr int FT = 2 * CB;     // factoring threads: a row's even and odd columns
+__device__ __forceinline__ void potrf_bar() { asm volatile("bar.sync 1, %0;" ::"n"(FT) : "memory"); }
 
 // FACTOR = false: the band already holds a Cholesky factor; only the diagonal block's inverse is
 // formed (block k0 = blockIdx.x CB, every block in one launch; no panel copy, nothing written back).
 template <bool FACTOR>
 __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int k0, const __grid_constant__ FactorBatch fb) {
-    static_assert(CB == 64 && POTRF_T >= CB, "two factoring warps");
+    static_assert(CB == 64 && POTRF_T > FT, "four factoring warps, the others copy");
     vx::pdl_begin();
     if constexpr (!FACTOR) k0 = blockIdx.x * CB;
     const FactorPtrs P = fptrs(fb, n, bw);
@@ -136,43 +139,51 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
     }
     __syncthreads();
     if (!FACTOR && t < CB) rinv[t] = 1.0 / D[t][t];
-    if (FACTOR && t < CB) {
-        double a[CB];
-        #pragma unroll
-        for (int c = 0; c < CB; ++c) a[c] = D[t][c];
-        #pragma unroll
-        for (int j = 0; j < CB; ++j) {
-            if (t == j) {
-                double d = a[j];
-                if (!(d > 0.0)) {                      // not positive definite: flag, keep finite
-                    if (j < w) atomicCAS(info, 0, k0 + j + 1);
-                    d = 1.0;
+    if (FACTOR && t < FT) {
+        // row t % CB; warps 0-1 hold its even columns, warps 2-3 its odd ones (H = t / CB)
+        const int row = t % CB;
+        auto factor_rows = [&](auto hc) {
+            constexpr int H = decltype(hc)::value;
+            double a[CB / 2];                          // a[i] = row, column 2 i + H
+            #pragma unroll
+            for (int i = 0; i < CB / 2; ++i) a[i] = D[row][2 * i + H];
+            #pragma unroll
+            for (int j = 0; j < CB; ++j) {
+                if ((j & 1) == H && row == j) {
+                    double d = a[j / 2];
+                    if (!(d > 0.0)) {                  // not positive definite: flag, keep finite
+                        if (j < w) atomicCAS(info, 0, k0 + j + 1);
+                        d = 1.0;
+                    }
+                    const double ri = rsqrt(d);
+                    a[j / 2] = d * ri;
+                    rinv[j] = ri;
                 }
-                const double ri = rsqrt(d);
-                a[j] = d * ri;
-                rinv[j] = ri;
+                potrf_bar();
+                if ((j & 1) == H && row > j) {
+                    a[j / 2] *= rinv[j];               // L[row][j]
+                    colj[row] = a[j / 2];
+                }
+                potrf_bar();
+                if (row > j) {
+                    const double l = colj[row];
+                    #pragma unroll
+                    for (int c = j + 1; c < CB; ++c)   // c > row: never read (upper part)
+                        if ((c & 1) == H) a[c / 2] -= l * colj[c];
+                }
+                potrf_bar();                           // colj is rewritten by the next pivot
             }
-            potrf_bar();
-            if (t > j) {
-                a[j] *= rinv[j];                       // L[t][j]
-                colj[t] = a[j];
-            }
-            potrf_bar();
-            if (t > j) {
-                const double l = a[j];
-                #pragma unroll
-                for (int c = j + 1; c < CB; ++c) a[c] -= l * colj[c];   // c > t: never read (upper part)
-            }
-            potrf_bar();                               // colj is rewritten by the next pivot
-        }
-        #pragma unroll
-        for (int c = 0; c < CB; ++c) D[t][c] = c <= t ? a[c] : 0.0;
-    } else if (FACTOR) {                               // meanwhile warps 2-7 copy the panel rows
+            #pragma unroll
+            for (int i = 0; i < CB / 2; ++i) D[row][2 * i + H] = 2 * i + H <= row ? a[i] : 0.0;
+        };
+        if (t < CB) factor_rows(std::integral_constant<int, 0>{});
+        else factor_rows(std::integral_constant<int, 1>{});
+    } else if (FACTOR) {                               // meanwhile warps 4-7 copy the panel rows
         // in batches whose loads are all issued before their stores: the band and the panel share
         // one workspace, so the compiler may not move a load above an earlier store by itself
-        constexpr int CPB = 16, CPT = POTRF_T - CB;
+        constexpr int CPB = 16, CPT = POTRF_T - FT;
         const int total = (rend - base) * CB;
-        for (int i0 = t - CB; i0 < total; i0 += CPB * CPT) {
+        for (int i0 = t - FT; i0 < total; i0 += CPB * CPT) {
             double v[CPB];
             #pragma unroll
             for (int u = 0; u < CPB; ++u) {
