@@ -9,10 +9,10 @@
 //   * per block column k of CB = 64 columns, two launches:
 //       band_potrf:   one CTA (a thread per row) factors the CB x CB diagonal block in shared memory
 //                     and inverts it;
-//       band_update:  one CTA per lower tile (I, J) of the rows the block column reaches (at most
-//                     bw below it) forms the panel rows L_I = A_I L_kk^-T and L_J the same way (a
-//                     64 x 64 product with the block's inverse), writes L_I (diagonal tiles only),
-//                     and subtracts L_I L_J^T from the band;
+//       band_update:  four CTAs per lower 64 x 64 tile (I, J) of the rows the block column reaches
+//                     (at most bw below it), one per 32 x 32 quadrant, form their rows of the panels
+//                     L_I = A_I L_kk^-T and L_J (a product with the block's inverse), write L_I
+//                     (diagonal tiles only) and subtract L_I L_J^T from the band;
 //   * band_inverse_blocked: X = L^-1 by blocks of 32 rows x 16 columns, a band GEMM per block and
 //                     the diagonal block inverses band_potrf kept (bands up to about 550 wide);
 //   * band_inverse:   (wider bands) X = L^-1 column by column: a CTA owns 32 consecutive columns (one warp each),
@@ -253,14 +253,18 @@ __global__ void __launch_bounds__(POTRF_T) band_potrf_kernel(int n, int bw, int 
     }
 }
 
-// One lower tile (I, J) of the rows below block column k0: rows ri = base + I*CB + r, rj = base +
-// J*CB + c, base = k0 + w.  Dynamic shared memory: the block inverse and the two panels (3 CB x CBP).
-// Thread t computes a 4 x 4 register block of every product: rows t / 16 + 16 a, columns t % 16 +
-// 16 b (a, b < 4), so each step of a sum loads 8 values for 16 (or 32) multiply-adds and the
-// accumulations run as independent chains.
+// One quadrant (qa, qb) of a lower tile (I, J) of the rows below block column k0, CTA 4 tile + 2 qa + qb:
+// rows ri = base + I CB + UQ qa + r, rj = base + J CB + UQ qb + c (r, c < UQ), base = k0 + w.  Four
+// CTAs per tile (each needs only its UQ rows of the two panels) keep the chain step short: about
+// 0.33M multiply-adds per CTA instead of 0.79M for a whole tile.  Dynamic shared memory: the block
+// inverse (CB x CBP) and the two half panels (2 UQ x CBP).  Thread t: rows t / 16 + 16 a, columns
+// t % 16 + 16 b of each product (a < 2; b < 4 for the panels, b < 2 for the trailing update), so the
+// accumulations run as independent chains.  The upper quadrant of a diagonal tile has nothing below
+// the diagonal and returns at once; its lower-left quadrants store the finished panel rows.
+constexpr int UQ = CB / 2;
 __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, int k0, int tiles,
                                                                const __grid_constant__ FactorBatch fb) {
-    static_assert(UPDATE_T == 256 && CB == 64, "16 x 16 threads, 4 x 4 outputs each");
+    static_assert(UPDATE_T == 256 && CB == 64, "16 x 16 threads over 32-row quadrants");
     vx::pdl_begin();
     const FactorPtrs P = fptrs(fb, n, bw);
     double* __restrict__ lb = P.lb;
@@ -269,99 +273,122 @@ __global__ void __launch_bounds__(UPDATE_T) band_update_kernel(int n, int bw, in
     extern __shared__ __align__(16) double sm[];
     double (*Xi)[CBP] = reinterpret_cast<double (*)[CBP]>(sm);
     double (*PI)[CBP] = reinterpret_cast<double (*)[CBP]>(sm + CB * CBP);
-    double (*PJ)[CBP] = reinterpret_cast<double (*)[CBP]>(sm + 2 * CB * CBP);
-    // tile index -> (I, J), I >= J
-    int I = 0, rem = blockIdx.x;
+    double (*PJ)[CBP] = reinterpret_cast<double (*)[CBP]>(sm + (CB + UQ) * CBP);
+    const int tile = int(blockIdx.x) >> 2, qa = (int(blockIdx.x) >> 1) & 1, qb = int(blockIdx.x) & 1;
+    int I = 0, rem = tile;                             // tile index -> (I, J), I >= J
     while (rem > I) { rem -= I + 1; ++I; }
     const int J = rem;
+    if (I == J && qa < qb) return;                     // upper quadrant of a diagonal tile
+    const bool same = I == J && qa == qb;              // both panels are the same rows
     const int w = min(CB, n - k0);
     const int base = k0 + w;
     const int rend = min(n, k0 + w + bw);              // rows the block column reaches
-    const int ri0 = base + I * CB, rj0 = base + J * CB;
-    if (ri0 >= rend) return;                           // (never: the grid covers the window exactly)
+    const int ri0 = base + I * CB + UQ * qa, rj0 = base + J * CB + UQ * qb;
+    if (ri0 >= rend) return;                           // the quadrant lies beyond the reach (rj0 <= ri0)
     #pragma unroll
-    for (int t = threadIdx.x; t < CB * CB; t += UPDATE_T) {
-        const int r = t / CB, c = t % CB;
-        Xi[r][c] = dinv[t];
+    for (int u = 0; u < CB * CB / UPDATE_T; ++u) {
+        const int i = threadIdx.x + u * UPDATE_T;
+        Xi[i / CB][i % CB] = dinv[i];
+    }
+    #pragma unroll
+    for (int u = 0; u < UQ * CB / UPDATE_T; ++u) {
+        const int i = threadIdx.x + u * UPDATE_T, r = i / CB, c = i % CB;
         const int ri = ri0 + r, rj = rj0 + r;
         PI[r][c] = ri < rend ? apanel[int64_t(ri - base) * CB + c] : 0.0;
-        PJ[r][c] = rj < rend ? apanel[int64_t(rj - base) * CB + c] : 0.0;
+        if (!same) PJ[r][c] = rj < rend ? apanel[int64_t(rj - base) * CB + c] : 0.0;
     }
     __syncthreads();
     const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
     // panels: P <- P X^T, P[r][m] = sum_p A[r][p] X[m][p] (X lower triangular: the full sum is exact)
-    double oi[4][4], oj[4][4];
+    double oi[2][4], oj[2][4];
     #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < 2; ++a) {
         #pragma unroll
         for (int b = 0; b < 4; ++b) { oi[a][b] = 0.0; oj[a][b] = 0.0; }
     }
-    #pragma unroll 4
-    for (int p = 0; p < CB; ++p) {
-        double ai[4], aj[4], x[4];
-        #pragma unroll
-        for (int a = 0; a < 4; ++a) { ai[a] = PI[tr + 16 * a][p]; aj[a] = PJ[tr + 16 * a][p]; }
-        #pragma unroll
-        for (int b = 0; b < 4; ++b) x[b] = Xi[tc + 16 * b][p];
-        #pragma unroll
-        for (int a = 0; a < 4; ++a) {
+    if (same) {
+        #pragma unroll 4
+        for (int p = 0; p < CB; ++p) {
+            double ai[2], x[4];
             #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                oi[a][b] = fma(ai[a], x[b], oi[a][b]);
-                oj[a][b] = fma(aj[a], x[b], oj[a][b]);
+            for (int a = 0; a < 2; ++a) ai[a] = PI[tr + 16 * a][p];
+            #pragma unroll
+            for (int b = 0; b < 4; ++b) x[b] = Xi[tc + 16 * b][p];
+            #pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                #pragma unroll
+                for (int b = 0; b < 4; ++b) oi[a][b] = fma(ai[a], x[b], oi[a][b]);
+            }
+        }
+    } else {
+        #pragma unroll 4
+        for (int p = 0; p < CB; ++p) {
+            double ai[2], aj[2], x[4];
+            #pragma unroll
+            for (int a = 0; a < 2; ++a) { ai[a] = PI[tr + 16 * a][p]; aj[a] = PJ[tr + 16 * a][p]; }
+            #pragma unroll
+            for (int b = 0; b < 4; ++b) x[b] = Xi[tc + 16 * b][p];
+            #pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                #pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    oi[a][b] = fma(ai[a], x[b], oi[a][b]);
+                    oj[a][b] = fma(aj[a], x[b], oj[a][b]);
+                }
             }
         }
     }
     __syncthreads();
     #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < 2; ++a) {
         #pragma unroll
         for (int b = 0; b < 4; ++b) {
             PI[tr + 16 * a][tc + 16 * b] = oi[a][b];
-            PJ[tr + 16 * a][tc + 16 * b] = oj[a][b];
+            if (!same) PJ[tr + 16 * a][tc + 16 * b] = oj[a][b];
         }
     }
     __syncthreads();
-    if (I == J) {                                      // the panel rows of tile I are final: store them
-        for (int t = threadIdx.x; t < CB * CB; t += UPDATE_T) {
+    double (*QJ)[CBP] = same ? PI : PJ;
+    if (I == J && qb == 0) {                           // these panel rows of tile I are final: store them
+        for (int t = threadIdx.x; t < UQ * CB; t += UPDATE_T) {
             const int r = t / CB, c = t % CB, ri = ri0 + r, col = k0 + c;
             if (c < w && ri < rend && ri - col <= bw) lb[bidx(ri, col, bw)] = PI[r][c];
         }
     }
-    // trailing update of the tile: A[ri][rj] -= sum_m L[ri][m] L[rj][m] (lower triangle, in the band)
-    double o[4][4];
+    // trailing update of the quadrant: A[ri][rj] -= sum_m L[ri][m] L[rj][m] (lower triangle, in the band)
+    double o[2][2];
     #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < 2; ++a) {
         #pragma unroll
-        for (int b = 0; b < 4; ++b) o[a][b] = 0.0;
+        for (int b = 0; b < 2; ++b) o[a][b] = 0.0;
     }
     #pragma unroll 4
     for (int m = 0; m < CB; ++m) {
-        double pi[4], pj[4];
+        double pi[2], pj[2];
         #pragma unroll
-        for (int a = 0; a < 4; ++a) pi[a] = PI[tr + 16 * a][m];
+        for (int a = 0; a < 2; ++a) pi[a] = PI[tr + 16 * a][m];
         #pragma unroll
-        for (int b = 0; b < 4; ++b) pj[b] = PJ[tc + 16 * b][m];
+        for (int b = 0; b < 2; ++b) pj[b] = QJ[tc + 16 * b][m];
         #pragma unroll
-        for (int a = 0; a < 4; ++a) {
+        for (int a = 0; a < 2; ++a) {
             #pragma unroll
-            for (int b = 0; b < 4; ++b) o[a][b] = fma(pi[a], pj[b], o[a][b]);
+            for (int b = 0; b < 2; ++b) o[a][b] = fma(pi[a], pj[b], o[a][b]);
         }
     }
-    double cur[4][4];                                  // every old value read before any write
+    double cur[2][2];                                  // every old value read before any write
     #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < 2; ++a) {
         #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < 2; ++b) {
             const int ri = ri0 + tr + 16 * a, rj = rj0 + tc + 16 * b;
             const bool in = ri < rend && rj < rend && rj <= ri && ri - rj <= bw;
             cur[a][b] = in ? lb[bidx(ri, rj, bw)] : 0.0;
         }
     }
     #pragma unroll
-    for (int a = 0; a < 4; ++a) {
+    for (int a = 0; a < 2; ++a) {
         #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < 2; ++b) {
             const int ri = ri0 + tr + 16 * a, rj = rj0 + tc + 16 * b;
             if (ri >= rend || rj >= rend || rj > ri || ri - rj > bw) continue;
             lb[bidx(ri, rj, bw)] = cur[a][b] - o[a][b];
@@ -669,7 +696,7 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
         }
     }
     const size_t psm = size_t(2 * CB * CBP + HB * HBP) * sizeof(double);
-    const size_t usm = size_t(3) * CB * CBP * sizeof(double);
+    const size_t usm = size_t(CB + 2 * UQ) * CBP * sizeof(double);
     const size_t ism = size_t(INV_STAGES + nw) * (bw + 1) * sizeof(double);
     static std::atomic<uint64_t> opt_p, opt_u, opt_i, opt_b;
     int st = smem_opt_in(opt_p, (const void*)band_potrf_kernel<true>, psm, what);
@@ -686,7 +713,7 @@ static int coarse_factor_batch(const char* what, int n, int bw, int count, const
         const int rows = std::min(n, k0 + w + bw) - (k0 + w);
         if (rows <= 0) continue;
         const int T = (rows + CB - 1) / CB;
-        vx::launch(band_update_kernel, dim3(unsigned(T * (T + 1) / 2), B), UPDATE_T, usm, stream, n, bw, k0, T, fb);
+        vx::launch(band_update_kernel, dim3(unsigned(4 * (T * (T + 1) / 2)), B), UPDATE_T, usm, stream, n, bw, k0, T, fb);
     }
     const InvbLayout<INV_TC> il(bw);
     if (il.bytes <= 227 * 1024) {
