@@ -117,6 +117,34 @@ class ElasticitySolver:
 
 _SOLVERS = OrderedDict()      # set-up key -> ElasticitySolver, least recently used first
 _SOLVER_CACHE_SIZE = 4
+_COPY_STREAMS = {}            # device index -> side stream for host-to-device staging
+
+
+def _stage_inputs(mask, E, force):
+    """Device copies of solve()'s inputs, mask first and force last.  Pinned CPU tensors go through a
+    side stream, so the current stream can refresh the hierarchy and factor the coarsest system as
+    soon as the mask and the moduli have arrived, while the force is still in transit; the current
+    stream waits on an event before each use.  Other inputs (numpy arrays, pageable tensors) are
+    copied on the current stream as before.  Returns (mask, E, force, wait) with wait(i) making the
+    current stream wait for input i (0 mask, 1 E, 2 force)."""
+    pinned = all(isinstance(a, torch.Tensor) and not a.is_cuda and a.is_pinned() for a in (mask, E, force))
+    if not pinned:
+        return mask, E, force, lambda i: None
+    cur = torch.cuda.current_stream()
+    side = _COPY_STREAMS.get(cur.device.index)
+    if side is None:
+        side = _COPY_STREAMS[cur.device.index] = torch.cuda.Stream(device=cur.device)
+    side.wait_stream(cur)                         # nothing earlier on the current stream is overtaken
+    out, events = [], []
+    with torch.cuda.stream(side):
+        for a in (mask, E, force):
+            d = a.to("cuda", non_blocking=True)
+            d.record_stream(cur)                  # freed only after the current stream's uses
+            ev = torch.cuda.Event()
+            ev.record(side)
+            out.append(d)
+            events.append(ev)
+    return out[0], out[1], out[2], lambda i: cur.wait_event(events[i])
 
 
 def clear_solver_cache():
@@ -136,12 +164,16 @@ def solve(shape, E, force, mask, *, ke=None, precision="mixed", tol=1e-8, maxite
     Solvers are kept for the last few set-ups (grid, element, precision, cycle, damping, levels):
     a call with a known set-up copies its inputs into that solver and recomputes every level's
     moduli, masks, diagonals and the coarsest factor from them, reusing the device buffers and
-    the captured solve graph."""
+    the captured solve graph.  With pinned CPU tensors as inputs the force is copied to the device
+    while the hierarchy refresh and the coarsest factorisation run."""
     shape = tuple(int(v) for v in shape)
     ke_key = None if ke is None else np.asarray(ke, dtype=np.float64).tobytes()
     om_key = tuple(omega) if isinstance(omega, (list, tuple)) else omega
     key = (shape, ke_key, precision, int(check_every), int(pre), int(post), om_key, int(max_coarse_x), levels)
     s = _SOLVERS.pop(key, None)
+    mask, E, force, wait = _stage_inputs(mask, E, force)
+    wait(0)
+    wait(1)
     if s is None:
         s = ElasticitySolver(shape, E, mask, ke=ke, precision=precision, pre=pre, post=post, omega=omega,
                              max_coarse_x=max_coarse_x, levels=levels, tol=tol, maxiter=maxiter,
@@ -152,6 +184,7 @@ def solve(shape, E, force, mask, *, ke=None, precision="mixed", tol=1e-8, maxite
     while len(_SOLVERS) > _SOLVER_CACHE_SIZE:
         _SOLVERS.popitem(last=False)
     s.fcg.tol, s.fcg.maxiter = float(tol), int(maxiter)
+    wait(2)
     f = _dev(force)
     s.fcg.launch(f, dot_with=f)                    # the compliance f . u comes back with the solver scalars
     res = s.fcg.finish()

@@ -262,6 +262,27 @@ def test_host_api_reuses_its_setup_for_new_inputs():
     assert rel(u1b, u1) < 1e-12
 
 
+def test_host_api_with_pinned_inputs_equals_numpy_inputs():
+    """Pinned CPU tensors go through the side copy stream (the force still in transit while the
+    hierarchy refresh and coarsest factorisation run); the result must be bit-for-bit the one from
+    numpy inputs, also into a pinned `out` buffer, on a cold and on a reused set-up."""
+    shape = (24, 12, 16)
+    mask, force = vo.cantilever_equal_split(shape)
+    E = vx.problems.simp_modulus(vx.problems.gaussian_random_field(shape, 4.0, 3), 1e-9).cpu().numpy()
+    kw = dict(precision="mixed", tol=1e-10, maxiter=200, check_every=1)
+    vx.clear_solver_cache()
+    u_np, i_np = vx.solve(shape, E, force, mask, **kw)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    for cold in (True, False):                                    # a new set-up, then the kept one
+        if cold:
+            vx.clear_solver_cache()
+        out = torch.empty(force.size, dtype=torch.float64).pin_memory()
+        u_pin, i_pin = vx.solve(shape, pin(E), pin(force), pin(mask), out=out, **kw)
+        assert i_pin["iterations"] == i_np["iterations"] and i_pin["converged"]
+        assert np.array_equal(np.asarray(u_pin), u_np)
+        assert i_pin["compliance"] == i_np["compliance"]
+
+
 def test_pcg_ir_matches_the_donor_record():
     """The 32x16x16 case (i.i.d. densities), donor pcg_ir at tol 1e-8, inner tolerance 0.1: the
     reference's run takes 6 outer passes and 1400 inner FP32 iterations.  The inner products here
